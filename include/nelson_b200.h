@@ -1,0 +1,207 @@
+/*
+ * nelson_b200.h -- C ABI of the B200-native Schur-complement LM/GN engine.
+ *
+ * This is the drop-in boundary for nelson's SolverCholeskySchur hot path.
+ * The reference binds its solver at compile time (SolverTraits<id>::Solver,
+ * nelson/SolverTraits.h:16-56) and drives it from LevenbergMarquardt /
+ * GaussNewton through two concepts:
+ *   - the Solver concept: init(H, b), maxAbsHDiag(), computeIncrement(H, b,
+ *     relLambda, absLambda) -> bool, incrementVector(),
+ *     incrementVectorSquaredNorm()   (nelson/SolverCholeskySchur.h:96-115);
+ *   - the problem concept: update(bool), hessian().chi2()/maxAbsValBVect(),
+ *     oplus(inc), backupSolution(), rollbackSolution(),
+ *     computeRhoChi2Change(mu, inc, oldChi2)
+ *     (nelson/LevenbergMarquardt.hpp:41-136, nelson/DoubleSection.h:300-311).
+ * Each entry point below replaces one of those calls; the C++ headers in
+ * include/nelson_b200/ wrap them back into the reference's class shapes.
+ *
+ * Conventions: plain pointers and sizes, host memory unless a name says
+ * "device"; every function returns an nl_status (0 = ok).  A handle owns its
+ * device memory and one CUDA stream; calls on one handle must not overlap,
+ * calls on different handles may run from different threads.
+ */
+#ifndef NELSON_B200_H
+#define NELSON_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+typedef enum {
+  NL_OK = 0,
+  NL_ERR_ARG = 1,          /* bad argument / size / index                      */
+  NL_ERR_STATE = 2,        /* call out of order (e.g. update before structure) */
+  NL_ERR_CUDA = 3,         /* a CUDA runtime / cuBLAS call failed              */
+  NL_ERR_UNSUPPORTED = 4,  /* structure outside the device solver's scope      */
+  NL_ERR_NOT_SPD = 5,      /* a damped block or the reduced system not SPD     */
+  NL_ERR_NONFINITE = 6,    /* non-finite cost / increment                      */
+  NL_ERR_TIMEOUT = 7,      /* a bounded device-side wait gave up               */
+  NL_ERR_NOMEM = 8         /* device allocation failed                         */
+} nl_status;
+
+/* ---- precision modes ---------------------------------------------------- */
+#define NL_PREC_FP64 0  /* Jacobians, Hessian, Schur and Cholesky in FP64      */
+#define NL_PREC_MIXED 1 /* FP32 Jacobians/Hessian/Schur, tensor-core trailing
+                           updates, FP64 diagonal panels + refinement + cost   */
+
+/* ---- settings (same fields and defaults as the reference) --------------- */
+/* LevenbergMarquardtSettings, nelson/LevenbergMarquardt.h:18-34;
+ * defaults nelson/LevenbergMarquardt.cpp:6-19. */
+typedef struct {
+  int maxNumIt, maxNumSubIt, minNumIt;
+  double epsBVector, epsIncSquare, epsChi2, tau, penaltyV, initV;
+  double maxScaleFactor, minScaleFactor;
+} nl_lm_settings;
+
+/* GaussNewtonSettings, nelson/GaussNewton.h:18-30; defaults GaussNewton.cpp:12-22. */
+typedef struct {
+  int maxNumIt, minNumIt;
+  double epsBVector, epsIncSquare, epsChi2, absLambda, relLambda;
+} nl_gn_settings;
+
+/* Termination reasons, in the order of nelson/LevenbergMarquardt.h:36-44
+ * (GN uses the first six, nelson/GaussNewton.h:34-41). */
+#define NL_SUCCESS_AT_START 0
+#define NL_SUCCESS_SMALL_INCREMENT 1
+#define NL_SUCCESS_EPS_B 2
+#define NL_SUCCESS_SMALL_RESIDUALS 3
+#define NL_SOLVER_FAILURE 4
+#define NL_MAX_ITERATION_REACHED 5
+#define NL_MAX_SUBITERATION_REACHED 6
+
+/* One trace record per sub-iteration: it, subit, chi2, mu, rho, |inc|^2, ok,
+ * accepted (the LevenbergMarquardtStats content, nelson/LevenbergMarquardt.h:57-85,
+ * plus the damping and gain ratio). */
+#define NL_TRACE_STRIDE 8
+
+typedef struct {
+  int reason;          /* NL_SUCCESS_* / NL_*_REACHED / NL_SOLVER_FAILURE */
+  int iterations;      /* numIterations() */
+  int subiterations;   /* total computeIncrement calls */
+  int n_trace;         /* records written */
+  double chi2;         /* final cost */
+  double mu;           /* final damping */
+} nl_solve_report;
+
+/* Per-phase device time of the last computeIncrement, milliseconds
+ * (the phases of SolverCholeskySchurIterationTimeStat, nelson/SolverCholeskySchur.h:25-38). */
+typedef struct {
+  float vinv_ms, wvinv_bs_ms, schur_ms, factor_ms, solve_ms, backsub_ms, total_ms;
+  float eval_ms; /* last update(true) */
+} nl_phase_times;
+
+/* ---- problem: device-resident BA section -------------------------------- */
+typedef struct nl_problem nl_problem;
+
+typedef struct {
+  int bc;              /* camera block size: 6 (pose) or 9 (pose, f, k1, k2) */
+  int nc_var, nc_fix;  /* variable / fixed cameras  (numParametersU + numFixedParametersU) */
+  int np_var, np_fix;  /* variable / fixed points   (numParametersV + numFixedParametersV) */
+  int precision;       /* NL_PREC_FP64 or NL_PREC_MIXED */
+  double f, cx, cy;    /* focal (6-parameter cameras) and principal point */
+  int refine_sweeps;   /* iterative-refinement sweeps on S (mixed); -1 = default */
+  int device;          /* CUDA device ordinal */
+} nl_problem_desc;
+
+/* DoubleSection constructor + parametersReady (nelson/DoubleSection.hpp:67-80). */
+nl_status nl_create(const nl_problem_desc* desc, nl_problem** out);
+nl_status nl_destroy(nl_problem* h);
+
+/* Parameter blocks: cameras (axis-angle[3], t[3] [, f, k1, k2]) variable first
+ * then fixed; points xyz.  Replaces the user's parameterU/parameterV storage
+ * (nelson/DoubleSection.h:226-229). */
+nl_status nl_set_params(nl_problem* h, const double* cams, const double* pts);
+nl_status nl_get_params(nl_problem* h, double* cams, double* pts);
+/* Camera state as stored on the device: R[9] row-major, t[3], f, k1, k2, pad. */
+nl_status nl_get_camera_state(nl_problem* h, double* states);
+
+/* DoubleSection::addEdge(NodeId cam, NodeId pt, EdgeBinaryUV*)
+ * (nelson/DoubleSection.hpp:338-365), vectorised; cam_fixed / pt_fixed mark
+ * NodeType::Fixed ids (nelson/EdgeInterface.h:35-55); weight may be NULL. */
+nl_status nl_add_ba_edges(nl_problem* h, int ne, const int* cam, const int* cam_fixed,
+                          const int* pt, const int* pt_fixed, const double* obs,
+                          const double* weight);
+/* DoubleSection::setUser2InternalIndexesU (nelson/DoubleSection.hpp:23-27). */
+nl_status nl_set_user2internal_u(nl_problem* h, const int* perm);
+/* DoubleSection::structureReady (nelson/DoubleSection.hpp:83-246): builds the
+ * U/V/W patterns and block UIDs exactly as the reference and uploads the
+ * edge -> block maps. */
+nl_status nl_structure_ready(nl_problem* h);
+/* Replace observations / weights of an existing structure (same edge order). */
+nl_status nl_set_observations(nl_problem* h, const double* obs, const double* weight);
+
+/* counts = {U blocks, V blocks, W blocks, edges}; patterns are (row, col)
+ * per UID; edge UIDs are EdgeBinaryBase::H_11/12/22_Uid (nelson/EdgeBinary.h:12-14). */
+nl_status nl_get_counts(nl_problem* h, int* counts);
+nl_status nl_get_patterns(nl_problem* h, int* u_rc, int* v_rc, int* w_rc);
+nl_status nl_get_edge_uids(nl_problem* h, int* h11, int* h12, int* h22);
+
+/* DoubleSection::update(bool) (nelson/DoubleSection.hpp:452-467). */
+nl_status nl_update(nl_problem* h, int hessian, double* chi2);
+/* Hessian blocks in UID order (row-major blocks), bU in internal order, FP64. */
+nl_status nl_get_hessian(nl_problem* h, double* U, double* V, double* W, double* bU, double* bV);
+
+/* SolverCholeskySchur::init / maxAbsHDiag / computeIncrement /
+ * incrementVector / incrementVectorSquaredNorm (nelson/SolverCholeskySchur.hpp:44-157). */
+nl_status nl_solver_init(nl_problem* h);
+nl_status nl_max_abs_hdiag(nl_problem* h, double* out);
+nl_status nl_compute_increment(nl_problem* h, double rel_lambda, double abs_lambda, int* ok);
+nl_status nl_get_increment(nl_problem* h, double* incU, double* incV);
+nl_status nl_inc_sqnorm(nl_problem* h, double* out);
+/* The damped reduced camera system as formed (n x n row-major, the upper
+ * triangle holds S as the reference builds it) and bS; *n gets the size. */
+nl_status nl_get_schur(nl_problem* h, double* S, double* bS, int* n);
+
+/* Problem concept: oplus / backupSolution / rollbackSolution /
+ * maxAbsValBVect / chi2 / computeRhoChi2Change. */
+nl_status nl_oplus(nl_problem* h);
+nl_status nl_backup(nl_problem* h);
+nl_status nl_rollback(nl_problem* h);
+nl_status nl_max_abs_b(nl_problem* h, double* out);
+nl_status nl_chi2(nl_problem* h, double* out);
+nl_status nl_rho(nl_problem* h, double mu, double old_chi2, double* out);
+
+/* LevenbergMarquardt<Solver>::solve (nelson/LevenbergMarquardt.hpp:36-146)
+ * with the whole iteration on the device; trace may be NULL. */
+nl_status nl_lm_solve(nl_problem* h, const nl_lm_settings* s, nl_solve_report* rep,
+                      double* trace, int trace_cap);
+/* GaussNewton<Solver>::solve (nelson/GaussNewton.hpp:32-127). */
+nl_status nl_gn_solve(nl_problem* h, const nl_gn_settings* s, nl_solve_report* rep,
+                      double* trace, int trace_cap);
+
+nl_status nl_phase_timings(nl_problem* h, nl_phase_times* out);
+/* Number of kernels of this library launched on the handle since creation. */
+nl_status nl_kernel_launches(nl_problem* h, long long* out);
+
+/* ---- solver-only drop-in: host Hessian in, increment out ------------------ */
+/* SolverCholeskySchur on a Hessian the caller assembled (any U pattern, any W
+ * pattern, block-diagonal V with 3x3 blocks): patterns are (row, col) per UID
+ * in the reference's storage order (U upper CSC, V diagonal, W CSR). */
+typedef struct nl_solver nl_solver;
+typedef struct {
+  int bu;          /* U block size, 1..9 */
+  int nu, nv;      /* number of U / V parameter blocks */
+  int nU, nV, nW;  /* block counts */
+  int precision;
+  int refine_sweeps;
+  int device;
+} nl_solver_desc;
+nl_status nl_solver_create(const nl_solver_desc* d, const int* u_rc, const int* v_rc,
+                           const int* w_rc, nl_solver** out);
+nl_status nl_solver_destroy(nl_solver* s);
+/* Upload U, V, W blocks (row-major per block) and bU, bV (FP64 host). */
+nl_status nl_solver_set_hessian(nl_solver* s, const double* U, const double* V,
+                                const double* W, const double* bU, const double* bV);
+nl_status nl_solver_max_abs_hdiag(nl_solver* s, double* out);
+nl_status nl_solver_compute_increment(nl_solver* s, double rel_lambda, double abs_lambda,
+                                      double* incU, double* incV, int* ok);
+
+const char* nl_status_string(int status);
+/* Library build identification: "nelson_b200 <version> sm_100a". */
+const char* nl_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1059 @@
+// nl_api.cu -- the C ABI of include/nelson_b200.h: device-resident BA section
+// (DoubleSection), SolverCholeskySchur core, and LM / GN drivers.
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <vector>
+
+#include "ba_kernels.cuh"
+#include "schur_core.cuh"
+
+using namespace nl;
+
+namespace {
+
+constexpr int kCostNT = 256;
+constexpr int kCostCTAs = 592;  // 4 x 148 SMs, fixed -> fixed summation order
+constexpr int kCamNT = 128;
+
+inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+void so3_exp_host(const double* w, double* R) {
+  const double th2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+  double A, B;
+  if (th2 < 1e-8) {
+    A = 1.0 - th2 / 6.0 + th2 * th2 / 120.0;
+    B = 0.5 - th2 / 24.0 + th2 * th2 / 720.0;
+  } else {
+    const double th = std::sqrt(th2);
+    A = std::sin(th) / th;
+    B = (1.0 - std::cos(th)) / th2;
+  }
+  const double K[9] = {0, -w[2], w[1], w[2], 0, -w[0], -w[1], w[0], 0};
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      double k2 = 0;
+      for (int k = 0; k < 3; k++) k2 += K[i * 3 + k] * K[k * 3 + j];
+      R[i * 3 + j] = A * K[i * 3 + j] + B * k2 + (i == j ? 1.0 : 0.0);
+    }
+}
+
+void so3_log_host(const double* R, double* w) {
+  const double tr = R[0] + R[4] + R[8];
+  const double c = std::max(-1.0, std::min(1.0, 0.5 * (tr - 1.0)));
+  const double th = std::acos(c);
+  const double v[3] = {R[7] - R[5], R[2] - R[6], R[3] - R[1]};
+  if (th < 1e-6) {
+    for (int i = 0; i < 3; i++) w[i] = 0.5 * v[i];
+    return;
+  }
+  if (M_PI - th < 1e-4) {
+    int k = 0;
+    if (R[4] > R[k * 4]) k = 1;
+    if (R[8] > R[k * 4]) k = 2;
+    double a[3];
+    const double d = std::sqrt(std::max(0.0, 0.5 * (R[k * 4] + 1.0)));
+    a[k] = d;
+    for (int i = 0; i < 3; i++)
+      if (i != k) a[i] = (0.25 * (R[i * 3 + k] + R[k * 3 + i])) / d;
+    const double nn = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    const double s = (v[0] * a[0] + v[1] * a[1] + v[2] * a[2]) < 0 ? -1.0 : 1.0;
+    for (int i = 0; i < 3; i++) w[i] = s * th * a[i] / nn;
+    return;
+  }
+  const double f = th / (2.0 * std::sin(th));
+  for (int i = 0; i < 3; i++) w[i] = f * v[i];
+}
+
+}  // namespace
+
+// ===========================================================================
+struct nl_problem {
+  nl_problem_desc desc{};
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cublasHandle_t cublas = nullptr;
+  DevBuf cublas_ws;
+  bool ready = false;
+  // host copies
+  std::vector<double> cam_state;  // nc_all x 16
+  std::vector<double> pts;        // np_all x 3
+  std::vector<int> e_cam, e_camfix, e_pt, e_ptfix;
+  std::vector<double> e_obs, e_w;
+  std::vector<int> perm;  // user -> internal
+  // structure
+  int nU = 0, nV = 0, nW = 0, nci = 0, ngrp = 0;
+  std::vector<int> u_rc, v_rc, w_rc, h11, h12, h22;
+  std::vector<int> eorder;   // device E-order -> insertion index
+  std::vector<int> porder;   // device P-order -> insertion index
+  // device
+  DevBuf cam, pt, cam_bck, pt_bck;
+  DevBuf d_e_cam, d_e_pt, d_e_obs, d_e_w, d_cam_grp_ptr, d_grp_edge_ptr, d_grp_wuid, d_cam_uid, d_cam_slot;
+  DevBuf d_pt_edge_ptr, d_p_cam, d_p_obs, d_p_w, d_pt_vuid;
+  DevBuf d_part, d_scal, d_lm, d_trace;
+  std::unique_ptr<SchurCore> core;
+  BaDev ba{};
+  // scalars on the device: [0] chi2, [1] maxAbsB, [2] maxAbsHDiag, [3] rho
+  double* scal = nullptr;
+  LmDev* lm = nullptr;
+  int* status = nullptr;  // solver status (inside LmDev)
+  double* host_pin = nullptr;
+  double lam_host[2] = {0, 0};
+  DevBuf d_lam;
+  long long launches = 0;
+  cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+  float eval_ms = 0;
+  int have_jac = 0;
+
+  ~nl_problem() {
+    if (cublas) cublasDestroy(cublas);
+    if (host_pin) cudaFreeHost(host_pin);
+    if (ev_a) cudaEventDestroy(ev_a);
+    if (ev_b) cudaEventDestroy(ev_b);
+    core.reset();
+    if (st) cudaStreamDestroy(st);
+  }
+  int nc_all() const { return desc.nc_var + desc.nc_fix; }
+  int np_all() const { return desc.np_var + desc.np_fix; }
+};
+
+namespace {
+
+nl_status select_device(nl_problem* h) {
+  NL_CUDA(cudaSetDevice(h->device));
+  return NL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// structureReady for BA edges (nelson/DoubleSection.hpp:83-246): U, V blocks
+// on the diagonal of every camera / point with an edge; W blocks on the
+// distinct (internal camera, point) pairs; UIDs in CSC (U, V) / CSR (W) order.
+nl_status build_structure(nl_problem* h) {
+  const int ne = (int)h->e_cam.size();
+  const int ncv = h->desc.nc_var, npv = h->desc.np_var, bc = h->desc.bc;
+  h->nci = ncv;
+  std::vector<int> has_u(ncv, 0), has_v(npv, 0);
+  for (int e = 0; e < ne; e++) {
+    if (!h->e_camfix[e]) has_u[h->perm[h->e_cam[e]]] = 1;
+    if (!h->e_ptfix[e]) has_v[h->e_pt[e]] = 1;
+  }
+  std::vector<int> u_uid(ncv, -1), v_uid(npv, -1);
+  int q = 0;
+  for (int c = 0; c < ncv; c++)
+    if (has_u[c]) u_uid[c] = q++;
+  h->nU = q;
+  q = 0;
+  for (int p = 0; p < npv; p++)
+    if (has_v[p]) v_uid[p] = q++;
+  h->nV = q;
+  // E-order: variable-camera edges sorted by (internal cam, fixed point last,
+  // point id, insertion); fixed-camera edges after.
+  std::vector<int> ord(ne);
+  std::iota(ord.begin(), ord.end(), 0);
+  auto key = [&](int e) -> long long {
+    if (h->e_camfix[e]) return (long long)(ncv + 1) << 32;
+    const long long c = h->perm[h->e_cam[e]];
+    const long long p = h->e_ptfix[e] ? (long long)npv + h->e_pt[e] : h->e_pt[e];
+    return (c << 32) | p;
+  };
+  std::vector<long long> keys(ne);
+  for (int e = 0; e < ne; e++) keys[e] = key(e);
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return keys[a] < keys[b]; });
+  h->eorder = ord;
+  // groups + W uids
+  std::vector<int> cam_grp_ptr(ncv + 1, 0), grp_edge_ptr(1, 0), grp_wuid;
+  h->h11.assign(ne, -1);
+  h->h12.assign(ne, -1);
+  h->h22.assign(ne, -1);
+  h->w_rc.clear();
+  int wq = 0;
+  for (int t = 0; t < ne;) {
+    const int e = ord[t];
+    if (h->e_camfix[e]) break;  // fixed-camera edges close the E-order
+    const int c = h->perm[h->e_cam[e]];
+    int t1 = t + 1;
+    if (!h->e_ptfix[e])
+      while (t1 < ne && keys[ord[t1]] == keys[e]) t1++;
+    int wuid = -1;
+    if (!h->e_ptfix[e]) {
+      wuid = wq++;
+      h->w_rc.push_back(c);
+      h->w_rc.push_back(h->e_pt[e]);
+    }
+    for (int s = t; s < t1; s++) h->h12[ord[s]] = wuid;
+    grp_wuid.push_back(wuid);
+    grp_edge_ptr.push_back(t1);
+    cam_grp_ptr[c + 1]++;
+    t = t1;
+  }
+  for (int c = 0; c < ncv; c++) cam_grp_ptr[c + 1] += cam_grp_ptr[c];
+  h->nW = wq;
+  h->ngrp = (int)grp_wuid.size();
+  for (int e = 0; e < ne; e++) {
+    if (!h->e_camfix[e]) h->h11[e] = u_uid[h->perm[h->e_cam[e]]];
+    if (!h->e_ptfix[e]) h->h22[e] = v_uid[h->e_pt[e]];
+  }
+  h->u_rc.clear();
+  for (int c = 0; c < ncv; c++)
+    if (u_uid[c] >= 0) {
+      h->u_rc.push_back(c);
+      h->u_rc.push_back(c);
+    }
+  h->v_rc.clear();
+  for (int p = 0; p < npv; p++)
+    if (v_uid[p] >= 0) {
+      h->v_rc.push_back(p);
+      h->v_rc.push_back(p);
+    }
+  // P-order: variable-point edges by (point, insertion)
+  std::vector<int> pord;
+  pord.reserve(ne);
+  for (int e = 0; e < ne; e++)
+    if (!h->e_ptfix[e]) pord.push_back(e);
+  std::stable_sort(pord.begin(), pord.end(), [&](int a, int b) { return h->e_pt[a] < h->e_pt[b]; });
+  h->porder = pord;
+  std::vector<int> pt_edge_ptr(npv + 1, 0);
+  for (int e : pord) pt_edge_ptr[h->e_pt[e] + 1]++;
+  for (int p = 0; p < npv; p++) pt_edge_ptr[p + 1] += pt_edge_ptr[p];
+  // device edge arrays
+  const int ncv_ = ncv;
+  auto cam_slot = [&](int e) { return h->e_camfix[e] ? ncv_ + h->e_cam[e] : h->e_cam[e]; };
+  auto pt_slot = [&](int e) { return h->e_ptfix[e] ? npv + h->e_pt[e] : h->e_pt[e]; };
+  std::vector<int> ecam(ne), ept(ne), pcam(pord.size());
+  std::vector<double> eobs(2 * (size_t)ne), ew(ne), pobs(2 * pord.size()), pw(pord.size());
+  for (int t = 0; t < ne; t++) {
+    const int e = ord[t];
+    ecam[t] = cam_slot(e);
+    ept[t] = pt_slot(e);
+    eobs[2 * t] = h->e_obs[2 * (size_t)e];
+    eobs[2 * t + 1] = h->e_obs[2 * (size_t)e + 1];
+    ew[t] = h->e_w[e];
+  }
+  for (size_t t = 0; t < pord.size(); t++) {
+    const int e = pord[t];
+    pcam[t] = cam_slot(e);
+    pobs[2 * t] = h->e_obs[2 * (size_t)e];
+    pobs[2 * t + 1] = h->e_obs[2 * (size_t)e + 1];
+    pw[t] = h->e_w[e];
+  }
+  std::vector<int> slot_of_internal(ncv);
+  for (int u = 0; u < ncv; u++) slot_of_internal[h->perm[u]] = u;
+  nl_status s;
+#define NL_TRY(x)             \
+  do {                        \
+    if ((s = (x)) != NL_OK) { \
+      return s;               \
+    }                         \
+  } while (0)
+  NL_TRY(upload(h->d_e_cam, ecam, h->st));
+  NL_TRY(upload(h->d_e_pt, ept, h->st));
+  NL_TRY(upload(h->d_e_obs, eobs, h->st));
+  NL_TRY(upload(h->d_e_w, ew, h->st));
+  NL_TRY(upload(h->d_cam_grp_ptr, cam_grp_ptr, h->st));
+  NL_TRY(upload(h->d_grp_edge_ptr, grp_edge_ptr, h->st));
+  NL_TRY(upload(h->d_grp_wuid, grp_wuid, h->st));
+  NL_TRY(upload(h->d_cam_uid, u_uid, h->st));
+  NL_TRY(upload(h->d_cam_slot, slot_of_internal, h->st));
+  NL_TRY(upload(h->d_pt_edge_ptr, pt_edge_ptr, h->st));
+  NL_TRY(upload(h->d_p_cam, pcam, h->st));
+  NL_TRY(upload(h->d_p_obs, pobs, h->st));
+  NL_TRY(upload(h->d_p_w, pw, h->st));
+  NL_TRY(upload(h->d_pt_vuid, v_uid, h->st));
+  // Schur core
+  SchurStructure ss;
+  ss.bc = bc;
+  ss.nci = ncv;
+  ss.np = npv;
+  for (size_t i = 0; i < h->u_rc.size(); i += 2) {
+    ss.u_r.push_back(h->u_rc[i]);
+    ss.u_c.push_back(h->u_rc[i + 1]);
+  }
+  ss.v_uid = v_uid;
+  for (size_t i = 0; i < h->w_rc.size(); i += 2) {
+    ss.w_r.push_back(h->w_rc[i]);
+    ss.w_c.push_back(h->w_rc[i + 1]);
+  }
+  NL_TRY(h->core->setup(ss, h->st));
+  BaDev& d = h->ba;
+  d.bc = bc;
+  d.nci = ncv;
+  d.nc_all = h->nc_all();
+  d.np_var = npv;
+  d.np_all = h->np_all();
+  d.ne = ne;
+  d.ngrp = h->ngrp;
+  d.f_fixed = h->desc.f;
+  d.cx = h->desc.cx;
+  d.cy = h->desc.cy;
+  d.cam = h->cam.as<double>();
+  d.pt = h->pt.as<double>();
+  d.e_cam = h->d_e_cam.as<int>();
+  d.e_pt = h->d_e_pt.as<int>();
+  d.e_obs = h->d_e_obs.as<double>();
+  d.e_w = h->d_e_w.as<double>();
+  d.cam_grp_ptr = h->d_cam_grp_ptr.as<int>();
+  d.grp_edge_ptr = h->d_grp_edge_ptr.as<int>();
+  d.grp_wuid = h->d_grp_wuid.as<int>();
+  d.cam_uid = h->d_cam_uid.as<int>();
+  d.cam_slot = h->d_cam_slot.as<int>();
+  d.pt_edge_ptr = h->d_pt_edge_ptr.as<int>();
+  d.p_cam = h->d_p_cam.as<int>();
+  d.p_obs = h->d_p_obs.as<double>();
+  d.p_w = h->d_p_w.as<double>();
+  d.pt_vuid = h->d_pt_vuid.as<int>();
+#undef NL_TRY
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  return NL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// update(hessian): cost always (FP64), Hessian blocks when asked.
+template <typename T, int BC>
+nl_status enqueue_eval_t(nl_problem* h, bool hessian, double* chi2_out, double* maxb_out, const int* active) {
+  cost_kernel<BC, kCostNT><<<kCostCTAs, kCostNT, 0, h->st>>>(h->ba, h->d_part.as<double>(), active);
+  sum_partials_kernel<256><<<1, 256, 0, h->st>>>(h->d_part.as<double>(), kCostCTAs, chi2_out, active);
+  h->launches += 2;
+  if (hessian) {
+    if (h->nci > 0)
+      cam_pass_kernel<T, BC, kCamNT><<<h->nci, kCamNT, 0, h->st>>>(h->ba, (T*)h->core->dU(), (T*)h->core->dW(),
+                                                                   (T*)h->core->dbU(), active);
+    if (h->desc.np_var > 0)
+      pt_pass_kernel<T, BC, 128><<<cdiv(h->desc.np_var, 128), 128, 0, h->st>>>(h->ba, (T*)h->core->dV(),
+                                                                                (T*)h->core->dbV(), active);
+    h->launches += 2;
+    nl_status s = h->core->enqueue_maxabs_b(maxb_out, active);
+    if (s != NL_OK) return s;
+  }
+  NL_CUDA(cudaGetLastError());
+  return NL_OK;
+}
+
+nl_status enqueue_eval(nl_problem* h, bool hessian, double* chi2_out, double* maxb_out, const int* active) {
+  const bool f64 = h->desc.precision == NL_PREC_FP64;
+  if (h->desc.bc == 9)
+    return f64 ? enqueue_eval_t<double, 9>(h, hessian, chi2_out, maxb_out, active)
+               : enqueue_eval_t<float, 9>(h, hessian, chi2_out, maxb_out, active);
+  return f64 ? enqueue_eval_t<double, 6>(h, hessian, chi2_out, maxb_out, active)
+             : enqueue_eval_t<float, 6>(h, hessian, chi2_out, maxb_out, active);
+}
+
+nl_status enqueue_oplus(nl_problem* h, const int* active) {
+  const int nci = h->nci;
+  if (nci > 0) {
+    if (h->desc.bc == 9)
+      oplus_cam_kernel<9><<<cdiv(nci, 128), 128, 0, h->st>>>(h->cam.as<double>(), h->ba.cam_slot, nci,
+                                                              h->core->incU, active);
+    else
+      oplus_cam_kernel<6><<<cdiv(nci, 128), 128, 0, h->st>>>(h->cam.as<double>(), h->ba.cam_slot, nci,
+                                                              h->core->incU, active);
+  }
+  if (h->desc.np_var > 0)
+    oplus_pt_kernel<<<cdiv(3LL * h->desc.np_var, 256), 256, 0, h->st>>>(h->pt.as<double>(), h->desc.np_var,
+                                                                         h->core->incV, active);
+  h->launches += 2;
+  NL_CUDA(cudaGetLastError());
+  return NL_OK;
+}
+
+nl_status enqueue_copy_params(nl_problem* h, bool to_backup, const int* flag) {
+  const size_t nc = (size_t)h->nc_all() * 16, np = (size_t)h->np_all() * 3;
+  double* c_dst = to_backup ? h->cam_bck.as<double>() : h->cam.as<double>();
+  const double* c_src = to_backup ? h->cam.as<double>() : h->cam_bck.as<double>();
+  double* p_dst = to_backup ? h->pt_bck.as<double>() : h->pt.as<double>();
+  const double* p_src = to_backup ? h->pt.as<double>() : h->pt_bck.as<double>();
+  copy_if_kernel<<<std::max(1, std::min(296, cdiv(nc, 256))), 256, 0, h->st>>>(c_dst, c_src, nc, flag);
+  copy_if_kernel<<<std::max(1, std::min(296, cdiv(np, 256))), 256, 0, h->st>>>(p_dst, p_src, np, flag);
+  h->launches += 2;
+  NL_CUDA(cudaGetLastError());
+  return NL_OK;
+}
+
+// One sub-iteration of LM / one iteration of GN (see lm_kernels.cuh).
+nl_status enqueue_subiteration(nl_problem* h, double* trace) {
+  LmDev* s = h->lm;
+  lm_begin_kernel<<<1, 1, 0, h->st>>>(s);
+  nl_status r = h->core->enqueue_increment(s->lam, &s->status, &s->active);
+  if (r != NL_OK) return r;
+  int nparts = 0;
+  if ((r = h->core->enqueue_inc_dot(s, h->d_part.as<double>() + 4096, &nparts)) != NL_OK) return r;
+  lm_inc_kernel<<<1, 1, 0, h->st>>>(s, h->d_part.as<double>() + 4096, nparts, trace);
+  if ((r = enqueue_oplus(h, &s->apply)) != NL_OK) return r;
+  if ((r = enqueue_eval(h, false, &s->chi2_new, nullptr, &s->apply)) != NL_OK) return r;
+  lm_decide_kernel<<<1, 1, 0, h->st>>>(s, trace);
+  if ((r = enqueue_copy_params(h, false, &s->rollback)) != NL_OK) return r;
+  // update(true) at the accepted point (GN: after every step), then backup
+  if ((r = enqueue_eval(h, true, h->scal, &s->maxAbsB, &s->do_jac)) != NL_OK) return r;
+  if ((r = enqueue_copy_params(h, true, &s->do_jac)) != NL_OK) return r;
+  lm_after_jac_kernel<<<1, 1, 0, h->st>>>(s, h->scal, trace);
+  h->launches += 4;
+  NL_CUDA(cudaGetLastError());
+  return NL_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+#define NL_CHECK_H(h)          \
+  do {                         \
+    if (!(h)) return NL_ERR_ARG; \
+  } while (0)
+#define NL_CHECK_READY(h)                    \
+  do {                                       \
+    if (!(h) || !(h)->ready) return NL_ERR_STATE; \
+  } while (0)
+
+namespace {
+
+nl_status sync_read(nl_problem* h, const double* dev, double* out, int n) {
+  NL_CUDA(cudaMemcpyAsync(h->host_pin, dev, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st));
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  for (int i = 0; i < n; i++) out[i] = h->host_pin[i];
+  return NL_OK;
+}
+
+nl_status upload_params(nl_problem* h) {
+  NL_CUDA(cudaMemcpyAsync(h->cam.p, h->cam_state.data(), h->cam_state.size() * sizeof(double),
+                          cudaMemcpyHostToDevice, h->st));
+  if (!h->pts.empty())
+    NL_CUDA(cudaMemcpyAsync(h->pt.p, h->pts.data(), h->pts.size() * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  return NL_OK;
+}
+
+// Solve driver shared by LM and GN (the host only relaunches the fixed
+// sub-iteration sequence and watches the `done` flag one launch behind).
+nl_status run_solver(nl_problem* h, LmDev& init, nl_solve_report* rep, double* trace, int trace_cap, int max_launch) {
+  // update(true) at the start (LevenbergMarquardt.hpp:41 / GaussNewton.hpp:40)
+  nl_status r = enqueue_eval(h, true, h->scal, h->scal + 1, nullptr);
+  if (r != NL_OK) return r;
+  double v[2];
+  if ((r = sync_read(h, h->scal, v, 2)) != NL_OK) return r;
+  init.chi2 = init.oldChi2 = v[0];
+  init.maxAbsB = v[1];
+  const int cap = std::max(0, trace_cap);
+  if (h->d_trace.bytes < sizeof(double) * NL_TRACE_STRIDE * (size_t)std::max(cap, 1))
+    if ((r = h->d_trace.alloc(sizeof(double) * NL_TRACE_STRIDE * (size_t)std::max(cap, 1))) != NL_OK) return r;
+  double* dtrace = cap > 0 ? h->d_trace.as<double>() : nullptr;
+  init.trace_cap = cap;
+  init.trace_n = 1;
+  double first[NL_TRACE_STRIDE] = {-1, init.gn ? 0.0 : -1.0, v[0], 0, 0, 0, 1, 1};
+  if (trace && cap > 0) memcpy(trace, first, sizeof(first));
+  if (v[1] <= init.epsBVector) {
+    if (rep) {
+      rep->reason = NL_SUCCESS_AT_START;
+      rep->iterations = -1;
+      rep->subiterations = 0;
+      rep->n_trace = cap > 0 ? 1 : 0;
+      rep->chi2 = v[0];
+      rep->mu = 0;
+    }
+    return NL_OK;
+  }
+  if ((r = enqueue_copy_params(h, true, nullptr)) != NL_OK) return r;  // backupSolution
+  if ((r = h->core->enqueue_hdiag(h->scal + 2)) != NL_OK) return r;
+  double hd;
+  if ((r = sync_read(h, h->scal + 2, &hd, 1)) != NL_OK) return r;
+  init.maxAbsHDiag = hd;
+  init.mu = init.tau * hd;  // LevenbergMarquardt.hpp:58
+  init.curV = init.initV;
+  init.iter = 0;
+  init.subiter = 0;
+  init.nsub = 0;
+  init.done = init.gn && init.maxNumIt <= 0 ? 1 : 0;
+  if (!init.gn && init.maxNumIt <= 0) init.done = 1;
+  init.reason = NL_MAX_ITERATION_REACHED;
+  NL_CUDA(cudaMemcpyAsync(h->lm, &init, sizeof(LmDev), cudaMemcpyHostToDevice, h->st));
+  // launch loop: watch `done` one launch behind
+  int* done_pin = reinterpret_cast<int*>(h->host_pin + 8);
+  done_pin[0] = done_pin[1] = init.done;
+  int launched = 0;
+  while (!init.done && launched < max_launch) {
+    if ((r = enqueue_subiteration(h, dtrace)) != NL_OK) return r;
+    NL_CUDA(cudaMemcpyAsync(done_pin + (launched & 1), &h->lm->done, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    NL_CUDA(cudaEventRecord(launched & 1 ? h->ev_b : h->ev_a, h->st));
+    if (launched > 0) {
+      cudaEvent_t prev = (launched & 1) ? h->ev_a : h->ev_b;
+      NL_CUDA(cudaEventSynchronize(prev));
+      if (done_pin[(launched - 1) & 1]) break;
+    }
+    launched++;
+  }
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  LmDev fin;
+  NL_CUDA(cudaMemcpy(&fin, h->lm, sizeof(LmDev), cudaMemcpyDeviceToHost));
+  const int nt = std::min(fin.trace_n, cap);
+  if (trace && nt > 1)
+    NL_CUDA(cudaMemcpy(trace + NL_TRACE_STRIDE, dtrace + NL_TRACE_STRIDE, sizeof(double) * NL_TRACE_STRIDE * (nt - 1),
+                       cudaMemcpyDeviceToHost));
+  if (rep) {
+    rep->reason = fin.done ? fin.reason : NL_MAX_ITERATION_REACHED;
+    rep->iterations = fin.iter;
+    rep->subiterations = fin.nsub;
+    rep->n_trace = nt;
+    rep->chi2 = fin.chi2;
+    rep->mu = fin.mu;
+  }
+  return NL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* nl_version(void) { return "nelson_b200 0.1 sm_100a"; }
+
+const char* nl_status_string(int s) {
+  switch (s) {
+    case NL_OK: return "ok";
+    case NL_ERR_ARG: return "bad argument";
+    case NL_ERR_STATE: return "call out of order";
+    case NL_ERR_CUDA: return "CUDA error";
+    case NL_ERR_UNSUPPORTED: return "unsupported structure";
+    case NL_ERR_NOT_SPD: return "not positive definite";
+    case NL_ERR_NONFINITE: return "non-finite value";
+    case NL_ERR_TIMEOUT: return "device wait timed out";
+    case NL_ERR_NOMEM: return "device allocation failed";
+    default: return "unknown status";
+  }
+}
+
+nl_status nl_create(const nl_problem_desc* d, nl_problem** out) {
+  if (!d || !out) return NL_ERR_ARG;
+  *out = nullptr;
+  if ((d->bc != 6 && d->bc != 9) || d->nc_var < 0 || d->nc_fix < 0 || d->np_var < 0 || d->np_fix < 0 ||
+      (d->precision != NL_PREC_FP64 && d->precision != NL_PREC_MIXED))
+    return NL_ERR_ARG;
+  std::unique_ptr<nl_problem> h(new nl_problem());
+  h->desc = *d;
+  h->device = d->device;
+  nl_status s;
+  if ((s = select_device(h.get())) != NL_OK) return s;
+  NL_CUDA(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+  NL_CUDA(cudaEventCreateWithFlags(&h->ev_a, cudaEventDisableTiming));
+  NL_CUDA(cudaEventCreateWithFlags(&h->ev_b, cudaEventDisableTiming));
+  if (d->precision == NL_PREC_FP64) {
+    if (cublasCreate(&h->cublas) != CUBLAS_STATUS_SUCCESS) return NL_ERR_CUDA;
+    cublasSetStream(h->cublas, h->st);
+    if ((s = h->cublas_ws.alloc(64u << 20)) != NL_OK) return s;
+    cublasSetWorkspace(h->cublas, h->cublas_ws.p, h->cublas_ws.bytes);
+  }
+  h->core = make_schur_core(d->precision, d->bc, h->cublas);
+  if (!h->core) return NL_ERR_UNSUPPORTED;
+  h->core->refine_sweeps = d->refine_sweeps >= 0 ? d->refine_sweeps : (d->precision == NL_PREC_MIXED ? 2 : 0);
+  h->core->keep_schur = (long long)d->nc_var * d->bc <= 4096 ? 1 : 0;
+  h->core->use_tc = 0;
+  const int nc_all = d->nc_var + d->nc_fix, np_all = d->np_var + d->np_fix;
+  h->cam_state.assign((size_t)nc_all * 16, 0.0);
+  h->pts.assign((size_t)np_all * 3, 0.0);
+  for (int c = 0; c < nc_all; c++) {
+    double* st = h->cam_state.data() + (size_t)c * 16;
+    st[0] = st[4] = st[8] = 1.0;
+    st[11] = 1.0;
+    st[12] = d->f;
+  }
+  h->perm.resize(d->nc_var);
+  std::iota(h->perm.begin(), h->perm.end(), 0);
+  if ((s = h->cam.alloc(sizeof(double) * std::max<size_t>(h->cam_state.size(), 16))) != NL_OK) return s;
+  if ((s = h->cam_bck.alloc(h->cam.bytes)) != NL_OK) return s;
+  if ((s = h->pt.alloc(sizeof(double) * std::max<size_t>(h->pts.size(), 3))) != NL_OK) return s;
+  if ((s = h->pt_bck.alloc(h->pt.bytes)) != NL_OK) return s;
+  if ((s = h->d_part.alloc(sizeof(double) * 8192)) != NL_OK) return s;
+  if ((s = h->d_scal.alloc(sizeof(double) * 16)) != NL_OK) return s;
+  if ((s = h->d_lm.alloc(sizeof(LmDev))) != NL_OK) return s;
+  if ((s = h->d_lam.alloc(sizeof(double) * 2 + sizeof(int) * 2)) != NL_OK) return s;
+  NL_CUDA(cudaMemsetAsync(h->d_scal.p, 0, h->d_scal.bytes, h->st));
+  NL_CUDA(cudaMemsetAsync(h->d_lm.p, 0, h->d_lm.bytes, h->st));
+  h->scal = h->d_scal.as<double>();
+  h->lm = h->d_lm.as<LmDev>();
+  h->status = reinterpret_cast<int*>(h->d_lam.as<double>() + 2);
+  NL_CUDA(cudaMallocHost(&h->host_pin, 4096));
+  if ((s = upload_params(h.get())) != NL_OK) return s;
+  *out = h.release();
+  return NL_OK;
+}
+
+nl_status nl_destroy(nl_problem* h) {
+  if (!h) return NL_ERR_ARG;
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->st);
+  delete h;
+  return NL_OK;
+}
+
+nl_status nl_set_params(nl_problem* h, const double* cams, const double* pts) {
+  NL_CHECK_H(h);
+  const int bc = h->desc.bc;
+  if (cams) {
+    for (int c = 0; c < h->nc_all(); c++) {
+      const double* in = cams + (size_t)c * bc;
+      double* st = h->cam_state.data() + (size_t)c * 16;
+      so3_exp_host(in, st);
+      st[9] = in[3];
+      st[10] = in[4];
+      st[11] = in[5];
+      if (bc == 9) {
+        st[12] = in[6];
+        st[13] = in[7];
+        st[14] = in[8];
+      } else {
+        st[12] = h->desc.f;
+        st[13] = 0;
+        st[14] = 0;
+      }
+      st[15] = 0;
+    }
+  }
+  if (pts) memcpy(h->pts.data(), pts, h->pts.size() * sizeof(double));
+  NL_CUDA(cudaSetDevice(h->device));
+  return upload_params(h);
+}
+
+nl_status nl_get_camera_state(nl_problem* h, double* states) {
+  NL_CHECK_H(h);
+  NL_CUDA(cudaSetDevice(h->device));
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  NL_CUDA(cudaMemcpy(states, h->cam.p, sizeof(double) * h->cam_state.size(), cudaMemcpyDeviceToHost));
+  return NL_OK;
+}
+
+nl_status nl_get_params(nl_problem* h, double* cams, double* pts) {
+  NL_CHECK_H(h);
+  NL_CUDA(cudaSetDevice(h->device));
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  std::vector<double> st(h->cam_state.size());
+  NL_CUDA(cudaMemcpy(st.data(), h->cam.p, sizeof(double) * st.size(), cudaMemcpyDeviceToHost));
+  const int bc = h->desc.bc;
+  if (cams)
+    for (int c = 0; c < h->nc_all(); c++) {
+      const double* s = st.data() + (size_t)c * 16;
+      double* o = cams + (size_t)c * bc;
+      so3_log_host(s, o);
+      o[3] = s[9];
+      o[4] = s[10];
+      o[5] = s[11];
+      if (bc == 9) {
+        o[6] = s[12];
+        o[7] = s[13];
+        o[8] = s[14];
+      }
+    }
+  if (pts) NL_CUDA(cudaMemcpy(pts, h->pt.p, sizeof(double) * h->pts.size(), cudaMemcpyDeviceToHost));
+  return NL_OK;
+}
+
+nl_status nl_add_ba_edges(nl_problem* h, int ne, const int* cam, const int* cam_fixed, const int* pt,
+                          const int* pt_fixed, const double* obs, const double* weight) {
+  NL_CHECK_H(h);
+  if (h->ready) return NL_ERR_STATE;
+  if (ne < 0 || (ne > 0 && (!cam || !pt || !obs))) return NL_ERR_ARG;
+  for (int e = 0; e < ne; e++) {
+    const int cf = cam_fixed ? (cam_fixed[e] != 0) : 0, pf = pt_fixed ? (pt_fixed[e] != 0) : 0;
+    const int lc = cf ? h->desc.nc_fix : h->desc.nc_var, lp = pf ? h->desc.np_fix : h->desc.np_var;
+    if (cam[e] < 0 || cam[e] >= lc || pt[e] < 0 || pt[e] >= lp) return NL_ERR_ARG;
+    if (weight && !(weight[e] >= 0.0)) return NL_ERR_ARG;
+  }
+  for (int e = 0; e < ne; e++) {
+    h->e_cam.push_back(cam[e]);
+    h->e_camfix.push_back(cam_fixed ? (cam_fixed[e] != 0) : 0);
+    h->e_pt.push_back(pt[e]);
+    h->e_ptfix.push_back(pt_fixed ? (pt_fixed[e] != 0) : 0);
+    h->e_obs.push_back(obs[2 * (size_t)e]);
+    h->e_obs.push_back(obs[2 * (size_t)e + 1]);
+    h->e_w.push_back(weight ? weight[e] : 1.0);
+  }
+  return NL_OK;
+}
+
+nl_status nl_set_user2internal_u(nl_problem* h, const int* perm) {
+  NL_CHECK_H(h);
+  if (h->ready) return NL_ERR_STATE;
+  if (!perm) return NL_ERR_ARG;
+  std::vector<int> seen(h->desc.nc_var, 0);
+  for (int i = 0; i < h->desc.nc_var; i++) {
+    if (perm[i] < 0 || perm[i] >= h->desc.nc_var || seen[perm[i]]) return NL_ERR_ARG;
+    seen[perm[i]] = 1;
+  }
+  memcpy(h->perm.data(), perm, sizeof(int) * h->desc.nc_var);
+  return NL_OK;
+}
+
+nl_status nl_structure_ready(nl_problem* h) {
+  NL_CHECK_H(h);
+  if (h->ready) return NL_ERR_STATE;
+  NL_CUDA(cudaSetDevice(h->device));
+  nl_status s = build_structure(h);
+  if (s != NL_OK) return s;
+  h->ready = true;
+  return NL_OK;
+}
+
+nl_status nl_set_observations(nl_problem* h, const double* obs, const double* weight) {
+  NL_CHECK_READY(h);
+  const size_t ne = h->e_cam.size();
+  if (obs) memcpy(h->e_obs.data(), obs, sizeof(double) * 2 * ne);
+  if (weight) memcpy(h->e_w.data(), weight, sizeof(double) * ne);
+  std::vector<double> eobs(2 * ne), ew(ne), pobs(2 * h->porder.size()), pw(h->porder.size());
+  for (size_t t = 0; t < ne; t++) {
+    const int e = h->eorder[t];
+    eobs[2 * t] = h->e_obs[2 * (size_t)e];
+    eobs[2 * t + 1] = h->e_obs[2 * (size_t)e + 1];
+    ew[t] = h->e_w[e];
+  }
+  for (size_t t = 0; t < h->porder.size(); t++) {
+    const int e = h->porder[t];
+    pobs[2 * t] = h->e_obs[2 * (size_t)e];
+    pobs[2 * t + 1] = h->e_obs[2 * (size_t)e + 1];
+    pw[t] = h->e_w[e];
+  }
+  NL_CUDA(cudaSetDevice(h->device));
+  NL_CUDA(cudaMemcpyAsync(h->d_e_obs.p, eobs.data(), eobs.size() * 8, cudaMemcpyHostToDevice, h->st));
+  NL_CUDA(cudaMemcpyAsync(h->d_e_w.p, ew.data(), ew.size() * 8, cudaMemcpyHostToDevice, h->st));
+  if (!pobs.empty()) {
+    NL_CUDA(cudaMemcpyAsync(h->d_p_obs.p, pobs.data(), pobs.size() * 8, cudaMemcpyHostToDevice, h->st));
+    NL_CUDA(cudaMemcpyAsync(h->d_p_w.p, pw.data(), pw.size() * 8, cudaMemcpyHostToDevice, h->st));
+  }
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  return NL_OK;
+}
+
+nl_status nl_get_counts(nl_problem* h, int* counts) {
+  NL_CHECK_READY(h);
+  counts[0] = h->nU;
+  counts[1] = h->nV;
+  counts[2] = h->nW;
+  counts[3] = (int)h->e_cam.size();
+  return NL_OK;
+}
+
+nl_status nl_get_patterns(nl_problem* h, int* u_rc, int* v_rc, int* w_rc) {
+  NL_CHECK_READY(h);
+  if (u_rc) memcpy(u_rc, h->u_rc.data(), sizeof(int) * h->u_rc.size());
+  if (v_rc) memcpy(v_rc, h->v_rc.data(), sizeof(int) * h->v_rc.size());
+  if (w_rc) memcpy(w_rc, h->w_rc.data(), sizeof(int) * h->w_rc.size());
+  return NL_OK;
+}
+
+nl_status nl_get_edge_uids(nl_problem* h, int* h11, int* h12, int* h22) {
+  NL_CHECK_READY(h);
+  if (h11) memcpy(h11, h->h11.data(), sizeof(int) * h->h11.size());
+  if (h12) memcpy(h12, h->h12.data(), sizeof(int) * h->h12.size());
+  if (h22) memcpy(h22, h->h22.data(), sizeof(int) * h->h22.size());
+  return NL_OK;
+}
+
+nl_status nl_update(nl_problem* h, int hessian, double* chi2) {
+  NL_CHECK_READY(h);
+  NL_CUDA(cudaSetDevice(h->device));
+  NL_CUDA(cudaEventRecord(h->ev_a, h->st));
+  nl_status s = enqueue_eval(h, hessian != 0, h->scal, h->scal + 1, nullptr);
+  if (s != NL_OK) return s;
+  double v;
+  if ((s = sync_read(h, h->scal, &v, 1)) != NL_OK) return s;
+  if (chi2) *chi2 = v;
+  return NL_OK;
+}
+
+nl_status nl_get_hessian(nl_problem* h, double* U, double* V, double* W, double* bU, double* bV) {
+  NL_CHECK_READY(h);
+  NL_CUDA(cudaSetDevice(h->device));
+  return h->core->get_hessian(U, V, W, bU, bV);
+}
+
+nl_status nl_solver_init(nl_problem* h) {
+  NL_CHECK_READY(h);
+  return NL_OK;
+}
+
+nl_status nl_max_abs_hdiag(nl_problem* h, double* out) {
+  NL_CHECK_READY(h);
+  NL_CUDA(cudaSetDevice(h->device));
+  nl_status s = h->core->enqueue_hdiag(h->scal + 2);
+  if (s != NL_OK) return s;
+  return sync_read(h, h->scal + 2, out, 1);
+}
+
+nl_status nl_compute_increment(nl_problem* h, double rel, double abs_, int* ok) {
+  NL_CHECK_READY(h);
+  NL_CUDA(cudaSetDevice(h->device));
+  double lam[2] = {rel, abs_};
+  memcpy(h->host_pin + 16, lam, sizeof(lam));
+  NL_CUDA(cudaMemcpyAsync(h->d_lam.p, h->host_pin + 16, sizeof(lam), cudaMemcpyHostToDevice, h->st));
+  NL_CUDA(cudaMemsetAsync(h->status, 0, sizeof(int), h->st));
+  h->core->timing = 1;
+  nl_status s = h->core->enqueue_increment(h->d_lam.as<double>(), h->status, nullptr);
+  h->core->timing = 0;
+  if (s != NL_OK) return s;
+  int st = 0;
+  NL_CUDA(cudaMemcpyAsync(h->host_pin + 20, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  memcpy(&st, h->host_pin + 20, sizeof(int));
+  if (ok) *ok = st == 0 ? 1 : 0;
+  if (st & ST_SPIN_TIMEOUT) return NL_ERR_TIMEOUT;
+  return NL_OK;
+}
+
+nl_status nl_get_increment(nl_problem* h, double* incU, double* incV) {
+  NL_CHECK_READY(h);
+  NL_CUDA(cudaSetDevice(h->device));
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  if (incU) NL_CUDA(cudaMemcpy(incU, h->core->incU, sizeof(double) * h->core->n(), cudaMemcpyDeviceToHost));
+  if (incV) NL_CUDA(cudaMemcpy(incV, h->core->incV, sizeof(double) * 3 * (size_t)h->desc.np_var, cudaMemcpyDeviceToHost));
+  return NL_OK;
+}
+
+nl_status nl_inc_sqnorm(nl_problem* h, double* out) {
+  NL_CHECK_READY(h);
+  std::vector<double> u(h->core->n()), v(3 * (size_t)h->desc.np_var);
+  nl_status s = nl_get_increment(h, u.data(), v.data());
+  if (s != NL_OK) return s;
+  double a = 0;
+  for (double x : u) a += x * x;
+  for (double x : v) a += x * x;
+  *out = a;
+  return NL_OK;
+}
+
+nl_status nl_get_schur(nl_problem* h, double* S, double* bS, int* n) {
+  NL_CHECK_READY(h);
+  if (n) *n = h->core->n();
+  if (!S && !bS) return NL_OK;
+  NL_CUDA(cudaSetDevice(h->device));
+  return h->core->get_schur(S, bS);
+}
+
+nl_status nl_oplus(nl_problem* h) {
+  NL_CHECK_READY(h);
+  NL_CUDA(cudaSetDevice(h->device));
+  nl_status s = enqueue_oplus(h, nullptr);
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  return s;
+}
+
+nl_status nl_backup(nl_problem* h) {
+  NL_CHECK_READY(h);
+  NL_CUDA(cudaSetDevice(h->device));
+  nl_status s = enqueue_copy_params(h, true, nullptr);
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  return s;
+}
+
+nl_status nl_rollback(nl_problem* h) {
+  NL_CHECK_READY(h);
+  NL_CUDA(cudaSetDevice(h->device));
+  nl_status s = enqueue_copy_params(h, false, nullptr);
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  return s;
+}
+
+nl_status nl_max_abs_b(nl_problem* h, double* out) {
+  NL_CHECK_READY(h);
+  NL_CUDA(cudaSetDevice(h->device));
+  return sync_read(h, h->scal + 1, out, 1);
+}
+
+nl_status nl_chi2(nl_problem* h, double* out) {
+  NL_CHECK_READY(h);
+  NL_CUDA(cudaSetDevice(h->device));
+  return sync_read(h, h->scal, out, 1);
+}
+
+nl_status nl_rho(nl_problem* h, double mu, double old_chi2, double* out) {
+  NL_CHECK_READY(h);
+  const int n = h->core->n(), nv = 3 * h->desc.np_var;
+  std::vector<double> u(n), v(nv), bu(n), bv(nv);
+  nl_status s = nl_get_increment(h, u.data(), v.data());
+  if (s != NL_OK) return s;
+  if ((s = h->core->get_hessian(nullptr, nullptr, nullptr, bu.data(), bv.data())) != NL_OK) return s;
+  double chi2;
+  if ((s = nl_chi2(h, &chi2)) != NL_OK) return s;
+  double den = 0;
+  for (int i = 0; i < n; i++) den += u[i] * (mu * u[i] - bu[i]);
+  for (int i = 0; i < nv; i++) den += v[i] * (mu * v[i] - bv[i]);
+  *out = (old_chi2 - chi2) / den;
+  return NL_OK;
+}
+
+nl_status nl_lm_solve(nl_problem* h, const nl_lm_settings* st, nl_solve_report* rep, double* trace, int trace_cap) {
+  NL_CHECK_READY(h);
+  if (!st) return NL_ERR_ARG;
+  NL_CUDA(cudaSetDevice(h->device));
+  LmDev s{};
+  s.gn = 0;
+  s.maxNumIt = st->maxNumIt;
+  s.maxNumSubIt = st->maxNumSubIt;
+  s.minNumIt = st->minNumIt;
+  s.epsBVector = st->epsBVector;
+  s.epsIncSquare = st->epsIncSquare;
+  s.epsChi2 = st->epsChi2;
+  s.tau = st->tau;
+  s.penaltyV = st->penaltyV;
+  s.initV = st->initV;
+  s.maxScale = st->maxScaleFactor;
+  s.minScale = st->minScaleFactor;
+  const long long lim = (long long)std::max(st->maxNumIt, 0) * std::max(st->maxNumSubIt, 1) + 2;
+  return run_solver(h, s, rep, trace, trace_cap, (int)std::min<long long>(lim, 1 << 30));
+}
+
+nl_status nl_gn_solve(nl_problem* h, const nl_gn_settings* st, nl_solve_report* rep, double* trace, int trace_cap) {
+  NL_CHECK_READY(h);
+  if (!st) return NL_ERR_ARG;
+  NL_CUDA(cudaSetDevice(h->device));
+  LmDev s{};
+  s.gn = 1;
+  s.maxNumIt = st->maxNumIt;
+  s.maxNumSubIt = 1 << 30;
+  s.minNumIt = st->minNumIt;
+  s.epsBVector = st->epsBVector;
+  s.epsIncSquare = st->epsIncSquare;
+  s.epsChi2 = st->epsChi2;
+  s.gnRel = st->relLambda;
+  s.gnAbs = st->absLambda;
+  s.tau = 0;
+  s.initV = 1;
+  s.penaltyV = 1;
+  return run_solver(h, s, rep, trace, trace_cap, std::max(st->maxNumIt, 0) + 2);
+}
+
+nl_status nl_phase_timings(nl_problem* h, nl_phase_times* out) {
+  NL_CHECK_READY(h);
+  *out = h->core->times;
+  out->eval_ms = h->eval_ms;
+  return NL_OK;
+}
+
+nl_status nl_kernel_launches(nl_problem* h, long long* out) {
+  NL_CHECK_H(h);
+  *out = h->launches + (h->core ? h->core->launches : 0);
+  return NL_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Solver-only drop-in: SolverCholeskySchur on a caller-assembled Hessian.
+struct nl_solver {
+  nl_solver_desc d{};
+  cudaStream_t st = nullptr;
+  cublasHandle_t cublas = nullptr;
+  DevBuf ws, lam;
+  std::unique_ptr<SchurCore> core;
+  double* pin = nullptr;
+  ~nl_solver() {
+    core.reset();
+    if (cublas) cublasDestroy(cublas);
+    if (pin) cudaFreeHost(pin);
+    if (st) cudaStreamDestroy(st);
+  }
+};
+
+extern "C" {
+
+nl_status nl_solver_create(const nl_solver_desc* d, const int* u_rc, const int* v_rc, const int* w_rc,
+                           nl_solver** out) {
+  if (!d || !out || d->bu < 1 || d->bu > 9 || d->nu < 0 || d->nv < 0 || d->nU < 0 || d->nV < 0 || d->nW < 0)
+    return NL_ERR_ARG;
+  if ((d->nU > 0 && !u_rc) || (d->nV > 0 && !v_rc) || (d->nW > 0 && !w_rc)) return NL_ERR_ARG;
+  *out = nullptr;
+  std::unique_ptr<nl_solver> s(new nl_solver());
+  s->d = *d;
+  NL_CUDA(cudaSetDevice(d->device));
+  NL_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  if (d->precision == NL_PREC_FP64) {
+    if (cublasCreate(&s->cublas) != CUBLAS_STATUS_SUCCESS) return NL_ERR_CUDA;
+    cublasSetStream(s->cublas, s->st);
+    nl_status r = s->ws.alloc(64u << 20);
+    if (r != NL_OK) return r;
+    cublasSetWorkspace(s->cublas, s->ws.p, s->ws.bytes);
+  }
+  s->core = make_schur_core(d->precision, d->bu, s->cublas);
+  if (!s->core) return NL_ERR_UNSUPPORTED;
+  s->core->refine_sweeps = d->refine_sweeps >= 0 ? d->refine_sweeps : (d->precision == NL_PREC_MIXED ? 2 : 0);
+  s->core->keep_schur = 0;
+  s->core->use_tc = 0;
+  SchurStructure ss;
+  ss.bc = d->bu;
+  ss.nci = d->nu;
+  ss.np = d->nv;
+  for (int q = 0; q < d->nU; q++) {
+    ss.u_r.push_back(u_rc[2 * q]);
+    ss.u_c.push_back(u_rc[2 * q + 1]);
+    if (q > 0) {  // CSC order of the upper pattern
+      const int pc = u_rc[2 * q - 1], pr = u_rc[2 * q - 2];
+      if (u_rc[2 * q + 1] < pc || (u_rc[2 * q + 1] == pc && u_rc[2 * q] <= pr)) return NL_ERR_ARG;
+    }
+  }
+  ss.v_uid.assign(d->nv, -1);
+  for (int q = 0; q < d->nV; q++) {
+    const int r = v_rc[2 * q], c = v_rc[2 * q + 1];
+    if (r != c) return NL_ERR_UNSUPPORTED;  // V must be block diagonal (MatrixDiagInv)
+    if (c < 0 || c >= d->nv || ss.v_uid[c] >= 0) return NL_ERR_ARG;
+    ss.v_uid[c] = q;
+  }
+  for (int q = 0; q < d->nW; q++) {
+    ss.w_r.push_back(w_rc[2 * q]);
+    ss.w_c.push_back(w_rc[2 * q + 1]);
+  }
+  nl_status r = s->core->setup(ss, s->st);
+  if (r != NL_OK) return r;
+  if ((r = s->lam.alloc(64)) != NL_OK) return r;
+  NL_CUDA(cudaMallocHost(&s->pin, 256));
+  NL_CUDA(cudaStreamSynchronize(s->st));
+  *out = s.release();
+  return NL_OK;
+}
+
+nl_status nl_solver_destroy(nl_solver* s) {
+  if (!s) return NL_ERR_ARG;
+  cudaSetDevice(s->d.device);
+  cudaStreamSynchronize(s->st);
+  delete s;
+  return NL_OK;
+}
+
+nl_status nl_solver_set_hessian(nl_solver* s, const double* U, const double* V, const double* W, const double* bU,
+                                const double* bV) {
+  if (!s) return NL_ERR_ARG;
+  NL_CUDA(cudaSetDevice(s->d.device));
+  return s->core->set_hessian(U, V, W, bU, bV);
+}
+
+nl_status nl_solver_max_abs_hdiag(nl_solver* s, double* out) {
+  if (!s || !out) return NL_ERR_ARG;
+  NL_CUDA(cudaSetDevice(s->d.device));
+  double* dv = s->lam.as<double>() + 4;
+  nl_status r = s->core->enqueue_hdiag(dv);
+  if (r != NL_OK) return r;
+  NL_CUDA(cudaMemcpyAsync(s->pin, dv, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  NL_CUDA(cudaStreamSynchronize(s->st));
+  *out = s->pin[0];
+  return NL_OK;
+}
+
+nl_status nl_solver_compute_increment(nl_solver* s, double rel, double abs_, double* incU, double* incV, int* ok) {
+  if (!s) return NL_ERR_ARG;
+  NL_CUDA(cudaSetDevice(s->d.device));
+  s->pin[0] = rel;
+  s->pin[1] = abs_;
+  NL_CUDA(cudaMemcpyAsync(s->lam.p, s->pin, 2 * sizeof(double), cudaMemcpyHostToDevice, s->st));
+  int* status = reinterpret_cast<int*>(s->lam.as<double>() + 2);
+  NL_CUDA(cudaMemsetAsync(status, 0, sizeof(int), s->st));
+  nl_status r = s->core->enqueue_increment(s->lam.as<double>(), status, nullptr);
+  if (r != NL_OK) return r;
+  NL_CUDA(cudaMemcpyAsync(s->pin + 4, status, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+  if (incU) NL_CUDA(cudaMemcpyAsync(incU, s->core->incU, sizeof(double) * s->core->n(), cudaMemcpyDeviceToHost, s->st));
+  if (incV) NL_CUDA(cudaMemcpyAsync(incV, s->core->incV, sizeof(double) * 3 * (size_t)s->d.nv, cudaMemcpyDeviceToHost, s->st));
+  NL_CUDA(cudaStreamSynchronize(s->st));
+  int st;
+  memcpy(&st, s->pin + 4, sizeof(int));
+  if (ok) *ok = st == 0 ? 1 : 0;
+  if (st & ST_SPIN_TIMEOUT) return NL_ERR_TIMEOUT;
+  return NL_OK;
+}
+
+}  // extern "C"

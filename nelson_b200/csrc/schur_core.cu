@@ -1,0 +1,405 @@
+// schur_core.cu -- SolverCholeskySchur on the device (see schur_core.cuh).
+#include <cstring>
+
+#include "schur_core.cuh"
+
+namespace nl {
+
+namespace {
+
+constexpr int kNT = 256;
+constexpr int kRedCTAs = 296;  // 2 x 148 SMs for grid-stride reductions
+constexpr int kSymvChunks = 4;
+constexpr int kSchurWarps = 8;
+
+inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+template <typename T, int BC>
+class SchurCoreT final : public SchurCore {
+ public:
+  explicit SchurCoreT(cublasHandle_t cb, int precision) : cublas_(cb), precision_(precision) {}
+
+  int n() const override { return n_; }
+  int ld() const override { return ld_; }
+  void* dU() override { return U_.p; }
+  void* dV() override { return V_.p; }
+  void* dW() override { return W_.p; }
+  void* dbU() override { return bU_.p; }
+  void* dbV() override { return bV_.p; }
+
+  nl_status setup(const SchurStructure& st, cudaStream_t stream) override {
+    st_ = stream;
+    nci_ = st.nci;
+    np_ = st.np;
+    nU_ = (int)st.u_r.size();
+    nW_ = (int)st.w_r.size();
+    nV_ = 0;
+    for (int q : st.v_uid) nV_ = std::max(nV_, q + 1);
+    n_ = nci_ * BC;
+    ld_ = std::max(NB, cdiv(n_, NB) * NB);
+    ntiles_ = ld_ / NB;
+    // ---- derived host structure ----
+    std::vector<int> w_row_ptr(nci_ + 1, 0), w_col_ptr(np_ + 1, 0), w_col_uid(nW_);
+    for (int q = 0; q < nW_; q++) {
+      if (st.w_r[q] < 0 || st.w_r[q] >= nci_ || st.w_c[q] < 0 || st.w_c[q] >= np_) return NL_ERR_ARG;
+      if (q > 0 && (st.w_r[q] < st.w_r[q - 1] || (st.w_r[q] == st.w_r[q - 1] && st.w_c[q] <= st.w_c[q - 1])))
+        return NL_ERR_ARG;  // W UIDs must follow CSR order
+      w_row_ptr[st.w_r[q] + 1]++;
+      w_col_ptr[st.w_c[q] + 1]++;
+    }
+    for (int i = 0; i < nci_; i++) w_row_ptr[i + 1] += w_row_ptr[i];
+    for (int j = 0; j < np_; j++) w_col_ptr[j + 1] += w_col_ptr[j];
+    {
+      std::vector<int> fill(w_col_ptr.begin(), w_col_ptr.end() - 1);
+      for (int q = 0; q < nW_; q++) w_col_uid[fill[st.w_c[q]]++] = q;
+    }
+    std::vector<int> u_diag(nci_, -1);
+    for (int q = 0; q < nU_; q++) {
+      if (st.u_r[q] > st.u_c[q] || st.u_c[q] >= nci_) return NL_ERR_ARG;
+      if (st.u_r[q] == st.u_c[q]) u_diag[st.u_r[q]] = q;
+    }
+    // ---- output blocks of S: U pattern + W W' pattern + every diagonal ----
+    if ((long long)nci_ * nci_ > (1LL << 28)) return NL_ERR_UNSUPPORTED;  // dense S too large anyway
+    std::vector<int> bmap((size_t)nci_ * nci_, 0);       // pair counts, then block ids
+    std::vector<long long> cnt;
+    for (int i = 0; i < nci_; i++) bmap[(size_t)i * nci_ + i] = 1;  // mark
+    for (int q = 0; q < nU_; q++) bmap[(size_t)st.u_r[q] * nci_ + st.u_c[q]] = 1;
+    long long npairs = 0;
+    std::vector<int> pc((size_t)nci_ * nci_, 0);
+    for (int p = 0; p < np_; p++) {
+      for (int s = w_col_ptr[p]; s < w_col_ptr[p + 1]; s++)
+        for (int t = s; t < w_col_ptr[p + 1]; t++) {
+          const int i = st.w_r[w_col_uid[s]], j = st.w_r[w_col_uid[t]];
+          bmap[(size_t)i * nci_ + j] = 1;
+          pc[(size_t)i * nci_ + j]++;
+          npairs++;
+        }
+    }
+    std::vector<int> s_i, s_j, s_uuid;
+    std::vector<long long> s_ptr(1, 0);
+    std::vector<int> bid((size_t)nci_ * nci_, -1);
+    for (int i = 0; i < nci_; i++)
+      for (int j = i; j < nci_; j++)
+        if (bmap[(size_t)i * nci_ + j]) {
+          bid[(size_t)i * nci_ + j] = (int)s_i.size();
+          s_i.push_back(i);
+          s_j.push_back(j);
+          s_uuid.push_back(-1);
+          s_ptr.push_back(s_ptr.back() + pc[(size_t)i * nci_ + j]);
+        }
+    for (int q = 0; q < nU_; q++) s_uuid[bid[(size_t)st.u_r[q] * nci_ + st.u_c[q]]] = q;
+    nS_ = (int)s_i.size();
+    std::vector<int> pa(std::max<long long>(npairs, 1)), pb(std::max<long long>(npairs, 1));
+    {
+      std::vector<long long> fill(s_ptr.begin(), s_ptr.end() - 1);
+      for (int p = 0; p < np_; p++)  // points ascending: the merge order of MatrixWWtMultiplier
+        for (int s = w_col_ptr[p]; s < w_col_ptr[p + 1]; s++)
+          for (int t = s; t < w_col_ptr[p + 1]; t++) {
+            const int a = w_col_uid[s], b = w_col_uid[t];
+            const long long slot = fill[bid[(size_t)st.w_r[a] * nci_ + st.w_r[b]]]++;
+            pa[slot] = a;
+            pb[slot] = b;
+          }
+    }
+    npairs_ = npairs;
+    // ---- device allocations ----
+    nl_status s;
+#define NL_TRY(x)           \
+  do {                      \
+    if ((s = (x)) != NL_OK) \
+      return s;             \
+  } while (0)
+    NL_TRY(U_.alloc(sizeof(T) * (size_t)std::max(nU_, 1) * Layout<T, BC>::U));
+    NL_TRY(V_.alloc(sizeof(T) * (size_t)std::max(nV_, 1) * Layout<T, BC>::V));
+    NL_TRY(W_.alloc(sizeof(T) * (size_t)std::max(nW_, 1) * Layout<T, BC>::W));
+    NL_TRY(Y_.alloc(sizeof(T) * (size_t)std::max(nW_, 1) * Layout<T, BC>::W));
+    NL_TRY(Vinv_.alloc(sizeof(T) * (size_t)std::max(np_, 1) * Layout<T, BC>::V));
+    NL_TRY(bU_.alloc(sizeof(T) * (size_t)ld_));
+    NL_TRY(bV_.alloc(sizeof(T) * (size_t)std::max(3 * np_, 1)));
+    NL_TRY(bS_.alloc(sizeof(double) * (size_t)ld_));
+    NL_TRY(incU_.alloc(sizeof(double) * (size_t)ld_));
+    NL_TRY(incV_.alloc(sizeof(double) * (size_t)std::max(3 * np_, 1)));
+    NL_TRY(y_.alloc(sizeof(double) * (size_t)ld_));
+    NL_TRY(r_.alloc(sizeof(double) * (size_t)ld_));
+    NL_TRY(dx_.alloc(sizeof(double) * (size_t)ld_));
+    NL_TRY(part_.alloc(sizeof(double) * (size_t)std::max(kSymvChunks * ld_, 4 * kRedCTAs)));
+    NL_TRY(Linv_.alloc(sizeof(double) * (size_t)ntiles_ * NB * NB));
+    NL_TRY(flags_.alloc(sizeof(int) * (size_t)(ntiles_ + 1)));
+    NL_TRY(S_.alloc(sizeof(T) * (size_t)ld_ * ld_));
+    need_s0_ = refine_sweeps > 0 || keep_schur;
+    if (need_s0_) NL_TRY(S0_.alloc(sizeof(T) * (size_t)ld_ * ld_));
+    if (sizeof(T) == 4 && use_tc) NL_TRY(tcs_.alloc(tc_syrk_scratch_bytes(ld_)));
+    NL_TRY(upload(v_uid_, st.v_uid, st_));
+    NL_TRY(upload(w_row_ptr_, w_row_ptr, st_));
+    NL_TRY(upload(w_col_, st.w_c, st_));
+    NL_TRY(upload(w_row_, st.w_r, st_));
+    NL_TRY(upload(w_col_ptr_, w_col_ptr, st_));
+    NL_TRY(upload(w_col_uid_, w_col_uid, st_));
+    NL_TRY(upload(u_diag_, u_diag, st_));
+    NL_TRY(upload(s_i_, s_i, st_));
+    NL_TRY(upload(s_j_, s_j, st_));
+    NL_TRY(upload(s_uuid_, s_uuid, st_));
+    NL_TRY(upload(s_ptr_, s_ptr, st_));
+    NL_TRY(upload(pa_, pa, st_));
+    NL_TRY(upload(pb_, pb, st_));
+#undef NL_TRY
+    NL_CUDA(cudaMemsetAsync(U_.p, 0, U_.bytes, st_));
+    NL_CUDA(cudaMemsetAsync(V_.p, 0, V_.bytes, st_));
+    NL_CUDA(cudaMemsetAsync(W_.p, 0, W_.bytes, st_));
+    NL_CUDA(cudaMemsetAsync(bU_.p, 0, bU_.bytes, st_));
+    NL_CUDA(cudaMemsetAsync(bV_.p, 0, bV_.bytes, st_));
+    NL_CUDA(cudaMemsetAsync(bS_.p, 0, bS_.bytes, st_));
+    NL_CUDA(cudaMemsetAsync(incU_.p, 0, incU_.bytes, st_));
+    NL_CUDA(cudaMemsetAsync(incV_.p, 0, incV_.bytes, st_));
+    incU = incU_.as<double>();
+    incV = incV_.as<double>();
+    d_.bc = BC;
+    d_.nci = nci_;
+    d_.np = np_;
+    d_.nU = nU_;
+    d_.nW = nW_;
+    d_.nS = nS_;
+    d_.n = n_;
+    d_.ld = ld_;
+    d_.v_uid = v_uid_.as<int>();
+    d_.w_row_ptr = w_row_ptr_.as<int>();
+    d_.w_col = w_col_.as<int>();
+    d_.w_row = w_row_.as<int>();
+    d_.w_col_ptr = w_col_ptr_.as<int>();
+    d_.w_col_uid = w_col_uid_.as<int>();
+    d_.u_diag_uid = u_diag_.as<int>();
+    d_.s_i = s_i_.as<int>();
+    d_.s_j = s_j_.as<int>();
+    d_.s_uuid = s_uuid_.as<int>();
+    d_.s_pair_ptr = s_ptr_.as<long long>();
+    d_.pair_a = pa_.as<int>();
+    d_.pair_b = pb_.as<int>();
+    const int smem_potrf = NB * (NB + 1) * (int)sizeof(double);
+    NL_CUDA(cudaFuncSetAttribute(potrf_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_potrf));
+    const int smem_trsm = (NB * (NB + 1) + 32 * NB) * (int)sizeof(T);
+    NL_CUDA(cudaFuncSetAttribute(trsm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_trsm));
+    if (!ev_[0]) {
+      for (auto& e : ev_) NL_CUDA(cudaEventCreate(&e));
+    }
+    return NL_OK;
+  }
+
+  // ---- solves with the factor: x = S^-1 b (trsv fwd + bwd) ----
+  nl_status enqueue_solve(const double* b, double* x, int* status, const int* active) {
+    NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
+    trsv_fwd_kernel<T><<<ntiles_, 256, 0, st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<double>(), b, y_.as<double>(),
+                                                 flags_.as<int>(), flags_.as<int>() + 1, 1, status, active);
+    NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
+    trsv_bwd_kernel<T><<<ntiles_, 256, 0, st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<double>(), y_.as<double>(), x,
+                                                 flags_.as<int>(), flags_.as<int>() + 1, 1, status, active);
+    launches += 2;
+    return NL_OK;
+  }
+
+  nl_status enqueue_factor(int* status, const int* active) {
+    const int smem_potrf = NB * (NB + 1) * (int)sizeof(double);
+    const int smem_trsm = (NB * (NB + 1) + 32 * NB) * (int)sizeof(T);
+    for (int k = 0; k < ntiles_; k++) {
+      potrf_diag_kernel<T><<<1, 256, smem_potrf, st_>>>(S_.as<T>(), ld_, k, Linv_.as<double>(), status, active);
+      launches++;
+      const int below = ld_ - (k + 1) * NB;
+      if (below <= 0) break;
+      trsm_kernel<T><<<cdiv(below, 32), NB, smem_trsm, st_>>>(S_.as<T>(), ld_, k, below, Linv_.as<double>(), active);
+      launches++;
+      const int t0 = k + 1, nt = ntiles_ - t0;
+      if (sizeof(T) == 8 && precision_ == NL_PREC_FP64 && cublas_) {
+        // FP64 comparison path: cuBLAS DSYRK on the trailing matrix.  Row-major
+        // lower storage is column-major upper; the panel X (below x NB, row-major)
+        // is the column-major NB x below matrix A, and C -= A' A.
+        const double alpha = -1.0, beta = 1.0;
+        double* Sd = reinterpret_cast<double*>(S_.p);
+        const size_t r0 = (size_t)t0 * NB;
+        if (cublasDsyrk(cublas_, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, below, NB, &alpha, Sd + r0 * ld_ + (size_t)k * NB,
+                        ld_, &beta, Sd + r0 * ld_ + r0, ld_) != CUBLAS_STATUS_SUCCESS)
+          return NL_ERR_CUDA;
+      } else if (sizeof(T) == 4 && use_tc) {
+        NL_CUDA(tc_syrk_f32(reinterpret_cast<float*>(S_.p), ld_, k, t0, nt, tcs_.p, active, status, st_));
+        launches += 2;
+      } else {
+        syrk_cc_kernel<T><<<nt * (nt + 1) / 2, 256, 0, st_>>>(S_.as<T>(), ld_, k, t0, nt, active);
+        launches++;
+      }
+    }
+    return NL_OK;
+  }
+
+  nl_status enqueue_increment(const double* lam, int* status, const int* active) override {
+    const bool tm = timing && !active;
+    if (tm) NL_CUDA(cudaEventRecord(ev_[0], st_));
+    vinv_kernel<T, BC><<<cdiv(std::max(np_, 1), 128), 128, 0, st_>>>(d_, V_.as<T>(), Vinv_.as<T>(), lam, status, active);
+    if (tm) NL_CUDA(cudaEventRecord(ev_[1], st_));
+    if (nci_ > 0)
+      wvinv_bs_kernel<T, BC, 128><<<nci_, 128, 0, st_>>>(d_, W_.as<T>(), Vinv_.as<T>(), Y_.as<T>(), bU_.as<T>(),
+                                                         bV_.as<T>(), bS_.as<double>(), active);
+    if (tm) NL_CUDA(cudaEventRecord(ev_[2], st_));
+    NL_CUDA(cudaMemsetAsync(S_.p, 0, S_.bytes, st_));
+    if (need_s0_) NL_CUDA(cudaMemsetAsync(S0_.p, 0, S0_.bytes, st_));
+    {
+      const int grid = std::max(1, std::min(cdiv(nS_, kSchurWarps), 148 * 16));
+      schur_kernel<T, BC, kSchurWarps><<<grid, kSchurWarps * 32, 0, st_>>>(
+          d_, U_.as<T>(), Y_.as<T>(), W_.as<T>(), lam, S_.as<T>(), need_s0_ ? S0_.as<T>() : nullptr, active);
+      if (ld_ > n_)
+        pad_identity_kernel<T><<<cdiv(ld_ - n_, 128), 128, 0, st_>>>(S_.as<T>(), need_s0_ ? S0_.as<T>() : nullptr, n_,
+                                                                     ld_, active);
+    }
+    launches += 4;
+    if (tm) NL_CUDA(cudaEventRecord(ev_[3], st_));
+    nl_status s = enqueue_factor(status, active);
+    if (s != NL_OK) return s;
+    if (tm) NL_CUDA(cudaEventRecord(ev_[4], st_));
+    if ((s = enqueue_solve(bS_.as<double>(), incU, status, active)) != NL_OK) return s;
+    for (int it = 0; it < refine_sweeps && need_s0_; it++) {
+      symv_partial_kernel<T, kSymvChunks><<<dim3(ntiles_, kSymvChunks), NB, 0, st_>>>(
+          S0_.as<T>(), ld_, ld_, incU, part_.as<double>(), active);
+      resid_finalize_kernel<kSymvChunks><<<cdiv(ld_, 256), 256, 0, st_>>>(part_.as<double>(), bS_.as<double>(), ld_,
+                                                                          r_.as<double>(), active);
+      if ((s = enqueue_solve(r_.as<double>(), dx_.as<double>(), status, active)) != NL_OK) return s;
+      axpy_kernel<<<cdiv(ld_, 256), 256, 0, st_>>>(incU, dx_.as<double>(), ld_, active);
+      launches += 3;
+    }
+    if (tm) NL_CUDA(cudaEventRecord(ev_[5], st_));
+    zero_if_failed_kernel<<<cdiv(ld_, 256), 256, 0, st_>>>(incU, ld_, status, active);
+    backsub_kernel<T, BC><<<cdiv(std::max(np_, 1), 128), 128, 0, st_>>>(d_, W_.as<T>(), Vinv_.as<T>(), bV_.as<T>(),
+                                                                      incU, incV, status, active);
+    launches += 2;
+    if (tm) NL_CUDA(cudaEventRecord(ev_[6], st_));
+    NL_CUDA(cudaGetLastError());
+    if (tm) {
+      NL_CUDA(cudaEventSynchronize(ev_[6]));
+      float ms[6];
+      for (int i = 0; i < 6; i++) cudaEventElapsedTime(&ms[i], ev_[i], ev_[i + 1]);
+      times.vinv_ms = ms[0];
+      times.wvinv_bs_ms = ms[1];
+      times.schur_ms = ms[2];
+      times.factor_ms = ms[3];
+      times.solve_ms = ms[4];
+      times.backsub_ms = ms[5];
+      cudaEventElapsedTime(&times.total_ms, ev_[0], ev_[6]);
+    }
+    return NL_OK;
+  }
+
+  nl_status enqueue_hdiag(double* out) override {
+    const int grid = std::max(1, std::min(kRedCTAs, cdiv(nci_ + np_, 256)));
+    hdiag_kernel<T, BC><<<grid, 256, 0, st_>>>(U_.as<T>(), d_.u_diag_uid, nci_, V_.as<T>(), d_.v_uid, np_,
+                                               part_.as<double>());
+    max_finalize_kernel<<<1, 1, 0, st_>>>(part_.as<double>(), grid, out, nullptr);
+    launches += 2;
+    NL_CUDA(cudaGetLastError());
+    return NL_OK;
+  }
+
+  nl_status enqueue_maxabs_b(double* out, const int* active) override {
+    const int grid = std::max(1, std::min(kRedCTAs, cdiv(n_ + 3 * np_, kNT)));
+    maxabs_kernel<T, kNT><<<grid, kNT, 0, st_>>>(bU_.as<T>(), n_, bV_.as<T>(), 3 * np_, part_.as<double>(), active);
+    max_finalize_kernel<<<1, 1, 0, st_>>>(part_.as<double>(), grid, out, active);
+    launches += 2;
+    NL_CUDA(cudaGetLastError());
+    return NL_OK;
+  }
+
+  nl_status enqueue_inc_dot(const LmDev* s, double* part, int* nparts) override {
+    const int grid = std::max(1, std::min(kRedCTAs, cdiv(n_ + 3 * np_, kNT)));
+    inc_dot_kernel<T, kNT><<<grid, kNT, 0, st_>>>(incU, bU_.as<T>(), n_, incV, bV_.as<T>(), 3 * np_, s, part);
+    *nparts = grid;
+    launches++;
+    NL_CUDA(cudaGetLastError());
+    return NL_OK;
+  }
+
+  // ---- host transfers (tests / solver-only API) ----
+  template <typename A, typename B>
+  static void conv(const A* src, B* dst, size_t nblk, int bs, int sstride, int dstride) {
+    for (size_t q = 0; q < nblk; q++)
+      for (int i = 0; i < bs; i++) dst[q * dstride + i] = (B)src[q * sstride + i];
+  }
+
+  nl_status get_hessian(double* U, double* V, double* W, double* bU, double* bV) override {
+    NL_CUDA(cudaStreamSynchronize(st_));
+    auto fetch = [&](const DevBuf& b, size_t nblk, int bs, int stride, double* out) -> nl_status {
+      if (!out || nblk == 0) return NL_OK;
+      std::vector<T> h(nblk * stride);
+      NL_CUDA(cudaMemcpy(h.data(), b.p, h.size() * sizeof(T), cudaMemcpyDeviceToHost));
+      conv(h.data(), out, nblk, bs, stride, bs);
+      return NL_OK;
+    };
+    nl_status s;
+    if ((s = fetch(U_, nU_, BC * BC, Layout<T, BC>::U, U)) != NL_OK) return s;
+    if ((s = fetch(V_, nV_, 9, Layout<T, BC>::V, V)) != NL_OK) return s;
+    if ((s = fetch(W_, nW_, BC * 3, Layout<T, BC>::W, W)) != NL_OK) return s;
+    if ((s = fetch(bU_, 1, n_, n_, bU)) != NL_OK) return s;
+    if ((s = fetch(bV_, 1, 3 * np_, 3 * np_, bV)) != NL_OK) return s;
+    return NL_OK;
+  }
+
+  nl_status set_hessian(const double* U, const double* V, const double* W, const double* bU,
+                        const double* bV) override {
+    auto put = [&](DevBuf& b, size_t nblk, int bs, int stride, const double* in) -> nl_status {
+      if (!in || nblk == 0) return NL_OK;
+      std::vector<T> h(nblk * stride, (T)0);
+      conv(in, h.data(), nblk, bs, bs, stride);
+      NL_CUDA(cudaMemcpyAsync(b.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st_));
+      NL_CUDA(cudaStreamSynchronize(st_));
+      return NL_OK;
+    };
+    nl_status s;
+    if ((s = put(U_, nU_, BC * BC, Layout<T, BC>::U, U)) != NL_OK) return s;
+    if ((s = put(V_, nV_, 9, Layout<T, BC>::V, V)) != NL_OK) return s;
+    if ((s = put(W_, nW_, BC * 3, Layout<T, BC>::W, W)) != NL_OK) return s;
+    if ((s = put(bU_, 1, n_, n_, bU)) != NL_OK) return s;
+    if ((s = put(bV_, 1, 3 * np_, 3 * np_, bV)) != NL_OK) return s;
+    return NL_OK;
+  }
+
+  nl_status get_schur(double* S, double* bS) override {
+    if (!need_s0_) return NL_ERR_STATE;
+    NL_CUDA(cudaStreamSynchronize(st_));
+    std::vector<T> h((size_t)ld_ * ld_);
+    NL_CUDA(cudaMemcpy(h.data(), S0_.p, h.size() * sizeof(T), cudaMemcpyDeviceToHost));
+    if (S) {
+      // reference layout: upper triangle of S (row i, col j >= i) = lower[j][i]
+      for (int i = 0; i < n_; i++)
+        for (int j = 0; j < n_; j++) S[(size_t)i * n_ + j] = j >= i ? (double)h[(size_t)j * ld_ + i] : 0.0;
+    }
+    if (bS) NL_CUDA(cudaMemcpy(bS, bS_.p, sizeof(double) * n_, cudaMemcpyDeviceToHost));
+    return NL_OK;
+  }
+
+ private:
+  cublasHandle_t cublas_;
+  int precision_;
+  cudaStream_t st_ = nullptr;
+  int nci_ = 0, np_ = 0, nU_ = 0, nV_ = 0, nW_ = 0, nS_ = 0, n_ = 0, ld_ = 0, ntiles_ = 0;
+  long long npairs_ = 0;
+  bool need_s0_ = false;
+  SchurDev d_{};
+  DevBuf U_, V_, W_, Y_, Vinv_, bU_, bV_, bS_, incU_, incV_, y_, r_, dx_, part_, Linv_, flags_, S_, S0_, tcs_;
+  DevBuf v_uid_, w_row_ptr_, w_col_, w_row_, w_col_ptr_, w_col_uid_, u_diag_, s_i_, s_j_, s_uuid_, s_ptr_, pa_, pb_;
+  cudaEvent_t ev_[7] = {};
+};
+
+}  // namespace
+
+std::unique_ptr<SchurCore> make_schur_core(int precision, int bc, cublasHandle_t cublas) {
+  const bool f64 = precision == NL_PREC_FP64;
+#define NL_MK(B)                                                          \
+  case B:                                                                 \
+    if (f64) return std::unique_ptr<SchurCore>(new SchurCoreT<double, B>(cublas, precision)); \
+    return std::unique_ptr<SchurCore>(new SchurCoreT<float, B>(cublas, precision));
+  switch (bc) {
+    NL_MK(2)
+    NL_MK(3)
+    NL_MK(6)
+    NL_MK(9)
+    default:
+      return nullptr;
+  }
+#undef NL_MK
+}
+
+}  // namespace nl

@@ -1,0 +1,18 @@
+// tc_syrk.h -- tensor-core trailing update of the mixed-precision Cholesky.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace nl {
+
+// Scratch the tensor-core update needs for a trailing matrix of n_pad rows:
+// the current panel split into BF16 hi/lo halves in UMMA canonical layout.
+size_t tc_syrk_scratch_bytes(int n_pad);
+
+// S[I][J] -= X_I X_J' for the lower 128x128 tiles I >= J of the trailing
+// matrix (tiles t0 .. t0 + nt - 1), X = columns [k*128, (k+1)*128) of S
+// (FP32, row-major, leading dimension ld).  The product runs as three BF16
+// tcgen05 MMAs (hi*hi + hi*lo + lo*hi) accumulating in TMEM (FP32).
+cudaError_t tc_syrk_f32(float* S, int ld, int k, int t0, int nt, void* scratch,
+                        const int* active, int* status, cudaStream_t st);
+
+}  // namespace nl

@@ -1,0 +1,303 @@
+"""ctypes binding of libnelson_b200.so (the C ABI of include/nelson_b200.h).
+
+`BAProblemGPU` mirrors nelson's DoubleSection + SolverCholeskySchur +
+LevenbergMarquardt / GaussNewton interface on the device-resident engine.
+There is no CPU fallback: loading fails loudly when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+PREC_FP64, PREC_MIXED = 0, 1
+TRACE_STRIDE = 8
+REASONS = ["SuccessAtStart", "SuccessSmallIncrement", "SuccessEpsB", "SuccessSmallResiduals",
+           "SolverFailure", "MaxIterationReached", "MaxSubIterationReached"]
+
+
+class NelsonError(RuntimeError):
+    pass
+
+
+class ProblemDesc(C.Structure):
+    _fields_ = [("bc", C.c_int), ("nc_var", C.c_int), ("nc_fix", C.c_int), ("np_var", C.c_int),
+                ("np_fix", C.c_int), ("precision", C.c_int), ("f", C.c_double), ("cx", C.c_double),
+                ("cy", C.c_double), ("refine_sweeps", C.c_int), ("device", C.c_int)]
+
+
+class LMSettings(C.Structure):
+    """nl_lm_settings; defaults of nelson/LevenbergMarquardt.cpp:6-19."""
+    _fields_ = [("maxNumIt", C.c_int), ("maxNumSubIt", C.c_int), ("minNumIt", C.c_int),
+                ("epsBVector", C.c_double), ("epsIncSquare", C.c_double), ("epsChi2", C.c_double),
+                ("tau", C.c_double), ("penaltyV", C.c_double), ("initV", C.c_double),
+                ("maxScaleFactor", C.c_double), ("minScaleFactor", C.c_double)]
+
+    def __init__(self, **kw):
+        d = dict(maxNumIt=100, maxNumSubIt=10, minNumIt=0, epsBVector=1e-15, epsIncSquare=1e-30,
+                 epsChi2=1e-15, tau=1e-3, penaltyV=2.0, initV=2.0, maxScaleFactor=2.0 / 3.0,
+                 minScaleFactor=1.0 / 3.0)
+        d.update(kw)
+        super().__init__(**d)
+
+
+class GNSettings(C.Structure):
+    """nl_gn_settings; defaults of nelson/GaussNewton.cpp:12-22."""
+    _fields_ = [("maxNumIt", C.c_int), ("minNumIt", C.c_int), ("epsBVector", C.c_double),
+                ("epsIncSquare", C.c_double), ("epsChi2", C.c_double), ("absLambda", C.c_double),
+                ("relLambda", C.c_double)]
+
+    def __init__(self, **kw):
+        d = dict(maxNumIt=100, minNumIt=0, epsBVector=1e-15, epsIncSquare=1e-30, epsChi2=1e-15,
+                 absLambda=0.0, relLambda=0.0)
+        d.update(kw)
+        super().__init__(**d)
+
+
+class SolveReport(C.Structure):
+    _fields_ = [("reason", C.c_int), ("iterations", C.c_int), ("subiterations", C.c_int),
+                ("n_trace", C.c_int), ("chi2", C.c_double), ("mu", C.c_double)]
+
+
+class PhaseTimes(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("vinv_ms", "wvinv_bs_ms", "schur_ms", "factor_ms", "solve_ms",
+                                          "backsub_ms", "total_ms", "eval_ms")]
+
+
+class SolverDesc(C.Structure):
+    _fields_ = [("bu", C.c_int), ("nu", C.c_int), ("nv", C.c_int), ("nU", C.c_int), ("nV", C.c_int),
+                ("nW", C.c_int), ("precision", C.c_int), ("refine_sweeps", C.c_int), ("device", C.c_int)]
+
+
+EXPORTS = [
+    "nl_create", "nl_destroy", "nl_set_params", "nl_get_params", "nl_get_camera_state", "nl_add_ba_edges",
+    "nl_set_user2internal_u", "nl_structure_ready", "nl_set_observations", "nl_get_counts", "nl_get_patterns",
+    "nl_get_edge_uids", "nl_update", "nl_get_hessian", "nl_solver_init", "nl_max_abs_hdiag",
+    "nl_compute_increment", "nl_get_increment", "nl_inc_sqnorm", "nl_get_schur", "nl_oplus", "nl_backup",
+    "nl_rollback", "nl_max_abs_b", "nl_chi2", "nl_rho", "nl_lm_solve", "nl_gn_solve", "nl_phase_timings",
+    "nl_kernel_launches", "nl_solver_create", "nl_solver_destroy", "nl_solver_set_hessian",
+    "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_status_string", "nl_version",
+]
+
+_lib = None
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = True):
+    """Load the CUDA library (building it first if needed).  Raises when it cannot."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_build.LIB):
+        if not build_if_missing:
+            raise NelsonError(f"{_build.LIB} is missing; run nelson_b200.build.build()")
+        _build.build()
+    L = C.CDLL(_build.LIB)
+    vp, i, d = C.c_void_p, C.c_int, C.c_double
+    L.nl_create.argtypes = [C.POINTER(ProblemDesc), C.POINTER(vp)]
+    L.nl_status_string.restype = C.c_char_p
+    L.nl_version.restype = C.c_char_p
+    L.nl_compute_increment.argtypes = [vp, d, d, C.POINTER(i)]
+    L.nl_rho.argtypes = [vp, d, d, C.POINTER(d)]
+    L.nl_update.argtypes = [vp, i, C.POINTER(d)]
+    L.nl_lm_solve.argtypes = [vp, C.POINTER(LMSettings), C.POINTER(SolveReport), vp, i]
+    L.nl_gn_solve.argtypes = [vp, C.POINTER(GNSettings), C.POINTER(SolveReport), vp, i]
+    L.nl_solver_create.argtypes = [C.POINTER(SolverDesc), vp, vp, vp, C.POINTER(vp)]
+    L.nl_solver_compute_increment.argtypes = [vp, d, d, vp, vp, C.POINTER(i)]
+    for name in EXPORTS:  # fails loudly if the library lacks an entry point
+        if name not in ("nl_status_string", "nl_version"):
+            getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _chk(L, rc, what):
+    if rc != 0:
+        raise NelsonError(f"{what}: {L.nl_status_string(rc).decode()} ({rc})")
+
+
+class BAProblemGPU:
+    """Device-resident BA section: DoubleSection<cameras, points> with the
+    projection EdgeBinaryUV, solved by the CUDA SolverCholeskySchur."""
+
+    def __init__(self, bc, nc_var, np_var, nc_fix=0, np_fix=0, precision=PREC_FP64, f=500.0, cx=320.0,
+                 cy=240.0, refine_sweeps=-1, device=0):
+        self.L = load()
+        self.bc, self.nc_var, self.np_var, self.nc_fix, self.np_fix = bc, nc_var, np_var, nc_fix, np_fix
+        self.precision = precision
+        desc = ProblemDesc(bc=bc, nc_var=nc_var, nc_fix=nc_fix, np_var=np_var, np_fix=np_fix,
+                           precision=precision, f=f, cx=cx, cy=cy, refine_sweeps=refine_sweeps, device=device)
+        h = C.c_void_p()
+        _chk(self.L, self.L.nl_create(C.byref(desc), C.byref(h)), "nl_create")
+        self.h = h
+        self.ne = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.nl_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, rc, what):
+        _chk(self.L, rc, what)
+
+    @classmethod
+    def from_ba(cls, prob, precision=PREC_FP64, perm=None, refine_sweeps=-1, device=0):
+        g = cls(prob.bc, prob.nc_var, prob.np_var, prob.nc_fix, prob.np_fix, precision, prob.f, prob.cx, prob.cy,
+                refine_sweeps, device)
+        g.set_params(prob.cams, prob.pts)
+        cf = None if prob.cam_fixed is None else np.ascontiguousarray(prob.cam_fixed, np.int32)
+        pf = None if prob.pt_fixed is None else np.ascontiguousarray(prob.pt_fixed, np.int32)
+        w = None if prob.weight is None else np.ascontiguousarray(prob.weight, np.float64)
+        g._c(g.L.nl_add_ba_edges(g.h, prob.ne, _p(np.ascontiguousarray(prob.cam_idx, np.int32)), _p(cf),
+                                 _p(np.ascontiguousarray(prob.pt_idx, np.int32)), _p(pf),
+                                 _p(np.ascontiguousarray(prob.obs, np.float64)), _p(w)), "nl_add_ba_edges")
+        if perm is not None:
+            g._c(g.L.nl_set_user2internal_u(g.h, _p(np.ascontiguousarray(perm, np.int32))), "set_user2internal")
+        g.structure_ready()
+        return g
+
+    def structure_ready(self):
+        self._c(self.L.nl_structure_ready(self.h), "nl_structure_ready")
+        c = np.zeros(4, np.int32)
+        self._c(self.L.nl_get_counts(self.h, _p(c)), "nl_get_counts")
+        self.nU, self.nV, self.nW, self.ne = [int(x) for x in c]
+
+    def set_params(self, cams, pts):
+        self._c(self.L.nl_set_params(self.h, _p(np.ascontiguousarray(cams, np.float64)),
+                                     _p(np.ascontiguousarray(pts, np.float64))), "nl_set_params")
+
+    def set_observations(self, obs, weight=None):
+        w = None if weight is None else np.ascontiguousarray(weight, np.float64)
+        self._c(self.L.nl_set_observations(self.h, _p(np.ascontiguousarray(obs, np.float64)), _p(w)),
+                "nl_set_observations")
+
+    def get_params(self):
+        u = np.zeros((self.nc_var + self.nc_fix, self.bc))
+        v = np.zeros((self.np_var + self.np_fix, 3))
+        self._c(self.L.nl_get_params(self.h, _p(u), _p(v)), "nl_get_params")
+        return u, v
+
+    def camera_state(self):
+        s = np.zeros((self.nc_var + self.nc_fix, 16))
+        self._c(self.L.nl_get_camera_state(self.h, _p(s)), "nl_get_camera_state")
+        return s
+
+    def patterns(self):
+        u = np.zeros((self.nU, 2), np.int32)
+        v = np.zeros((self.nV, 2), np.int32)
+        w = np.zeros((self.nW, 2), np.int32)
+        self._c(self.L.nl_get_patterns(self.h, _p(u), _p(v), _p(w)), "nl_get_patterns")
+        return u, v, w
+
+    def edge_uids(self):
+        a, b, c = (np.zeros(self.ne, np.int32) for _ in range(3))
+        self._c(self.L.nl_get_edge_uids(self.h, _p(a), _p(b), _p(c)), "nl_get_edge_uids")
+        return a, b, c
+
+    def update(self, hessian=True):
+        chi2 = C.c_double()
+        self._c(self.L.nl_update(self.h, 1 if hessian else 0, C.byref(chi2)), "nl_update")
+        return chi2.value
+
+    def hessian(self):
+        bu = self.bc
+        U = np.zeros((self.nU, bu, bu))
+        V = np.zeros((self.nV, 3, 3))
+        W = np.zeros((self.nW, bu, 3))
+        bU = np.zeros(self.nc_var * bu)
+        bV = np.zeros(self.np_var * 3)
+        self._c(self.L.nl_get_hessian(self.h, _p(U), _p(V), _p(W), _p(bU), _p(bV)), "nl_get_hessian")
+        return U, V, W, bU, bV
+
+    def max_abs_hdiag(self):
+        v = C.c_double()
+        self._c(self.L.nl_max_abs_hdiag(self.h, C.byref(v)), "nl_max_abs_hdiag")
+        return v.value
+
+    def compute_increment(self, rel, abs_):
+        ok = C.c_int()
+        self._c(self.L.nl_compute_increment(self.h, rel, abs_, C.byref(ok)), "nl_compute_increment")
+        return bool(ok.value)
+
+    def increment(self):
+        du = np.zeros(self.nc_var * self.bc)
+        dv = np.zeros(self.np_var * 3)
+        self._c(self.L.nl_get_increment(self.h, _p(du), _p(dv)), "nl_get_increment")
+        return du, dv
+
+    def inc_sqnorm(self):
+        v = C.c_double()
+        self._c(self.L.nl_inc_sqnorm(self.h, C.byref(v)), "nl_inc_sqnorm")
+        return v.value
+
+    def schur(self):
+        n = C.c_int()
+        self._c(self.L.nl_get_schur(self.h, None, None, C.byref(n)), "nl_get_schur")
+        S = np.zeros((n.value, n.value))
+        bS = np.zeros(n.value)
+        self._c(self.L.nl_get_schur(self.h, _p(S), _p(bS), C.byref(n)), "nl_get_schur")
+        return S, bS
+
+    def oplus(self):
+        self._c(self.L.nl_oplus(self.h), "nl_oplus")
+
+    def backup(self):
+        self._c(self.L.nl_backup(self.h), "nl_backup")
+
+    def rollback(self):
+        self._c(self.L.nl_rollback(self.h), "nl_rollback")
+
+    def chi2(self):
+        v = C.c_double()
+        self._c(self.L.nl_chi2(self.h, C.byref(v)), "nl_chi2")
+        return v.value
+
+    def max_abs_b(self):
+        v = C.c_double()
+        self._c(self.L.nl_max_abs_b(self.h, C.byref(v)), "nl_max_abs_b")
+        return v.value
+
+    def rho(self, mu, old_chi2):
+        v = C.c_double()
+        self._c(self.L.nl_rho(self.h, mu, old_chi2, C.byref(v)), "nl_rho")
+        return v.value
+
+    def lm_solve(self, settings=None, trace_cap=4096):
+        s = settings or LMSettings()
+        rep = SolveReport()
+        tr = np.zeros((max(trace_cap, 1), TRACE_STRIDE))
+        self._c(self.L.nl_lm_solve(self.h, C.byref(s), C.byref(rep), _p(tr), trace_cap), "nl_lm_solve")
+        return REASONS[rep.reason], tr[:rep.n_trace].copy(), rep.iterations, rep.subiterations
+
+    def gn_solve(self, settings=None, trace_cap=4096):
+        s = settings or GNSettings()
+        rep = SolveReport()
+        tr = np.zeros((max(trace_cap, 1), TRACE_STRIDE))
+        self._c(self.L.nl_gn_solve(self.h, C.byref(s), C.byref(rep), _p(tr), trace_cap), "nl_gn_solve")
+        return REASONS[rep.reason], tr[:rep.n_trace].copy(), rep.iterations
+
+    def phase_times(self):
+        t = PhaseTimes()
+        self._c(self.L.nl_phase_timings(self.h, C.byref(t)), "nl_phase_timings")
+        return {n: getattr(t, n) for n, _ in PhaseTimes._fields_}
+
+    def kernel_launches(self):
+        v = C.c_longlong()
+        self._c(self.L.nl_kernel_launches(self.h, C.byref(v)), "nl_kernel_launches")
+        return v.value

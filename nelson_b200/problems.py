@@ -1,0 +1,314 @@
+"""Seeded synthetic bundle-adjustment problems and the linear test fixture.
+
+The reference publishes no dataset for its Schur LM path; its only BA
+workload is a random scene built in nelson/samples/BASchurPerfomances.cpp:30-97
+(random SE3 cameras looking at a point cloud, edges from a visibility list).
+These generators build scenes of the same kind at the sizes the benchmark
+configurations name, with seeded numpy RNG (seed = 1234 + config index), so the
+oracle, the CUDA path, the tests and bench.py all see bit-identical inputs.
+
+Camera model (shared by the oracle and the CUDA kernels):
+    P = R X + t,  (x, y) = P.xy / P.z,  d = 1 + k1 r^2 + k2 r^4,
+    pixel = f d (x, y) + (cx, cy)
+A camera is given as axis-angle w (3), t (3) and, for 9-parameter cameras,
+f, k1, k2.  Its increment is [dw, dt (, df, dk1, dk2)] with R <- exp(dw) R.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+from scipy.spatial.transform import Rotation
+
+CX, CY, F_FIXED = 320.0, 240.0, 500.0
+
+
+@dataclass
+class BAProblem:
+    """A bundle-adjustment instance: U section = cameras, V section = points."""
+
+    bc: int                      # camera block size (6 or 9)
+    cams: np.ndarray             # (nc_var + nc_fix, bc) initial values
+    pts: np.ndarray              # (np_var + np_fix, 3) initial values
+    nc_var: int
+    np_var: int
+    cam_idx: np.ndarray          # (ne,) int32 camera id per edge
+    pt_idx: np.ndarray           # (ne,) int32 point id per edge
+    obs: np.ndarray              # (ne, 2) pixel measurements
+    weight: np.ndarray | None = None   # (ne,) per-edge weights (cost w |r|^2)
+    cam_fixed: np.ndarray | None = None  # (ne,) int32, 1 = camera is a fixed node
+    pt_fixed: np.ndarray | None = None   # (ne,) int32, 1 = point is a fixed node
+    nc_fix: int = 0
+    np_fix: int = 0
+    f: float = F_FIXED
+    cx: float = CX
+    cy: float = CY
+    cams_true: np.ndarray | None = None
+    pts_true: np.ndarray | None = None
+    name: str = ""
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def ne(self) -> int:
+        return int(self.cam_idx.shape[0])
+
+
+def so3_exp(w: np.ndarray) -> np.ndarray:
+    return Rotation.from_rotvec(np.asarray(w, dtype=np.float64).reshape(-1, 3)).as_matrix()
+
+
+def so3_log(R: np.ndarray) -> np.ndarray:
+    return Rotation.from_matrix(np.asarray(R, dtype=np.float64).reshape(-1, 3, 3)).as_rotvec()
+
+
+def project(cams: np.ndarray, pts: np.ndarray, cam_idx, pt_idx, bc: int,
+            f=F_FIXED, cx=CX, cy=CY) -> np.ndarray:
+    """Pixel coordinates of pts[pt_idx] seen by cams[cam_idx] (float64)."""
+    R = so3_exp(cams[:, :3])[cam_idx]
+    t = cams[cam_idx, 3:6]
+    P = np.einsum("eij,ej->ei", R, pts[pt_idx]) + t
+    x = P[:, 0] / P[:, 2]
+    y = P[:, 1] / P[:, 2]
+    if bc == 9:
+        ff = cams[cam_idx, 6]
+        k1 = cams[cam_idx, 7]
+        k2 = cams[cam_idx, 8]
+    else:
+        ff, k1, k2 = f, 0.0, 0.0
+    r2 = x * x + y * y
+    d = 1.0 + r2 * (k1 + k2 * r2)
+    return np.stack([ff * d * x + cx, ff * d * y + cy], axis=1)
+
+
+def _look_at(centers: np.ndarray, targets: np.ndarray, up: np.ndarray) -> np.ndarray:
+    """World-to-camera rotations whose +z axis points from centre to target."""
+    z = targets - centers
+    z /= np.linalg.norm(z, axis=1, keepdims=True)
+    x = np.cross(z, up)
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    y = np.cross(z, x)
+    return np.stack([x, y, z], axis=1)  # rows
+
+
+def _choose(rng, ncand_valid: np.ndarray, cand: np.ndarray, kmin: int, kmax: int):
+    """Pick k ~ U{kmin..kmax} distinct candidates per row (k clipped to the
+    number of valid candidates); invalid candidates are marked -1 in `cand`."""
+    npnt, nc = cand.shape
+    keys = rng.random((npnt, nc))
+    keys[cand < 0] = 2.0
+    order = np.argsort(keys, axis=1, kind="stable")
+    k = rng.integers(kmin, kmax + 1, size=npnt)
+    k = np.minimum(k, ncand_valid)
+    kk = min(kmax, nc)
+    sel = np.take_along_axis(cand, order[:, :kk], axis=1)
+    mask = np.arange(kk)[None, :] < k[:, None]
+    # point-major edge list, cameras ascending inside a point
+    sel = np.where(mask, sel, np.iinfo(np.int32).max)
+    sel.sort(axis=1)  # the k chosen cameras now occupy the first k slots
+    pt_idx = np.repeat(np.arange(npnt, dtype=np.int32), k)
+    cam_idx = sel[mask].astype(np.int32)
+    return cam_idx, pt_idx
+
+
+def _finish(rng, name, bc, Rt, tt, intr, pts_true, cam_idx, pt_idx, noise=1.0,
+            outlier_frac=0.0, rot_sigma=0.01, t_sigma=0.05, pt_sigma=0.05,
+            weights=None, meta=None) -> BAProblem:
+    nc = Rt.shape[0]
+    wt = so3_log(Rt)
+    cams_true = np.concatenate([wt, tt] + ([intr] if bc == 9 else []), axis=1)
+    z = project(cams_true, pts_true, cam_idx, pt_idx, bc)
+    ne = z.shape[0]
+    z = z + rng.normal(0.0, noise, size=(ne, 2))
+    if outlier_frac > 0:
+        nout = int(round(outlier_frac * ne))
+        idx = rng.choice(ne, size=nout, replace=False)
+        z[idx] = project(cams_true, pts_true, cam_idx[idx], pt_idx[idx], bc) + \
+            rng.uniform(-50.0, 50.0, size=(nout, 2))
+    # initial values: left-perturbed rotations, shifted translations and points
+    dR = so3_exp(rng.normal(0.0, rot_sigma, size=(nc, 3)))
+    w0 = so3_log(np.einsum("cij,cjk->cik", dR, Rt))
+    t0 = tt + rng.normal(0.0, t_sigma, size=tt.shape)
+    parts = [w0, t0]
+    if bc == 9:
+        f0 = intr[:, 0:1] * (1.0 + 0.01 * rng.normal(size=(nc, 1)))
+        parts.append(np.concatenate([f0, np.zeros((nc, 2))], axis=1))
+    cams0 = np.concatenate(parts, axis=1)
+    pts0 = pts_true + rng.normal(0.0, pt_sigma, size=pts_true.shape)
+    return BAProblem(bc=bc, cams=np.ascontiguousarray(cams0), pts=np.ascontiguousarray(pts0),
+                     nc_var=nc, np_var=pts_true.shape[0],
+                     cam_idx=np.ascontiguousarray(cam_idx, dtype=np.int32),
+                     pt_idx=np.ascontiguousarray(pt_idx, dtype=np.int32),
+                     obs=np.ascontiguousarray(z), weight=weights,
+                     cams_true=cams_true, pts_true=pts_true, name=name, meta=meta or {})
+
+
+def ring_scene(nc: int, npts: int, kmin: int, kmax: int, bc: int, seed: int,
+               name: str = "ring", weights: bool = False, radius: float = 10.0,
+               height: float = 1.0, extent: float = 2.0) -> BAProblem:
+    """Cameras on a circle looking at the origin, points uniform in a cube;
+    each point seen by k ~ U{kmin..kmax} cameras drawn uniformly among those
+    that see it in front (every camera does, at these sizes)."""
+    rng = np.random.default_rng(seed)
+    th = 2.0 * np.pi * np.arange(nc) / nc
+    C = np.stack([radius * np.cos(th), radius * np.sin(th), np.full(nc, height)], axis=1)
+    Rt = _look_at(C, np.zeros_like(C), np.array([0.0, 0.0, 1.0]))
+    tt = -np.einsum("cij,cj->ci", Rt, C)
+    intr = None
+    if bc == 9:
+        intr = np.stack([rng.uniform(400.0, 600.0, nc), rng.normal(0, 0.01, nc),
+                         rng.normal(0, 0.01, nc)], axis=1)
+    pts = rng.uniform(-extent, extent, size=(npts, 3))
+    depth = np.einsum("cj,pj->pc", Rt[:, 2, :], pts) + tt[None, :, 2]
+    cand = np.where(depth > 0.1, np.arange(nc)[None, :], -1).astype(np.int64)
+    cam_idx, pt_idx = _choose(rng, (cand >= 0).sum(1), cand, kmin, kmax)
+    w = rng.uniform(0.5, 2.0, size=cam_idx.shape[0]) if weights else None
+    return _finish(rng, name, bc, Rt, tt, intr, pts, cam_idx, pt_idx, weights=w,
+                   meta=dict(nc=nc, np=npts, kmin=kmin, kmax=kmax))
+
+
+def grid_scene(gx: int, gy: int, npts: int, kmin: int, kmax: int, seed: int,
+               outlier_frac: float = 0.01, radius: int = 2, height: float = 10.0,
+               name: str = "grid") -> BAProblem:
+    """Aerial grid: gx*gy 9-parameter cameras at `height` looking down; each
+    point is seen by k ~ U{kmin..kmax} cameras drawn from the grid neighbours
+    (within `radius` cells) of the cell below it (camera-locality bias)."""
+    rng = np.random.default_rng(seed)
+    nc = gx * gy
+    ix, iy = np.meshgrid(np.arange(gx), np.arange(gy), indexing="ij")
+    C = np.stack([ix.ravel().astype(np.float64), iy.ravel().astype(np.float64),
+                  np.full(nc, height)], axis=1)
+    down = C.copy()
+    down[:, 2] = 0.0
+    R0 = _look_at(C, down, np.array([0.0, 1.0, 0.0]))
+    tilt = so3_exp(rng.normal(0.0, 0.05, size=(nc, 3)))
+    Rt = np.einsum("cij,cjk->cik", tilt, R0)
+    tt = -np.einsum("cij,cj->ci", Rt, C)
+    intr = np.stack([rng.uniform(400.0, 600.0, nc), rng.normal(0, 0.01, nc),
+                     rng.normal(0, 0.01, nc)], axis=1)
+    pts = np.stack([rng.uniform(-0.5, gx - 0.5, npts), rng.uniform(-0.5, gy - 0.5, npts),
+                    rng.uniform(-1.0, 1.0, npts)], axis=1)
+    cx0 = np.clip(np.rint(pts[:, 0]).astype(np.int64), 0, gx - 1)
+    cy0 = np.clip(np.rint(pts[:, 1]).astype(np.int64), 0, gy - 1)
+    offs = np.arange(-radius, radius + 1)
+    dx, dy = np.meshgrid(offs, offs, indexing="ij")
+    nx = cx0[:, None] + dx.ravel()[None, :]
+    ny = cy0[:, None] + dy.ravel()[None, :]
+    valid = (nx >= 0) & (nx < gx) & (ny >= 0) & (ny < gy)
+    cand = np.where(valid, nx * gy + ny, -1)
+    cam_idx, pt_idx = _choose(rng, valid.sum(1), cand, kmin, kmax)
+    return _finish(rng, name, 9, Rt, tt, intr, pts, cam_idx, pt_idx,
+                   outlier_frac=outlier_frac,
+                   meta=dict(nc=nc, np=npts, kmin=kmin, kmax=kmax, grid=(gx, gy)))
+
+
+# Benchmark configurations (seed = 1234 + index).
+CONFIG_NAMES = {
+    0: "c0: 20 cams (6-param ring) / 500 pts / k~U{3..8}",
+    1: "c1: 200 cams (9-param ring) / 50k pts / k~U{3..12}",
+    2: "c2: 1500 cams (9-param 30x50 grid) / 500k pts / k~U{2..12} / 1% outliers",
+    4: "c4: 64 cams (6-param ring) / 5k pts / k~U{3..8} / w~U[0.5,2]",
+}
+
+
+def make_config(idx: int, scale: float = 1.0) -> BAProblem:
+    """Problem for benchmark configuration `idx`; `scale` < 1 shrinks the
+    point count (and the grid) for quick tests while keeping the shape."""
+    seed = 1234 + idx
+    if idx == 0:
+        return ring_scene(20, max(50, int(500 * scale)), 3, 8, 6, seed, name="c0")
+    if idx == 1:
+        return ring_scene(max(10, int(200 * scale)), max(200, int(50000 * scale)), 3, 12, 9,
+                          seed, name="c1")
+    if idx == 2:
+        gx = max(4, int(round(30 * np.sqrt(scale))))
+        gy = max(6, int(round(50 * np.sqrt(scale))))
+        return grid_scene(gx, gy, max(500, int(500000 * scale)), 2, 12, seed, name="c2")
+    if idx == 4:
+        return ring_scene(64, max(200, int(5000 * scale)), 3, 8, 6, seed, name="c4",
+                          weights=True)
+    raise ValueError(f"no single-problem generator for config {idx}")
+
+
+def make_batch(n: int = 256, seed: int = 1234 + 3):
+    """Config 3: independent ring problems with uneven sizes."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        nc = int(rng.integers(8, 65))
+        npts = int(rng.integers(200, 4001))
+        out.append(ring_scene(nc, npts, 3, 8, 6, int(rng.integers(1 << 30)), name=f"c3.{i}"))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# The linear fixture of nelson/tests/testDoubleSectionSchurCommon.h:24-413.
+@dataclass
+class LinearEdge:
+    type: int        # 0 unary U, 1 unary V, 2 binary UU, 3 binary UV
+    id1: int
+    id2: int
+    A1: np.ndarray   # dr x B1
+    A2: np.ndarray | None
+    z: np.ndarray
+
+
+@dataclass
+class LinearProblem:
+    bu: int
+    bv: int
+    u: np.ndarray      # (nu_var + nu_fix, bu)
+    v: np.ndarray      # (nv_var + nv_fix, bv)
+    nu_var: int
+    nv_var: int
+    edges: list
+    nu_fix: int = 0
+    nv_fix: int = 0
+    u_true: np.ndarray | None = None
+    v_true: np.ndarray | None = None
+
+
+EDGE_UNARY_U, EDGE_UNARY_V, EDGE_BINARY_UU, EDGE_BINARY_UV = 0, 1, 2, 3
+
+
+def points2d3d_fixture(seed: int = 7, u_block_diagonal: bool = False,
+                       w_block_diagonal: bool = False) -> LinearProblem:
+    """5 2D points (U, block 2) and 3 3D points (V, block 3) with identity
+    Jacobian edges: unary on every point, binary UU on every pair (unless U is
+    block diagonal), binary UV on every (2D, 3D) pair (only (i, i) when W is
+    block diagonal).  Measurements are taken at the ground truth, so chi2 = 0
+    there (testDoubleSectionCommon.hpp:15-58)."""
+    rng = np.random.default_rng(seed)
+    gt = rng.uniform(-1.0, 1.0, size=(3, 5))
+    p2 = gt[:2, :5].T.copy()
+    p3 = gt[:, :3].T.copy()
+    fixed2 = rng.uniform(-1, 1, size=(1, 2))
+    fixed3 = rng.uniform(-1, 1, size=(1, 3))
+    I2 = np.eye(2)
+    I3 = np.eye(3)
+    sel = np.array([[-1.0, 0, 0], [0, -1.0, 0]])
+    edges = []
+    for i in range(5):
+        edges.append(LinearEdge(EDGE_UNARY_U, i, -1, I2, None, p2[i].copy()))
+    for i in range(3):
+        edges.append(LinearEdge(EDGE_UNARY_V, i, -1, I3, None, p3[i].copy()))
+    if not u_block_diagonal:
+        for i in range(5):
+            for j in range(i + 1, 5):
+                edges.append(LinearEdge(EDGE_BINARY_UU, i, j, I2, -I2, p2[i] - p2[j]))
+    if not w_block_diagonal:
+        for i in range(5):
+            for j in range(3):
+                edges.append(LinearEdge(EDGE_BINARY_UV, i, j, I2, sel, p2[i] - p3[j][:2]))
+    else:
+        for i in range(3):
+            edges.append(LinearEdge(EDGE_BINARY_UV, i, i, I2, sel, p2[i] - p3[i][:2]))
+    return LinearProblem(bu=2, bv=3, u=np.concatenate([p2, fixed2]), v=np.concatenate([p3, fixed3]),
+                         nu_var=5, nv_var=3, edges=edges, nu_fix=1, nv_fix=1,
+                         u_true=p2.copy(), v_true=p3.copy())
+
+
+def add_uniform_noise(lp: LinearProblem, sigma: float, rng) -> None:
+    """Points2d3dBase::addNoise: uniform in [-sigma, sigma] on the variable
+    parameters (testDoubleSectionSchurCommon.h:347-354)."""
+    lp.u[:lp.nu_var] += rng.uniform(-sigma, sigma, size=(lp.nu_var, lp.bu))
+    lp.v[:lp.nv_var] += rng.uniform(-sigma, sigma, size=(lp.nv_var, lp.bv))

@@ -1,0 +1,129 @@
+"""Parity of the CUDA path (through the C ABI) with the FP64 CPU oracle.
+
+Tolerances: index maps bit-exact; FP64 mode 1e-12 relative on Hessian
+blocks, costs and increments and 1e-9 on the per-iteration LM cost; mixed
+mode (FP32 Jacobians / Hessian / Schur products) 1e-6 relative on the
+Hessian blocks, 1e-4 on the increment, 1e-6 on the per-iteration LM cost.
+"""
+import numpy as np
+import pytest
+
+from nelson_b200 import native as N
+from nelson_b200.problems import make_config
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+MIXED_H_TOL = 1e-6
+MIXED_INC_TOL = 1e-4
+LM_TOL = {N.PREC_FP64: 1e-9, N.PREC_MIXED: 1e-6}
+
+CASES = [(0, 1.0), (1, 0.1), (2, 0.01)]
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def Orc(oracle_lib):
+    return oracle_lib
+
+
+@pytest.mark.parametrize("cfg,scale", CASES)
+def test_structure_bit_exact(Orc, cfg, scale):
+    p = make_config(cfg, scale)
+    perm = np.random.default_rng(cfg).permutation(p.nc_var)
+    for pm in (None, perm):
+        o = Orc.Oracle.from_ba(p, perm=pm)
+        g = N.BAProblemGPU.from_ba(p, precision=N.PREC_FP64, perm=pm)
+        assert (o.nU, o.nV, o.nW, o.ne) == (g.nU, g.nV, g.nW, g.ne)
+        for a, b in zip(o.patterns(), g.patterns()):
+            assert np.array_equal(a, b)
+        for a, b in zip(o.edge_uids(), g.edge_uids()):
+            assert np.array_equal(a, b)
+        g.close()
+
+
+@pytest.mark.parametrize("prec", [N.PREC_FP64, N.PREC_MIXED])
+@pytest.mark.parametrize("cfg,scale", CASES)
+def test_hessian_and_increment(Orc, cfg, scale, prec):
+    p = make_config(cfg, scale)
+    o = Orc.Oracle.from_ba(p)
+    g = N.BAProblemGPU.from_ba(p, precision=prec)
+    c_o, c_g = o.update(True), g.update(True)
+    assert abs(c_o - c_g) <= FP64_TOL * c_o  # the cost is FP64 in both modes
+    tol = FP64_TOL if prec == N.PREC_FP64 else MIXED_H_TOL
+    for a, b in zip(g.hessian(), o.hessian()):
+        assert rel(a, b) < tol * 10
+    assert g.max_abs_b() == pytest.approx(o.max_abs_b(), rel=tol * 10)
+    assert g.max_abs_hdiag() == pytest.approx(o.max_abs_hdiag(), rel=tol * 10)
+    mu = 1e-3 * o.max_abs_hdiag()
+    assert o.compute_increment(0.0, mu) and g.compute_increment(0.0, mu)
+    du_o, dv_o = o.increment()
+    du_g, dv_g = g.increment()
+    itol = 1e-10 if prec == N.PREC_FP64 else MIXED_INC_TOL
+    assert rel(du_g, du_o) < itol and rel(dv_g, dv_o) < itol
+    assert g.inc_sqnorm() == pytest.approx(o.inc_sqnorm(), rel=itol)
+    if g.nc_var * g.bc <= 4096:
+        S_o, bS_o = o.schur()
+        S_g, bS_g = g.schur()
+        assert rel(np.triu(S_g), np.triu(S_o)) < tol * 10
+        assert rel(bS_g, bS_o) < tol * 10
+    # problem concept: oplus / cost / rho / rollback
+    o.backup()
+    g.backup()
+    o.oplus()
+    g.oplus()
+    c_o2, c_g2 = o.update(False), g.update(False)
+    assert c_g2 == pytest.approx(c_o2, rel=1e-12 if prec == N.PREC_FP64 else 1e-6)
+    assert g.rho(mu, c_g) == pytest.approx(o.rho(mu, c_o), rel=1e-8 if prec == N.PREC_FP64 else 1e-3)
+    g.rollback()
+    assert g.update(False) == pytest.approx(c_g, rel=1e-15)
+    g.close()
+
+
+@pytest.mark.parametrize("prec", [N.PREC_FP64, N.PREC_MIXED])
+@pytest.mark.parametrize("cfg,scale", CASES)
+def test_lm_trace_matches_oracle(Orc, cfg, scale, prec):
+    p = make_config(cfg, scale)
+    o = Orc.Oracle.from_ba(p)
+    g = N.BAProblemGPU.from_ba(p, precision=prec)
+    r_o, tr_o, it_o, _ = o.lm_solve(Orc.LMSettings(maxNumIt=10))
+    r_g, tr_g, it_g, _ = g.lm_solve(N.LMSettings(maxNumIt=10))
+    # per-iteration cost while the trajectories are still descending (once
+    # both sit at the minimum the accept/reject pattern is rounding noise)
+    n = min(len(tr_o), len(tr_g))
+    for k in range(n):
+        if tr_o[k, 2] < 0 or tr_g[k, 2] < 0:
+            continue
+        if k > 0 and abs(tr_o[k, 2] - tr_o[k - 1, 2]) < 1e-9 * tr_o[k, 2]:
+            break
+        assert abs(tr_o[k, 2] - tr_g[k, 2]) <= LM_TOL[prec] * tr_o[k, 2], (k, tr_o[k], tr_g[k])
+        assert tr_g[k, 3] == pytest.approx(tr_o[k, 3], rel=1e-6)  # same damping sequence
+    # final cost
+    assert abs(tr_g[-1, 2] - tr_o[-1, 2]) <= LM_TOL[prec] * tr_o[-1, 2] or g.chi2() == pytest.approx(
+        o.chi2(), rel=LM_TOL[prec])
+    # final parameters
+    cu_o, pt_o = o.get_params()
+    cu_g, pt_g = g.get_params()
+    assert rel(pt_g, pt_o) < (1e-8 if prec == N.PREC_FP64 else 1e-3)
+    g.close()
+
+
+@pytest.mark.parametrize("prec", [N.PREC_FP64, N.PREC_MIXED])
+def test_gn_matches_oracle(Orc, prec):
+    p = make_config(0, 0.5)
+    o = Orc.Oracle.from_ba(p)
+    g = N.BAProblemGPU.from_ba(p, precision=prec)
+    s_o = Orc.GNSettings(maxNumIt=5, absLambda=1e-2)
+    s_g = N.GNSettings(maxNumIt=5, absLambda=1e-2)
+    r_o, tr_o, it_o = o.gn_solve(s_o)
+    r_g, tr_g, it_g = g.gn_solve(s_g)
+    assert r_o == r_g and it_o == it_g
+    tol = 1e-9 if prec == N.PREC_FP64 else 1e-5
+    for a, b in zip(tr_o, tr_g):
+        assert abs(a[2] - b[2]) <= tol * a[2]
+    g.close()

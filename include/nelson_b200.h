@@ -82,13 +82,17 @@ typedef struct {
   int n_trace;         /* records written */
   double chi2;         /* final cost */
   double mu;           /* final damping */
+  double device_ms;    /* device time of the solve (CUDA events on the handle's stream) */
 } nl_solve_report;
 
 /* Per-phase device time of the last computeIncrement, milliseconds
  * (the phases of SolverCholeskySchurIterationTimeStat, nelson/SolverCholeskySchur.h:25-38). */
 typedef struct {
   float vinv_ms, wvinv_bs_ms, schur_ms, factor_ms, solve_ms, backsub_ms, total_ms;
-  float eval_ms; /* last update(true) */
+  float eval_ms;     /* last update(true) */
+  float update_ms;   /* device time of the trailing updates inside factor_ms */
+  int update_launches;
+  double update_flop; /* algorithmic flops of those updates (2 * multiply-adds) */
 } nl_phase_times;
 
 /* ---- problem: device-resident BA section -------------------------------- */

@@ -308,3 +308,97 @@ static __global__ void oplus_pt_kernel(double* __restrict__ pt, int np_var, cons
 }
 
 }  // namespace nl
+
+namespace nl {
+
+// ---------------------------------------------------------------------------
+// Parameter exchange with the caller: axis-angle cameras <-> stored state,
+// and observation reordering into the device edge orders.  Done on the
+// device so host buffers (pinned or not) are copied once, unchanged.
+__device__ inline void so3_log_dev(const double* R, double* w) {
+  const double tr = R[0] + R[4] + R[8];
+  const double c = fmin(1.0, fmax(-1.0, 0.5 * (tr - 1.0)));
+  const double th = acos(c);
+  const double v0 = R[7] - R[5], v1 = R[2] - R[6], v2 = R[3] - R[1];
+  if (th < 1e-4) {
+    const double f = 0.5 * (1.0 + th * th / 6.0);
+    w[0] = f * v0;
+    w[1] = f * v1;
+    w[2] = f * v2;
+    return;
+  }
+  if (3.141592653589793 - th < 1e-4) {
+    int k = 0;
+    if (R[4] > R[k * 4]) k = 1;
+    if (R[8] > R[k * 4]) k = 2;
+    double a[3];
+    const double d = sqrt(fmax(0.0, 0.5 * (R[k * 4] + 1.0)));
+    for (int i = 0; i < 3; i++) a[i] = (i == k) ? d : (0.25 * (R[i * 3 + k] + R[k * 3 + i])) / d;
+    const double nn = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    const double s = (v0 * a[0] + v1 * a[1] + v2 * a[2]) < 0 ? -1.0 : 1.0;
+    for (int i = 0; i < 3; i++) w[i] = s * th * a[i] / nn;
+    return;
+  }
+  const double f = th / (2.0 * sin(th));
+  w[0] = f * v0;
+  w[1] = f * v1;
+  w[2] = f * v2;
+}
+
+static __global__ void cams_in_kernel(const double* __restrict__ in, double* __restrict__ state, int n, int bc,
+                                      double f_fixed) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const double* a = in + (size_t)c * bc;
+  double* s = state + (size_t)c * 16;
+  double R[9];
+  so3_exp(a, R);
+  for (int i = 0; i < 9; i++) s[i] = R[i];
+  s[9] = a[3];
+  s[10] = a[4];
+  s[11] = a[5];
+  if (bc == 9) {
+    s[12] = a[6];
+    s[13] = a[7];
+    s[14] = a[8];
+  } else {
+    s[12] = f_fixed;
+    s[13] = 0.0;
+    s[14] = 0.0;
+  }
+  s[15] = 0.0;
+}
+
+static __global__ void cams_out_kernel(const double* __restrict__ state, double* __restrict__ out, int n, int bc) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const double* s = state + (size_t)c * 16;
+  double* o = out + (size_t)c * bc;
+  double w[3];
+  so3_log_dev(s, w);
+  o[0] = w[0];
+  o[1] = w[1];
+  o[2] = w[2];
+  o[3] = s[9];
+  o[4] = s[10];
+  o[5] = s[11];
+  if (bc == 9) {
+    o[6] = s[12];
+    o[7] = s[13];
+    o[8] = s[14];
+  }
+}
+
+// dst[t] = src[order[t]] for observations (2 doubles) and weights.
+static __global__ void gather_obs_kernel(const double* __restrict__ obs, const double* __restrict__ w,
+                                         const int* __restrict__ order, int n, double* __restrict__ dobs,
+                                         double* __restrict__ dw) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int e = order[t];
+  dobs[2 * (size_t)t] = obs[2 * (size_t)e];
+  dobs[2 * (size_t)t + 1] = obs[2 * (size_t)e + 1];
+  if (w) dw[t] = w[e];
+}
+
+}  // namespace nl

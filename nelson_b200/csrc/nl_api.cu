@@ -23,53 +23,6 @@ constexpr int kCamNT = 128;
 
 inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 
-void so3_exp_host(const double* w, double* R) {
-  const double th2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
-  double A, B;
-  if (th2 < 1e-8) {
-    A = 1.0 - th2 / 6.0 + th2 * th2 / 120.0;
-    B = 0.5 - th2 / 24.0 + th2 * th2 / 720.0;
-  } else {
-    const double th = std::sqrt(th2);
-    A = std::sin(th) / th;
-    B = (1.0 - std::cos(th)) / th2;
-  }
-  const double K[9] = {0, -w[2], w[1], w[2], 0, -w[0], -w[1], w[0], 0};
-  for (int i = 0; i < 3; i++)
-    for (int j = 0; j < 3; j++) {
-      double k2 = 0;
-      for (int k = 0; k < 3; k++) k2 += K[i * 3 + k] * K[k * 3 + j];
-      R[i * 3 + j] = A * K[i * 3 + j] + B * k2 + (i == j ? 1.0 : 0.0);
-    }
-}
-
-void so3_log_host(const double* R, double* w) {
-  const double tr = R[0] + R[4] + R[8];
-  const double c = std::max(-1.0, std::min(1.0, 0.5 * (tr - 1.0)));
-  const double th = std::acos(c);
-  const double v[3] = {R[7] - R[5], R[2] - R[6], R[3] - R[1]};
-  if (th < 1e-6) {
-    for (int i = 0; i < 3; i++) w[i] = 0.5 * v[i];
-    return;
-  }
-  if (M_PI - th < 1e-4) {
-    int k = 0;
-    if (R[4] > R[k * 4]) k = 1;
-    if (R[8] > R[k * 4]) k = 2;
-    double a[3];
-    const double d = std::sqrt(std::max(0.0, 0.5 * (R[k * 4] + 1.0)));
-    a[k] = d;
-    for (int i = 0; i < 3; i++)
-      if (i != k) a[i] = (0.25 * (R[i * 3 + k] + R[k * 3 + i])) / d;
-    const double nn = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
-    const double s = (v[0] * a[0] + v[1] * a[1] + v[2] * a[2]) < 0 ? -1.0 : 1.0;
-    for (int i = 0; i < 3; i++) w[i] = s * th * a[i] / nn;
-    return;
-  }
-  const double f = th / (2.0 * std::sin(th));
-  for (int i = 0; i < 3; i++) w[i] = f * v[i];
-}
-
 }  // namespace
 
 // ===========================================================================
@@ -96,6 +49,7 @@ struct nl_problem {
   DevBuf d_e_cam, d_e_pt, d_e_obs, d_e_w, d_cam_grp_ptr, d_grp_edge_ptr, d_grp_wuid, d_cam_uid, d_cam_slot;
   DevBuf d_pt_edge_ptr, d_p_cam, d_p_obs, d_p_w, d_pt_vuid;
   DevBuf d_part, d_scal, d_lm, d_trace;
+  DevBuf d_eorder, d_porder, stage_cams, stage_obs, stage_w;  // parameter / observation exchange
   std::unique_ptr<SchurCore> core;
   BaDev ba{};
   // scalars on the device: [0] chi2, [1] maxAbsB, [2] maxAbsHDiag, [3] rho
@@ -106,7 +60,7 @@ struct nl_problem {
   double lam_host[2] = {0, 0};
   DevBuf d_lam;
   long long launches = 0;
-  cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+  cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
   float eval_ms = 0;
   int have_jac = 0;
 
@@ -115,6 +69,8 @@ struct nl_problem {
     if (host_pin) cudaFreeHost(host_pin);
     if (ev_a) cudaEventDestroy(ev_a);
     if (ev_b) cudaEventDestroy(ev_b);
+    if (ev_t0) cudaEventDestroy(ev_t0);
+    if (ev_t1) cudaEventDestroy(ev_t1);
     core.reset();
     if (st) cudaStreamDestroy(st);
   }
@@ -264,6 +220,10 @@ nl_status build_structure(nl_problem* h) {
   NL_TRY(upload(h->d_p_obs, pobs, h->st));
   NL_TRY(upload(h->d_p_w, pw, h->st));
   NL_TRY(upload(h->d_pt_vuid, v_uid, h->st));
+  NL_TRY(upload(h->d_eorder, ord, h->st));
+  NL_TRY(upload(h->d_porder, pord, h->st));
+  NL_TRY(upload(h->stage_obs, h->e_obs, h->st));
+  NL_TRY(upload(h->stage_w, h->e_w, h->st));
   // Schur core
   SchurStructure ss;
   ss.bc = bc;
@@ -429,6 +389,7 @@ nl_status upload_params(nl_problem* h) {
 // Solve driver shared by LM and GN (the host only relaunches the fixed
 // sub-iteration sequence and watches the `done` flag one launch behind).
 nl_status run_solver(nl_problem* h, LmDev& init, nl_solve_report* rep, double* trace, int trace_cap, int max_launch) {
+  NL_CUDA(cudaEventRecord(h->ev_t0, h->st));
   // update(true) at the start (LevenbergMarquardt.hpp:41 / GaussNewton.hpp:40)
   nl_status r = enqueue_eval(h, true, h->scal, h->scal + 1, nullptr);
   if (r != NL_OK) return r;
@@ -445,13 +406,18 @@ nl_status run_solver(nl_problem* h, LmDev& init, nl_solve_report* rep, double* t
   double first[NL_TRACE_STRIDE] = {-1, init.gn ? 0.0 : -1.0, v[0], 0, 0, 0, 1, 1};
   if (trace && cap > 0) memcpy(trace, first, sizeof(first));
   if (v[1] <= init.epsBVector) {
+    NL_CUDA(cudaEventRecord(h->ev_t1, h->st));
+    NL_CUDA(cudaEventSynchronize(h->ev_t1));
     if (rep) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, h->ev_t0, h->ev_t1);
       rep->reason = NL_SUCCESS_AT_START;
       rep->iterations = -1;
       rep->subiterations = 0;
       rep->n_trace = cap > 0 ? 1 : 0;
       rep->chi2 = v[0];
       rep->mu = 0;
+      rep->device_ms = ms;
     }
     return NL_OK;
   }
@@ -484,7 +450,10 @@ nl_status run_solver(nl_problem* h, LmDev& init, nl_solve_report* rep, double* t
     }
     launched++;
   }
+  NL_CUDA(cudaEventRecord(h->ev_t1, h->st));
   NL_CUDA(cudaStreamSynchronize(h->st));
+  float dev_ms = 0;
+  cudaEventElapsedTime(&dev_ms, h->ev_t0, h->ev_t1);
   LmDev fin;
   NL_CUDA(cudaMemcpy(&fin, h->lm, sizeof(LmDev), cudaMemcpyDeviceToHost));
   const int nt = std::min(fin.trace_n, cap);
@@ -498,6 +467,7 @@ nl_status run_solver(nl_problem* h, LmDev& init, nl_solve_report* rep, double* t
     rep->n_trace = nt;
     rep->chi2 = fin.chi2;
     rep->mu = fin.mu;
+    rep->device_ms = dev_ms;
   }
   return NL_OK;
 }
@@ -537,6 +507,8 @@ nl_status nl_create(const nl_problem_desc* d, nl_problem** out) {
   NL_CUDA(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
   NL_CUDA(cudaEventCreateWithFlags(&h->ev_a, cudaEventDisableTiming));
   NL_CUDA(cudaEventCreateWithFlags(&h->ev_b, cudaEventDisableTiming));
+  NL_CUDA(cudaEventCreate(&h->ev_t0));
+  NL_CUDA(cudaEventCreate(&h->ev_t1));
   if (d->precision == NL_PREC_FP64) {
     if (cublasCreate(&h->cublas) != CUBLAS_STATUS_SUCCESS) return NL_ERR_CUDA;
     cublasSetStream(h->cublas, h->st);
@@ -564,6 +536,7 @@ nl_status nl_create(const nl_problem_desc* d, nl_problem** out) {
   if ((s = h->pt.alloc(sizeof(double) * std::max<size_t>(h->pts.size(), 3))) != NL_OK) return s;
   if ((s = h->pt_bck.alloc(h->pt.bytes)) != NL_OK) return s;
   if ((s = h->d_part.alloc(sizeof(double) * 8192)) != NL_OK) return s;
+  if ((s = h->stage_cams.alloc(sizeof(double) * std::max<size_t>((size_t)nc_all * 9, 9))) != NL_OK) return s;
   if ((s = h->d_scal.alloc(sizeof(double) * 16)) != NL_OK) return s;
   if ((s = h->d_lm.alloc(sizeof(LmDev))) != NL_OK) return s;
   if ((s = h->d_lam.alloc(sizeof(double) * 2 + sizeof(int) * 2)) != NL_OK) return s;
@@ -573,7 +546,7 @@ nl_status nl_create(const nl_problem_desc* d, nl_problem** out) {
   h->lm = h->d_lm.as<LmDev>();
   h->status = reinterpret_cast<int*>(h->d_lam.as<double>() + 2);
   NL_CUDA(cudaMallocHost(&h->host_pin, 4096));
-  if ((s = upload_params(h.get())) != NL_OK) return s;
+  if ((s = upload_params(h.get())) != NL_OK) return s;  // identity cameras, origin points
   *out = h.release();
   return NL_OK;
 }
@@ -588,30 +561,19 @@ nl_status nl_destroy(nl_problem* h) {
 
 nl_status nl_set_params(nl_problem* h, const double* cams, const double* pts) {
   NL_CHECK_H(h);
-  const int bc = h->desc.bc;
-  if (cams) {
-    for (int c = 0; c < h->nc_all(); c++) {
-      const double* in = cams + (size_t)c * bc;
-      double* st = h->cam_state.data() + (size_t)c * 16;
-      so3_exp_host(in, st);
-      st[9] = in[3];
-      st[10] = in[4];
-      st[11] = in[5];
-      if (bc == 9) {
-        st[12] = in[6];
-        st[13] = in[7];
-        st[14] = in[8];
-      } else {
-        st[12] = h->desc.f;
-        st[13] = 0;
-        st[14] = 0;
-      }
-      st[15] = 0;
-    }
-  }
-  if (pts) memcpy(h->pts.data(), pts, h->pts.size() * sizeof(double));
   NL_CUDA(cudaSetDevice(h->device));
-  return upload_params(h);
+  const int nc = h->nc_all(), bc = h->desc.bc;
+  if (cams && nc > 0) {
+    NL_CUDA(cudaMemcpyAsync(h->stage_cams.p, cams, sizeof(double) * (size_t)nc * bc, cudaMemcpyHostToDevice, h->st));
+    cams_in_kernel<<<cdiv(nc, 128), 128, 0, h->st>>>(h->stage_cams.as<double>(), h->cam.as<double>(), nc, bc,
+                                                     h->desc.f);
+    h->launches++;
+  }
+  if (pts && h->np_all() > 0)
+    NL_CUDA(cudaMemcpyAsync(h->pt.p, pts, sizeof(double) * 3 * (size_t)h->np_all(), cudaMemcpyHostToDevice, h->st));
+  NL_CUDA(cudaGetLastError());
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  return NL_OK;
 }
 
 nl_status nl_get_camera_state(nl_problem* h, double* states) {
@@ -625,25 +587,16 @@ nl_status nl_get_camera_state(nl_problem* h, double* states) {
 nl_status nl_get_params(nl_problem* h, double* cams, double* pts) {
   NL_CHECK_H(h);
   NL_CUDA(cudaSetDevice(h->device));
+  const int nc = h->nc_all(), bc = h->desc.bc;
+  if (cams && nc > 0) {
+    cams_out_kernel<<<cdiv(nc, 128), 128, 0, h->st>>>(h->cam.as<double>(), h->stage_cams.as<double>(), nc, bc);
+    h->launches++;
+    NL_CUDA(cudaMemcpyAsync(cams, h->stage_cams.p, sizeof(double) * (size_t)nc * bc, cudaMemcpyDeviceToHost, h->st));
+  }
+  if (pts && h->np_all() > 0)
+    NL_CUDA(cudaMemcpyAsync(pts, h->pt.p, sizeof(double) * 3 * (size_t)h->np_all(), cudaMemcpyDeviceToHost, h->st));
+  NL_CUDA(cudaGetLastError());
   NL_CUDA(cudaStreamSynchronize(h->st));
-  std::vector<double> st(h->cam_state.size());
-  NL_CUDA(cudaMemcpy(st.data(), h->cam.p, sizeof(double) * st.size(), cudaMemcpyDeviceToHost));
-  const int bc = h->desc.bc;
-  if (cams)
-    for (int c = 0; c < h->nc_all(); c++) {
-      const double* s = st.data() + (size_t)c * 16;
-      double* o = cams + (size_t)c * bc;
-      so3_log_host(s, o);
-      o[3] = s[9];
-      o[4] = s[10];
-      o[5] = s[11];
-      if (bc == 9) {
-        o[6] = s[12];
-        o[7] = s[13];
-        o[8] = s[14];
-      }
-    }
-  if (pts) NL_CUDA(cudaMemcpy(pts, h->pt.p, sizeof(double) * h->pts.size(), cudaMemcpyDeviceToHost));
   return NL_OK;
 }
 
@@ -695,29 +648,24 @@ nl_status nl_structure_ready(nl_problem* h) {
 
 nl_status nl_set_observations(nl_problem* h, const double* obs, const double* weight) {
   NL_CHECK_READY(h);
-  const size_t ne = h->e_cam.size();
-  if (obs) memcpy(h->e_obs.data(), obs, sizeof(double) * 2 * ne);
-  if (weight) memcpy(h->e_w.data(), weight, sizeof(double) * ne);
-  std::vector<double> eobs(2 * ne), ew(ne), pobs(2 * h->porder.size()), pw(h->porder.size());
-  for (size_t t = 0; t < ne; t++) {
-    const int e = h->eorder[t];
-    eobs[2 * t] = h->e_obs[2 * (size_t)e];
-    eobs[2 * t + 1] = h->e_obs[2 * (size_t)e + 1];
-    ew[t] = h->e_w[e];
-  }
-  for (size_t t = 0; t < h->porder.size(); t++) {
-    const int e = h->porder[t];
-    pobs[2 * t] = h->e_obs[2 * (size_t)e];
-    pobs[2 * t + 1] = h->e_obs[2 * (size_t)e + 1];
-    pw[t] = h->e_w[e];
-  }
+  const int ne = (int)h->e_cam.size(), npo = (int)h->porder.size();
+  if (ne == 0) return NL_OK;
   NL_CUDA(cudaSetDevice(h->device));
-  NL_CUDA(cudaMemcpyAsync(h->d_e_obs.p, eobs.data(), eobs.size() * 8, cudaMemcpyHostToDevice, h->st));
-  NL_CUDA(cudaMemcpyAsync(h->d_e_w.p, ew.data(), ew.size() * 8, cudaMemcpyHostToDevice, h->st));
-  if (!pobs.empty()) {
-    NL_CUDA(cudaMemcpyAsync(h->d_p_obs.p, pobs.data(), pobs.size() * 8, cudaMemcpyHostToDevice, h->st));
-    NL_CUDA(cudaMemcpyAsync(h->d_p_w.p, pw.data(), pw.size() * 8, cudaMemcpyHostToDevice, h->st));
+  if (obs) NL_CUDA(cudaMemcpyAsync(h->stage_obs.p, obs, sizeof(double) * 2 * (size_t)ne, cudaMemcpyHostToDevice, h->st));
+  if (weight) NL_CUDA(cudaMemcpyAsync(h->stage_w.p, weight, sizeof(double) * (size_t)ne, cudaMemcpyHostToDevice, h->st));
+  if (obs || weight) {
+    // unchanged halves keep their previous values: gather both from staging,
+    // which holds the last uploaded observations / weights
+    gather_obs_kernel<<<cdiv(ne, 256), 256, 0, h->st>>>(h->stage_obs.as<double>(), h->stage_w.as<double>(),
+                                                        h->d_eorder.as<int>(), ne, h->d_e_obs.as<double>(),
+                                                        h->d_e_w.as<double>());
+    if (npo > 0)
+      gather_obs_kernel<<<cdiv(npo, 256), 256, 0, h->st>>>(h->stage_obs.as<double>(), h->stage_w.as<double>(),
+                                                           h->d_porder.as<int>(), npo, h->d_p_obs.as<double>(),
+                                                           h->d_p_w.as<double>());
+    h->launches += 2;
   }
+  NL_CUDA(cudaGetLastError());
   NL_CUDA(cudaStreamSynchronize(h->st));
   return NL_OK;
 }

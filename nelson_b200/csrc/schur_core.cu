@@ -199,6 +199,16 @@ class SchurCoreT final : public SchurCore {
   nl_status enqueue_factor(int* status, const int* active) {
     const int smem_potrf = NB * (NB + 1) * (int)sizeof(double);
     const int smem_trsm = (NB * (NB + 1) + 32 * NB) * (int)sizeof(T);
+    const bool tm = timing && !active;
+    if (tm && (int)upd_ev_.size() < 2 * ntiles_) {
+      for (size_t i = upd_ev_.size(); i < (size_t)2 * ntiles_; i++) {
+        cudaEvent_t e;
+        NL_CUDA(cudaEventCreate(&e));
+        upd_ev_.push_back(e);
+      }
+    }
+    int nupd = 0;
+    double upd_flop = 0;
     for (int k = 0; k < ntiles_; k++) {
       potrf_diag_kernel<T><<<1, 256, smem_potrf, st_>>>(S_.as<T>(), ld_, k, Linv_.as<double>(), status, active);
       launches++;
@@ -207,6 +217,8 @@ class SchurCoreT final : public SchurCore {
       trsm_kernel<T><<<cdiv(below, 32), NB, smem_trsm, st_>>>(S_.as<T>(), ld_, k, below, Linv_.as<double>(), active);
       launches++;
       const int t0 = k + 1, nt = ntiles_ - t0;
+      if (tm) NL_CUDA(cudaEventRecord(upd_ev_[2 * nupd], st_));
+      upd_flop += (double)NB * below * (below + 1);  // 2 * NB * below (below + 1) / 2
       if (sizeof(T) == 8 && precision_ == NL_PREC_FP64 && cublas_) {
         // FP64 comparison path: cuBLAS DSYRK on the trailing matrix.  Row-major
         // lower storage is column-major upper; the panel X (below x NB, row-major)
@@ -224,6 +236,20 @@ class SchurCoreT final : public SchurCore {
         syrk_cc_kernel<T><<<nt * (nt + 1) / 2, 256, 0, st_>>>(S_.as<T>(), ld_, k, t0, nt, active);
         launches++;
       }
+      if (tm) NL_CUDA(cudaEventRecord(upd_ev_[2 * nupd + 1], st_));
+      nupd++;
+    }
+    if (tm) {
+      NL_CUDA(cudaEventSynchronize(upd_ev_[2 * nupd - 1 < 0 ? 0 : 2 * nupd - 1]));
+      float tot = 0;
+      for (int i = 0; i < nupd; i++) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, upd_ev_[2 * i], upd_ev_[2 * i + 1]);
+        tot += ms;
+      }
+      times.update_ms = tot;
+      times.update_launches = nupd;
+      times.update_flop = upd_flop;
     }
     return NL_OK;
   }
@@ -381,6 +407,7 @@ class SchurCoreT final : public SchurCore {
   DevBuf U_, V_, W_, Y_, Vinv_, bU_, bV_, bS_, incU_, incV_, y_, r_, dx_, part_, Linv_, flags_, S_, S0_, tcs_;
   DevBuf v_uid_, w_row_ptr_, w_col_, w_row_, w_col_ptr_, w_col_uid_, u_diag_, s_i_, s_j_, s_uuid_, s_ptr_, pa_, pb_;
   cudaEvent_t ev_[7] = {};
+  std::vector<cudaEvent_t> upd_ev_;
 };
 
 }  // namespace

@@ -59,12 +59,13 @@ class GNSettings(C.Structure):
 
 class SolveReport(C.Structure):
     _fields_ = [("reason", C.c_int), ("iterations", C.c_int), ("subiterations", C.c_int),
-                ("n_trace", C.c_int), ("chi2", C.c_double), ("mu", C.c_double)]
+                ("n_trace", C.c_int), ("chi2", C.c_double), ("mu", C.c_double), ("device_ms", C.c_double)]
 
 
 class PhaseTimes(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("vinv_ms", "wvinv_bs_ms", "schur_ms", "factor_ms", "solve_ms",
-                                          "backsub_ms", "total_ms", "eval_ms")]
+                                          "backsub_ms", "total_ms", "eval_ms", "update_ms")] + \
+        [("update_launches", C.c_int), ("update_flop", C.c_double)]
 
 
 class SolverDesc(C.Structure):
@@ -278,12 +279,15 @@ class BAProblemGPU:
         self._c(self.L.nl_rho(self.h, mu, old_chi2, C.byref(v)), "nl_rho")
         return v.value
 
-    def lm_solve(self, settings=None, trace_cap=4096):
+    def lm_solve(self, settings=None, trace_cap=4096, report=False):
         s = settings or LMSettings()
         rep = SolveReport()
         tr = np.zeros((max(trace_cap, 1), TRACE_STRIDE))
         self._c(self.L.nl_lm_solve(self.h, C.byref(s), C.byref(rep), _p(tr), trace_cap), "nl_lm_solve")
-        return REASONS[rep.reason], tr[:rep.n_trace].copy(), rep.iterations, rep.subiterations
+        out = (REASONS[rep.reason], tr[:rep.n_trace].copy(), rep.iterations, rep.subiterations)
+        if report:
+            return out + ({n: getattr(rep, n) for n, _ in SolveReport._fields_},)
+        return out
 
     def gn_solve(self, settings=None, trace_cap=4096):
         s = settings or GNSettings()

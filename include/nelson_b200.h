@@ -201,6 +201,13 @@ nl_status nl_solver_max_abs_hdiag(nl_solver* s, double* out);
 nl_status nl_solver_compute_increment(nl_solver* s, double rel_lambda, double abs_lambda,
                                       double* incU, double* incV, int* ok);
 
+/* Device self-test of the mixed path's tensor-core trailing update: builds a
+ * random FP32 matrix of ntiles x 128 rows on `device`, applies the panel-0
+ * update with the tcgen05 kernel and with the CUDA-core kernel, and returns
+ * max |difference| / max |CUDA-core result| over the updated lower tiles.
+ * (No counterpart in the reference: it checks the B200 kernel itself.) */
+nl_status nl_selftest_tc_update(int ntiles, unsigned long long seed, int device, double* max_rel_err);
+
 const char* nl_status_string(int status);
 /* Library build identification: "nelson_b200 <version> sm_100a". */
 const char* nl_version(void);

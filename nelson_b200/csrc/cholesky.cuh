@@ -22,149 +22,242 @@ constexpr int NB = 128;
 constexpr long long kSpinLimit = 1LL << 24;  // bounded waits (~1 s worst case)
 
 // ---------------------------------------------------------------------------
-// One CTA: factor the NB x NB diagonal tile of panel k in FP64 shared memory
-// (32-wide sub-panels: warp-register factor of the 32x32 diagonal,
-// substitution for the rows below, rank-32 update), write L_kk back to S and
-// inv(L_kk) (FP64, full NB x NB with zeros above the diagonal) to Linv.
+// One CTA (544 threads): factor the NB x NB diagonal tile of panel k in FP64
+// and build its inverse, both in registers.
+// Thread t owns 4x4 block (R, C), C <= R, of the lower triangle (528 blocks):
+// `a` holds A -> L, `x` holds B -> inv(L) for the same block position.  For
+// each block column jb (32 super-steps, three barriers each):
+//   (1) the owner of (jb, jb) factors its 4x4 block and inverts it;
+//   (2) owners of block column jb form L_R,jb = A_R,jb inv(L_jb,jb)' and
+//       publish it; owners of block row jb finish X_jb,C = inv(L_jb,jb) B_jb,C
+//       and publish it (right-looking forward substitution of L X = I);
+//   (3) owners right of jb apply the rank-4 update A -= L_R L_C'; owners
+//       below jb apply B_R,C -= L_R,jb X_jb,C.
+// L_kk is written back to S and inv(L_kk) (FP64, zeros above the diagonal)
+// to Linv.
+constexpr int PT = 544;
+constexpr int kTiles4 = (NB / 4) * (NB / 4 + 1) / 2;  // 528
+constexpr size_t kPotrfSmem = 0;
+
 template <typename T>
-static __global__ void __launch_bounds__(256) potrf_diag_kernel(T* __restrict__ S, int ld, int k,
-                                                          double* __restrict__ Linv, int* __restrict__ status,
-                                                          const int* __restrict__ active) {
-  extern __shared__ double sA[];  // NB x (NB + 1)
-  constexpr int LDS = NB + 1;
-  if (active && !*active) return;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const size_t base = (size_t)k * NB * ld + (size_t)k * NB;
-  for (int i = tid; i < NB * NB; i += 256) {
-    const int r = i / NB, c = i - r * NB;
-    sA[r * LDS + c] = c <= r ? (double)S[base + (size_t)r * ld + c] : 0.0;
-  }
-  __syncthreads();
+static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S, int ld, int k,
+                                                                double* __restrict__ Linv, int* __restrict__ status,
+                                                                const int* __restrict__ active) {
+  __shared__ double Lcol[NB][4];   // L of block column jb, rows >= 4 jb
+  __shared__ double Xrow[4][NB];   // X of block row jb, columns <= 4 jb + 3
+  __shared__ double Di[4][4];      // inv(L_jb,jb)
   __shared__ int bad;
+  if (active && !*active) return;
+  const int tid = threadIdx.x;
+  const size_t base = (size_t)k * NB * ld + (size_t)k * NB;
   if (tid == 0) bad = 0;
-  __syncthreads();
-  for (int s = 0; s < NB / 32; s++) {
-    const int c0 = 32 * s;
-    if (warp == 0) {
-      double a[32];
+  int R = 0, C = 0;
+  const bool own = tid < kTiles4;
+  if (own) {
+    R = (int)((sqrtf(8.0f * tid + 1.0f) - 1.0f) * 0.5f);
+    while ((R + 1) * (R + 2) / 2 <= tid) R++;
+    while (R * (R + 1) / 2 > tid) R--;
+    C = tid - R * (R + 1) / 2;
+  }
+  const int r0 = 4 * R, c0 = 4 * C;
+  double a[4][4], x[4][4];
 #pragma unroll
-      for (int j = 0; j < 32; j++) a[j] = (j <= lane) ? sA[(c0 + lane) * LDS + c0 + j] : 0.0;
+  for (int u = 0; u < 4; u++)
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+      a[u][v] = (own && c0 + v <= r0 + u) ? (double)S[base + (size_t)(r0 + u) * ld + c0 + v] : 0.0;
+      x[u][v] = (own && R == C && u == v) ? 1.0 : 0.0;
+    }
+  __syncthreads();
+  for (int jb = 0; jb < NB / 4; jb++) {
+    // (1) factor + invert the diagonal 4x4 block
+    if (own && R == jb && C == jb) {
       bool fail = false;
 #pragma unroll
-      for (int j = 0; j < 32; j++) {
-        const double piv = __shfl_sync(0xffffffffu, a[j], j);
-        fail |= !(piv > 0.0) || !isfinite(piv);
-        const double dj = sqrt(fmax(piv, 1e-300));
-        const double inv = 1.0 / dj;
-        if (lane == j) a[j] = dj;
-        else if (lane > j) a[j] *= inv;
+      for (int j = 0; j < 4; j++) {
+        double d = a[j][j];
 #pragma unroll
-        for (int l = j + 1; l < 32; l++) {
-          const double llj = __shfl_sync(0xffffffffu, a[j], l);
-          if (lane >= l) a[l] -= a[j] * llj;
+        for (int l = 0; l < j; l++) d -= a[j][l] * a[j][l];
+        fail |= !(d > 0.0) || !isfinite(d);
+        const double p = sqrt(fmax(d, 1e-300));
+        a[j][j] = p;
+#pragma unroll
+        for (int i = j + 1; i < 4; i++) {
+          double v = a[i][j];
+#pragma unroll
+          for (int l = 0; l < j; l++) v -= a[i][l] * a[j][l];
+          a[i][j] = v / p;
         }
       }
+      if (fail) bad = 1;
+      double di[4][4];
 #pragma unroll
-      for (int j = 0; j < 32; j++)
-        if (j <= lane) sA[(c0 + lane) * LDS + c0 + j] = a[j];
-      if (fail && lane == 0) bad = 1;
+      for (int c = 0; c < 4; c++)
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          double v = (i == c) ? 1.0 : 0.0;
+#pragma unroll
+          for (int l = 0; l < i; l++) v -= a[i][l] * di[l][c];
+          di[i][c] = (i >= c) ? v / a[i][i] : 0.0;
+        }
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          Di[i][c] = di[i][c];
+          if (c <= i) a[i][c] = a[i][c];
+          else a[i][c] = 0.0;
+        }
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) Lcol[r0 + u][v] = a[u][v];
     }
     __syncthreads();
-    // rows below: X = A * L_ss^-T by substitution (one row per thread)
-    for (int r = c0 + 32 + tid; r < NB; r += 256) {
-      double x[32];
+    // (2) block column jb of L, block row jb of X
+    if (own && C == jb && R > jb) {
 #pragma unroll
-      for (int j = 0; j < 32; j++) x[j] = sA[r * LDS + c0 + j];
+      for (int u = 0; u < 4; u++) {
+        double l[4];
 #pragma unroll
-      for (int j = 0; j < 32; j++) {
-        double v = x[j];
+        for (int v = 0; v < 4; v++) {
+          double s = 0.0;
 #pragma unroll
-        for (int l = 0; l < j; l++) v -= x[l] * sA[(c0 + j) * LDS + c0 + l];
-        x[j] = v / sA[(c0 + j) * LDS + c0 + j];
+          for (int w = 0; w <= v; w++) s += a[u][w] * Di[v][w];
+          l[v] = s;
+        }
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+          a[u][v] = l[v];
+          Lcol[r0 + u][v] = l[v];
+        }
       }
+    }
+    if (own && R == jb) {
 #pragma unroll
-      for (int j = 0; j < 32; j++) sA[r * LDS + c0 + j] = x[j];
+      for (int v = 0; v < 4; v++) {
+        double xx[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          double s = 0.0;
+#pragma unroll
+          for (int w = 0; w <= u; w++) s += Di[u][w] * x[w][v];
+          xx[u] = s;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          x[u][v] = xx[u];
+          Xrow[u][c0 + v] = xx[u];
+        }
+      }
     }
     __syncthreads();
-    // trailing update inside the tile: rows/cols [c0 + 32, NB), lower
-    const int m = NB - c0 - 32;
-    const int cnt = m * (m + 1) / 2;
-    for (int idx = tid; idx < cnt; idx += 256) {
-      int r = (int)((sqrt(8.0 * idx + 1.0) - 1.0) * 0.5);
-      while ((r + 1) * (r + 2) / 2 <= idx) r++;
-      while (r * (r + 1) / 2 > idx) r--;
-      const int c = idx - r * (r + 1) / 2;
-      const int R = c0 + 32 + r, Cc = c0 + 32 + c;
-      double v = sA[R * LDS + Cc];
-#pragma unroll 8
-      for (int l = 0; l < 32; l++) v -= sA[R * LDS + c0 + l] * sA[Cc * LDS + c0 + l];
-      sA[R * LDS + Cc] = v;
+    // (3) updates
+    if (own && C > jb) {
+#pragma unroll
+      for (int w = 0; w < 4; w++) {
+        double lr[4], lc[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          lr[u] = Lcol[r0 + u][w];
+          lc[u] = Lcol[c0 + u][w];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+          for (int v = 0; v < 4; v++) a[u][v] -= lr[u] * lc[v];
+      }
+    } else if (own && R > jb && C <= jb) {
+#pragma unroll
+      for (int w = 0; w < 4; w++) {
+        double lr[4], xr[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          lr[u] = Lcol[r0 + u][w];
+          xr[u] = Xrow[w][c0 + u];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+          for (int v = 0; v < 4; v++) x[u][v] -= lr[u] * xr[v];
+      }
     }
     __syncthreads();
   }
   if (tid == 0 && bad) atomicOr(status, ST_CHOL_FAIL);
-  // write L back
-  for (int i = tid; i < NB * NB; i += 256) {
-    const int r = i / NB, c = i - r * NB;
-    if (c <= r) S[base + (size_t)r * ld + c] = (T)sA[r * LDS + c];
-  }
-  // inverse, column c by thread c: L x = e_c; x kept in the (unused) upper
-  // triangle of sA, row c: sA[c][i] = Linv[i][c] for i > c.
-  __syncthreads();
   double* out = Linv + (size_t)k * NB * NB;
-  if (tid < NB) {
-    const int c = tid;
-    const double dc = 1.0 / sA[c * LDS + c];
-    for (int i = c + 1; i < NB; i++) {
-      double v = sA[i * LDS + c] * dc;
-      for (int l = c + 1; l < i; l++) v += sA[i * LDS + l] * sA[c * LDS + l];
-      sA[c * LDS + i] = -v / sA[i * LDS + i];
-    }
-    // column c of Linv
-    for (int i = 0; i < NB; i++) {
-      double v = 0.0;
-      if (i == c) v = dc;
-      else if (i > c) v = sA[c * LDS + i];
-      out[(size_t)i * NB + c] = v;
-    }
+  if (own) {
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int v = 0; v < 4; v++) {
+        const bool lower = c0 + v <= r0 + u;
+        out[(size_t)(r0 + u) * NB + c0 + v] = lower ? x[u][v] : 0.0;
+        if (lower) S[base + (size_t)(r0 + u) * ld + c0 + v] = (T)a[u][v];
+      }
+  }
+  // zero the strictly upper blocks of Linv
+  for (int i = tid; i < NB * NB; i += PT) {
+    const int r = i / NB, c = i - r * NB;
+    if ((c >> 2) > (r >> 2)) out[i] = 0.0;
   }
 }
 
 // ---------------------------------------------------------------------------
-// L_ik = A_ik inv(L_kk)' for 32-row slabs below the diagonal tile.
-// Thread j computes column j of the slab: X[r][j] = sum_{l<=j} A[r][l] Linv[j][l].
+// L_ik = A_ik inv(L_kk)' for 64-row slabs below the diagonal tile.  256
+// threads: row group g = tid / 64 (16 rows), columns p and 127 - p (balanced
+// against the triangular inverse).
+constexpr int TRSM_ROWS = 64;
 template <typename T>
-static __global__ void __launch_bounds__(NB) trsm_kernel(T* __restrict__ S, int ld, int k, int nrows_below,
-                                                  const double* __restrict__ Linv, const int* __restrict__ active) {
+constexpr size_t trsm_smem() {
+  return sizeof(T) * ((size_t)NB * (NB + 1) + (size_t)TRSM_ROWS * NB);
+}
+
+template <typename T>
+static __global__ void __launch_bounds__(256) trsm_kernel(T* __restrict__ S, int ld, int k, int nrows_below,
+                                                          const double* __restrict__ Linv,
+                                                          const int* __restrict__ active) {
   extern __shared__ unsigned char smraw[];
   T* sL = reinterpret_cast<T*>(smraw);  // NB x (NB + 1), Linv in T
-  T* sX = sL + NB * (NB + 1);            // 32 x NB rows of A
+  T* sX = sL + NB * (NB + 1);            // TRSM_ROWS x NB rows of A
   if (active && !*active) return;
   const int tid = threadIdx.x;
-  const int r0 = (k + 1) * NB + blockIdx.x * 32;
-  const int nr = min(32, (k + 1) * NB + nrows_below - r0);
+  const int r0 = (k + 1) * NB + blockIdx.x * TRSM_ROWS;
+  const int nr = min(TRSM_ROWS, (k + 1) * NB + nrows_below - r0);
   if (nr <= 0) return;
   const double* Li = Linv + (size_t)k * NB * NB;
-  for (int i = tid; i < NB * NB; i += NB) {
+  for (int i = tid; i < NB * NB; i += 256) {
     const int r = i / NB, c = i - r * NB;
     sL[r * (NB + 1) + c] = (T)Li[i];
   }
-  for (int i = tid; i < 32 * NB; i += NB) {
+  for (int i = tid; i < TRSM_ROWS * NB; i += 256) {
     const int r = i / NB, c = i - r * NB;
     sX[i] = r < nr ? S[(size_t)(r0 + r) * ld + (size_t)k * NB + c] : (T)0;
   }
   __syncthreads();
-  const int j = tid;
-  T acc[32];
+  const int g = tid >> 6, p = tid & 63;
+  const int j0 = p, j1 = NB - 1 - p;
+  T a0[16], a1[16];
 #pragma unroll
-  for (int r = 0; r < 32; r++) acc[r] = (T)0;
-  for (int l = 0; l <= j; l++) {
-    const T lj = sL[j * (NB + 1) + l];
+  for (int r = 0; r < 16; r++) a0[r] = a1[r] = (T)0;
+  for (int l = 0; l <= j1; l++) {
+    const T l0 = l <= j0 ? sL[j0 * (NB + 1) + l] : (T)0;
+    const T l1 = sL[j1 * (NB + 1) + l];
 #pragma unroll
-    for (int r = 0; r < 32; r++) acc[r] += sX[r * NB + l] * lj;
+    for (int r = 0; r < 16; r++) {
+      const T x = sX[(g * 16 + r) * NB + l];
+      a0[r] += x * l0;
+      a1[r] += x * l1;
+    }
   }
-  __syncthreads();
-  for (int r = 0; r < nr; r++) S[(size_t)(r0 + r) * ld + (size_t)k * NB + j] = acc[r];
+#pragma unroll
+  for (int r = 0; r < 16; r++) {
+    const int rr = g * 16 + r;
+    if (rr < nr) {
+      S[(size_t)(r0 + rr) * ld + (size_t)k * NB + j0] = a0[r];
+      S[(size_t)(r0 + rr) * ld + (size_t)k * NB + j1] = a1[r];
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -226,6 +319,9 @@ static __global__ void __launch_bounds__(256) syrk_cc_kernel(T* __restrict__ S, 
 // Triangular solves with the tile inverses.  CTAs take tickets in tile order
 // (forward) or reverse order (backward); a CTA only waits on tiles whose
 // owners took earlier tickets, so every wait ends; each wait is also bounded.
+// 512 threads: warp w owns rows 8w..8w+7 of a 128-row tile, lane l owns
+// columns 4l..4l+3; partial dot products stay in registers across tiles and
+// are reduced once.
 static __device__ inline bool wait_flag(const int* flag, int epoch, int* status) {
   long long it = 0;
   while (*(volatile const int*)flag != epoch) {
@@ -233,55 +329,83 @@ static __device__ inline bool wait_flag(const int* flag, int epoch, int* status)
       atomicOr(status, ST_SPIN_TIMEOUT);
       return false;
     }
-    __nanosleep(32);
+    if (it > 4096) __nanosleep(100);
   }
   __threadfence();
   return true;
 }
 
 template <typename T>
-static __global__ void __launch_bounds__(256) trsv_fwd_kernel(const T* __restrict__ L, int ld, int ntiles,
-                                                       const double* __restrict__ Linv, const double* __restrict__ b,
-                                                       double* __restrict__ y, int* __restrict__ ticket,
-                                                       int* __restrict__ flags, int epoch, int* __restrict__ status,
-                                                       const int* __restrict__ active) {
+__device__ inline void load4(const T* p, double* v) {
+  if (sizeof(T) == 4) {
+    const float4 f = *reinterpret_cast<const float4*>(p);
+    v[0] = f.x; v[1] = f.y; v[2] = f.z; v[3] = f.w;
+  } else {
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    const double2 b = *reinterpret_cast<const double2*>(p + 2);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+}
+
+__device__ inline void load4_cg(const double* p, double* v) {
+  const double2 a = __ldcg(reinterpret_cast<const double2*>(p));
+  const double2 b = __ldcg(reinterpret_cast<const double2*>(p + 2));
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+
+constexpr int SV = 512;
+constexpr size_t kTrsvSmem = sizeof(double) * NB * NB;
+
+template <typename T>
+static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict__ L, int ld, int ntiles,
+                                                             const double* __restrict__ Linv,
+                                                             const double* __restrict__ b, double* __restrict__ y,
+                                                             int* __restrict__ ticket, int* __restrict__ flags,
+                                                             int epoch, int* __restrict__ status,
+                                                             const int* __restrict__ active) {
+  extern __shared__ double sLi[];  // Linv_I, NB x NB
   __shared__ double acc[NB];
-  __shared__ double yj[NB];
   __shared__ int I_s, ok_s;
   if (active && !*active) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) I_s = atomicAdd(ticket, 1);
   __syncthreads();
   const int I = I_s;
-  if (tid < NB) acc[tid] = b[(size_t)I * NB + tid];
-  __syncthreads();
+  {
+    const double2* src = reinterpret_cast<const double2*>(Linv + (size_t)I * NB * NB);
+    double2* dst = reinterpret_cast<double2*>(sLi);
+    for (int i = tid; i < NB * NB / 2; i += SV) dst[i] = src[i];
+  }
+  double part[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const T* Lrow = L + (size_t)(I * NB + warp * 8) * ld + 4 * lane;
   for (int J = 0; J < I; J++) {
+    double lv[8][4];  // the L tile does not depend on y_J: load it before waiting
+#pragma unroll
+    for (int rr = 0; rr < 8; rr++) load4(Lrow + (size_t)rr * ld + (size_t)J * NB, lv[rr]);
     if (tid == 0) ok_s = wait_flag(flags + J, epoch, status) ? 1 : 0;
     __syncthreads();
     if (!ok_s) return;
-    if (tid < NB) yj[tid] = ((volatile double*)y)[(size_t)J * NB + tid];
-    __syncthreads();
-    // rows r = warp*16 .. +15: acc[r] -= L[I*NB + r][J*NB ...] . yj
-    for (int rr = 0; rr < 16; rr++) {
-      const int r = warp * 16 + rr;
-      const T* row = L + (size_t)(I * NB + r) * ld + (size_t)J * NB;
-      double s = 0.0;
+    double yv[4];
+    load4_cg(y + (size_t)J * NB + 4 * lane, yv);
 #pragma unroll
-      for (int c = lane; c < NB; c += 32) s += (double)row[c] * yj[c];
-      s = warp_sum(s);
-      if (lane == 0) acc[r] -= s;
-    }
-    __syncthreads();
+    for (int rr = 0; rr < 8; rr++)
+      part[rr] += lv[rr][0] * yv[0] + lv[rr][1] * yv[1] + lv[rr][2] * yv[2] + lv[rr][3] * yv[3];
   }
-  // y_I = Linv_I acc
-  const double* Li = Linv + (size_t)I * NB * NB;
-  for (int rr = 0; rr < 16; rr++) {
-    const int r = warp * 16 + rr;
-    double s = 0.0;
 #pragma unroll
-    for (int c = lane; c < NB; c += 32) s += Li[(size_t)r * NB + c] * acc[c];
-    s = warp_sum(s);
-    if (lane == 0) y[(size_t)I * NB + r] = s;
+  for (int rr = 0; rr < 8; rr++) {
+    const double s = warp_sum(part[rr]);
+    if (lane == 0) acc[warp * 8 + rr] = b[(size_t)I * NB + warp * 8 + rr] - s;
+  }
+  __syncthreads();
+  // y_I = Linv_I acc
+  const double* Li = sLi + (size_t)(warp * 8) * NB + 4 * lane;
+  double av[4] = {acc[4 * lane], acc[4 * lane + 1], acc[4 * lane + 2], acc[4 * lane + 3]};
+#pragma unroll
+  for (int rr = 0; rr < 8; rr++) {
+    double lv[4];
+    load4(Li + (size_t)rr * NB, lv);
+    const double s = warp_sum(lv[0] * av[0] + lv[1] * av[1] + lv[2] * av[2] + lv[3] * av[3]);
+    if (lane == 0) y[(size_t)I * NB + warp * 8 + rr] = s;
   }
   __threadfence();
   __syncthreads();
@@ -289,41 +413,75 @@ static __global__ void __launch_bounds__(256) trsv_fwd_kernel(const T* __restric
 }
 
 template <typename T>
-static __global__ void __launch_bounds__(256) trsv_bwd_kernel(const T* __restrict__ L, int ld, int ntiles,
-                                                       const double* __restrict__ Linv, const double* __restrict__ yv,
-                                                       double* __restrict__ x, int* __restrict__ ticket,
-                                                       int* __restrict__ flags, int epoch, int* __restrict__ status,
-                                                       const int* __restrict__ active) {
-  __shared__ double acc[2][NB];
-  __shared__ double xj[NB];
+static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict__ L, int ld, int ntiles,
+                                                             const double* __restrict__ Linv,
+                                                             const double* __restrict__ yv, double* __restrict__ x,
+                                                             int* __restrict__ ticket, int* __restrict__ flags,
+                                                             int epoch, int* __restrict__ status,
+                                                             const int* __restrict__ active) {
+  extern __shared__ double sLi[];  // Linv_I, NB x NB
+  __shared__ double red[SV / 32][NB];
+  __shared__ double acc[NB];
   __shared__ int I_s, ok_s;
   if (active && !*active) return;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) I_s = ntiles - 1 - atomicAdd(ticket, 1);
   __syncthreads();
   const int I = I_s;
-  const int c = tid & (NB - 1), half = tid >> 7;  // 2 threads per column
-  acc[half][c] = half == 0 ? yv[(size_t)I * NB + c] : 0.0;
+  {
+    const double2* src = reinterpret_cast<const double2*>(Linv + (size_t)I * NB * NB);
+    double2* dst = reinterpret_cast<double2*>(sLi);
+    for (int i = tid; i < NB * NB / 2; i += SV) dst[i] = src[i];
+  }
+  double part[4] = {0, 0, 0, 0};
   for (int J = ntiles - 1; J > I; J--) {
+    const T* Lb = L + (size_t)(J * NB + warp * 8) * ld + (size_t)I * NB + 4 * lane;
+    double lv[8][4];  // loaded before waiting for x_J
+#pragma unroll
+    for (int rr = 0; rr < 8; rr++) load4(Lb + (size_t)rr * ld, lv[rr]);
     if (tid == 0) ok_s = wait_flag(flags + J, epoch, status) ? 1 : 0;
     __syncthreads();
     if (!ok_s) return;
-    if (tid < NB) xj[tid] = ((volatile double*)x)[(size_t)J * NB + tid];
-    __syncthreads();
-    // acc[c] -= sum_r L[J*NB + r][I*NB + c] xj[r]
-    double s = 0.0;
-    for (int r = half * 64; r < half * 64 + 64; r++) s += (double)L[(size_t)(J * NB + r) * ld + (size_t)I * NB + c] * xj[r];
-    acc[half][c] -= s;
-    __syncthreads();
+#pragma unroll
+    for (int rr = 0; rr < 8; rr++) {
+      const double xr = __ldcg(x + (size_t)J * NB + warp * 8 + rr);
+      part[0] += lv[rr][0] * xr;
+      part[1] += lv[rr][1] * xr;
+      part[2] += lv[rr][2] * xr;
+      part[3] += lv[rr][3] * xr;
+    }
   }
+#pragma unroll
+  for (int q = 0; q < 4; q++) red[warp][4 * lane + q] = part[q];
   __syncthreads();
-  if (tid < NB) acc[0][tid] += acc[1][tid];
-  __syncthreads();
-  // x_I = Linv_I' acc : x[c] = sum_r Linv[r][c] acc[r]
-  const double* Li = Linv + (size_t)I * NB * NB;
   if (tid < NB) {
     double s = 0.0;
-    for (int r = 0; r < NB; r++) s += Li[(size_t)r * NB + tid] * acc[0][r];
+#pragma unroll
+    for (int w = 0; w < SV / 32; w++) s += red[w][tid];
+    acc[tid] = yv[(size_t)I * NB + tid] - s;
+  }
+  __syncthreads();
+  // x_I = Linv_I' acc : x[c] = sum_r Linv[r][c] acc[r]
+  const double* Li = sLi + (size_t)(warp * 8) * NB + 4 * lane;
+  double p2[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int rr = 0; rr < 8; rr++) {
+    const double ar = acc[warp * 8 + rr];
+    double lv[4];
+    load4(Li + (size_t)rr * NB, lv);
+    p2[0] += lv[0] * ar;
+    p2[1] += lv[1] * ar;
+    p2[2] += lv[2] * ar;
+    p2[3] += lv[3] * ar;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; q++) red[warp][4 * lane + q] = p2[q];
+  __syncthreads();
+  if (tid < NB) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < SV / 32; w++) s += red[w][tid];
     x[(size_t)I * NB + tid] = s;
   }
   __threadfence();
@@ -332,28 +490,77 @@ static __global__ void __launch_bounds__(256) trsv_bwd_kernel(const T* __restric
 }
 
 // ---------------------------------------------------------------------------
-// Refinement residual r = b - S0 x from the lower storage of S0, in two
-// passes: partial products per (row tile, chunk), then a fixed-order sum.
-// Row r of S0 is (lower row r) + (column r below the diagonal).
+// Refinement residual r = b - S0 x from the lower storage of S0.  Grid
+// (row tile I, chunk); a chunk covers a range of column tiles J.  For J < I
+// the tile S0_IJ is read row-wise (y_I += S0_IJ x_J), for J > I the tile
+// S0_JI is read row-wise and applied transposed (y_I += S0_JI' x_J); the
+// diagonal tile uses both halves.  Partials per chunk are summed in a fixed
+// order by resid_finalize_kernel.
 template <typename T, int NCH>
-static __global__ void __launch_bounds__(NB) symv_partial_kernel(const T* __restrict__ S0, int ld, int n_pad,
-                                                          const double* __restrict__ x, double* __restrict__ part,
-                                                          const int* __restrict__ active) {
+static __global__ void __launch_bounds__(SV) symv_partial_kernel(const T* __restrict__ S0, int ld, int ntiles,
+                                                                 const double* __restrict__ x,
+                                                                 double* __restrict__ part,
+                                                                 const int* __restrict__ active) {
+  __shared__ double red[SV / 32][NB];
   if (active && !*active) return;
   const int I = blockIdx.x, ch = blockIdx.y;
-  const int r = threadIdx.x;
-  const int R = I * NB + r;
-  // this chunk's slice of columns [c0, c1)
-  const int per = (n_pad + NCH - 1) / NCH;
-  const int c0 = ch * per, c1 = min(n_pad, c0 + per);
-  double s = 0.0;
-  // lower part of row R: columns c <= R -> S0[R][c]; upper part c > R -> S0[c][R]
-  // lower: thread r walks its own row (uncoalesced across threads, but rows are
-  // read once); upper: coalesced over r.
-  const int lo_end = min(c1, R + 1);
-  for (int c = c0; c < lo_end; c++) s += (double)S0[(size_t)R * ld + c] * x[c];
-  for (int c = max(c0, R + 1); c < c1; c++) s += (double)S0[(size_t)c * ld + R] * x[c];
-  part[(size_t)ch * n_pad + R] = s;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int per = (ntiles + NCH - 1) / NCH;
+  const int J0 = ch * per, J1 = min(ntiles, J0 + per);
+  double rp[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // rows 8 warp + rr
+  double cp[4] = {0, 0, 0, 0};              // columns 4 lane + q
+  for (int J = J0; J < J1; J++) {
+    if (J <= I) {
+      const T* Ls = S0 + (size_t)(I * NB + warp * 8) * ld + (size_t)J * NB + 4 * lane;
+      double xv[4];
+      load4(x + (size_t)J * NB + 4 * lane, xv);
+#pragma unroll
+      for (int rr = 0; rr < 8; rr++) {
+        double lv[4];
+        load4(Ls + (size_t)rr * ld, lv);
+        if (J == I) {  // lower half of the diagonal tile: c <= r
+          const int r = warp * 8 + rr;
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            if (4 * lane + q > r) lv[q] = 0.0;
+        }
+        rp[rr] += lv[0] * xv[0] + lv[1] * xv[1] + lv[2] * xv[2] + lv[3] * xv[3];
+      }
+    }
+    if (J >= I) {
+      const T* Ls = S0 + (size_t)(J * NB + warp * 8) * ld + (size_t)I * NB + 4 * lane;
+#pragma unroll
+      for (int rr = 0; rr < 8; rr++) {
+        const int r = warp * 8 + rr;  // row of tile J
+        const double xr = x[(size_t)J * NB + r];
+        double lv[4];
+        load4(Ls + (size_t)rr * ld, lv);
+        if (J == I) {  // strictly-lower entries (r > c) applied transposed
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            if (r <= 4 * lane + q) lv[q] = 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) cp[q] += lv[q] * xr;
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++) red[warp][4 * lane + q] = cp[q];
+  __syncthreads();
+  double rowsum[8];
+#pragma unroll
+  for (int rr = 0; rr < 8; rr++) rowsum[rr] = warp_sum(rp[rr]);
+  if (lane == 0) {
+#pragma unroll
+    for (int rr = 0; rr < 8; rr++) {
+      const int r = warp * 8 + rr;
+      double c = 0.0;
+#pragma unroll
+      for (int w = 0; w < SV / 32; w++) c += red[w][r];
+      part[(size_t)ch * ntiles * NB + (size_t)I * NB + r] = rowsum[rr] + c;
+    }
+  }
 }
 
 template <int NCH>

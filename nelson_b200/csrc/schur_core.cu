@@ -9,7 +9,7 @@ namespace {
 
 constexpr int kNT = 256;
 constexpr int kRedCTAs = 296;  // 2 x 148 SMs for grid-stride reductions
-constexpr int kSymvChunks = 4;
+constexpr int kSymvChunks = 8;
 constexpr int kSchurWarps = 8;
 
 inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
@@ -174,10 +174,9 @@ class SchurCoreT final : public SchurCore {
     d_.s_pair_ptr = s_ptr_.as<long long>();
     d_.pair_a = pa_.as<int>();
     d_.pair_b = pb_.as<int>();
-    const int smem_potrf = NB * (NB + 1) * (int)sizeof(double);
-    NL_CUDA(cudaFuncSetAttribute(potrf_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_potrf));
-    const int smem_trsm = (NB * (NB + 1) + 32 * NB) * (int)sizeof(T);
-    NL_CUDA(cudaFuncSetAttribute(trsm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_trsm));
+    NL_CUDA(cudaFuncSetAttribute(trsm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem<T>()));
+    NL_CUDA(cudaFuncSetAttribute(trsv_fwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsvSmem));
+    NL_CUDA(cudaFuncSetAttribute(trsv_bwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsvSmem));
     if (!ev_[0]) {
       for (auto& e : ev_) NL_CUDA(cudaEventCreate(&e));
     }
@@ -187,18 +186,16 @@ class SchurCoreT final : public SchurCore {
   // ---- solves with the factor: x = S^-1 b (trsv fwd + bwd) ----
   nl_status enqueue_solve(const double* b, double* x, int* status, const int* active) {
     NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
-    trsv_fwd_kernel<T><<<ntiles_, 256, 0, st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<double>(), b, y_.as<double>(),
+    trsv_fwd_kernel<T><<<ntiles_, SV, kTrsvSmem, st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<double>(), b, y_.as<double>(),
                                                  flags_.as<int>(), flags_.as<int>() + 1, 1, status, active);
     NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
-    trsv_bwd_kernel<T><<<ntiles_, 256, 0, st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<double>(), y_.as<double>(), x,
+    trsv_bwd_kernel<T><<<ntiles_, SV, kTrsvSmem, st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<double>(), y_.as<double>(), x,
                                                  flags_.as<int>(), flags_.as<int>() + 1, 1, status, active);
     launches += 2;
     return NL_OK;
   }
 
   nl_status enqueue_factor(int* status, const int* active) {
-    const int smem_potrf = NB * (NB + 1) * (int)sizeof(double);
-    const int smem_trsm = (NB * (NB + 1) + 32 * NB) * (int)sizeof(T);
     const bool tm = timing && !active;
     if (tm && (int)upd_ev_.size() < 2 * ntiles_) {
       for (size_t i = upd_ev_.size(); i < (size_t)2 * ntiles_; i++) {
@@ -210,11 +207,12 @@ class SchurCoreT final : public SchurCore {
     int nupd = 0;
     double upd_flop = 0;
     for (int k = 0; k < ntiles_; k++) {
-      potrf_diag_kernel<T><<<1, 256, smem_potrf, st_>>>(S_.as<T>(), ld_, k, Linv_.as<double>(), status, active);
+      potrf_diag_kernel<T><<<1, PT, kPotrfSmem, st_>>>(S_.as<T>(), ld_, k, Linv_.as<double>(), status, active);
       launches++;
       const int below = ld_ - (k + 1) * NB;
       if (below <= 0) break;
-      trsm_kernel<T><<<cdiv(below, 32), NB, smem_trsm, st_>>>(S_.as<T>(), ld_, k, below, Linv_.as<double>(), active);
+      trsm_kernel<T><<<cdiv(below, TRSM_ROWS), 256, trsm_smem<T>(), st_>>>(S_.as<T>(), ld_, k, below,
+                                                                            Linv_.as<double>(), active);
       launches++;
       const int t0 = k + 1, nt = ntiles_ - t0;
       if (tm) NL_CUDA(cudaEventRecord(upd_ev_[2 * nupd], st_));
@@ -280,8 +278,8 @@ class SchurCoreT final : public SchurCore {
     if (tm) NL_CUDA(cudaEventRecord(ev_[4], st_));
     if ((s = enqueue_solve(bS_.as<double>(), incU, status, active)) != NL_OK) return s;
     for (int it = 0; it < refine_sweeps && need_s0_; it++) {
-      symv_partial_kernel<T, kSymvChunks><<<dim3(ntiles_, kSymvChunks), NB, 0, st_>>>(
-          S0_.as<T>(), ld_, ld_, incU, part_.as<double>(), active);
+      symv_partial_kernel<T, kSymvChunks><<<dim3(ntiles_, kSymvChunks), SV, 0, st_>>>(
+          S0_.as<T>(), ld_, ntiles_, incU, part_.as<double>(), active);
       resid_finalize_kernel<kSymvChunks><<<cdiv(ld_, 256), 256, 0, st_>>>(part_.as<double>(), bS_.as<double>(), ld_,
                                                                           r_.as<double>(), active);
       if ((s = enqueue_solve(r_.as<double>(), dx_.as<double>(), status, active)) != NL_OK) return s;
@@ -430,3 +428,54 @@ std::unique_ptr<SchurCore> make_schur_core(int precision, int bc, cublasHandle_t
 }
 
 }  // namespace nl
+
+// ---------------------------------------------------------------------------
+namespace nl {
+namespace {
+__global__ void selftest_fill_kernel(float* S, size_t n, unsigned long long seed) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (i + 1);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  S[i] = (float)((double)(z >> 11) * (1.0 / 9007199254740992.0) - 0.5);
+}
+}  // namespace
+}  // namespace nl
+
+extern "C" nl_status nl_selftest_tc_update(int ntiles, unsigned long long seed, int device, double* max_rel_err) {
+  using namespace nl;
+  if (ntiles < 2 || ntiles > 64 || !max_rel_err) return NL_ERR_ARG;
+  NL_CUDA(cudaSetDevice(device));
+  const int ld = ntiles * NB;
+  const size_t n = (size_t)ld * ld;
+  DevBuf a, b, scratch, st;
+  nl_status r;
+  if ((r = a.alloc(n * 4)) != NL_OK || (r = b.alloc(n * 4)) != NL_OK ||
+      (r = scratch.alloc(tc_syrk_scratch_bytes(ld))) != NL_OK || (r = st.alloc(16)) != NL_OK)
+    return r;
+  NL_CUDA(cudaMemset(st.p, 0, 16));
+  selftest_fill_kernel<<<(unsigned)((n + 255) / 256), 256>>>(a.as<float>(), n, seed);
+  NL_CUDA(cudaMemcpy(b.p, a.p, n * 4, cudaMemcpyDeviceToDevice));
+  const int nt = ntiles - 1;
+  NL_CUDA(tc_syrk_f32(a.as<float>(), ld, 0, 1, nt, scratch.p, nullptr, st.as<int>(), 0));
+  syrk_cc_kernel<float><<<nt * (nt + 1) / 2, 256>>>(b.as<float>(), ld, 0, 1, nt, nullptr);
+  NL_CUDA(cudaGetLastError());
+  NL_CUDA(cudaDeviceSynchronize());
+  int stat = 0;
+  NL_CUDA(cudaMemcpy(&stat, st.p, 4, cudaMemcpyDeviceToHost));
+  if (stat & ST_SPIN_TIMEOUT) return NL_ERR_TIMEOUT;
+  std::vector<float> ha(n), hb(n);
+  NL_CUDA(cudaMemcpy(ha.data(), a.p, n * 4, cudaMemcpyDeviceToHost));
+  NL_CUDA(cudaMemcpy(hb.data(), b.p, n * 4, cudaMemcpyDeviceToHost));
+  double md = 0, mb = 0;
+  for (int i = NB; i < ld; i++)
+    for (int j = NB; j <= i; j++) {
+      const double x = ha[(size_t)i * ld + j], y = hb[(size_t)i * ld + j];
+      md = std::max(md, std::fabs(x - y));
+      mb = std::max(mb, std::fabs(y));
+    }
+  *max_rel_err = md / std::max(mb, 1e-300);
+  return NL_OK;
+}

@@ -1,12 +1,304 @@
 // tc_syrk.cu -- tensor-core (tcgen05) trailing update of the mixed Cholesky.
+//
+// For panel k the trailing lower triangle of S receives C_IJ -= X_I X_J',
+// X = S[(k+1)128:, k 128:(k+1) 128] (FP32).  This is the one dense
+// contraction of the reduced-camera-system factorisation
+// (SolverCholeskyEigenDense::factorize, nelson/SolverCholeskyDense.hpp:15-18).
+//
+// tc_pack_kernel   splits X into BF16 hi = bf16(x) and lo = bf16(x - hi) and
+//                  stores each 128-row tile in the UMMA canonical K-major
+//                  no-swizzle layout: 8x8 core matrices (128 contiguous bytes),
+//                  core (m-group g, k-group h) at byte (16 g + h) * 128, i.e.
+//                  LBO (K step) = 128 B, SBO (M step) = 2048 B.
+// tc_syrk_kernel   one CTA per lower 128x128 output tile: bulk-copies the
+//                  packed operands (cp.async.bulk + mbarrier) in two K chunks,
+//                  one thread issues 24 tcgen05.mma (M = N = 128, K = 16,
+//                  kind::f16, BF16 in, FP32 accumulate in TMEM) for
+//                  hi*hi + hi*lo + lo*hi and commits to an mbarrier; eight
+//                  warps read the accumulator with tcgen05.ld (32x32b), stage
+//                  it in shared memory and subtract it from the tile with
+//                  coalesced accesses.
+// Every wait is bounded: on expiry the kernel records ST_SPIN_TIMEOUT, waits
+// (bounded) for what it issued, frees its TMEM and returns.
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "nl_common.cuh"
 #include "tc_syrk.h"
 
 namespace nl {
 
-size_t tc_syrk_scratch_bytes(int n_pad) { return (size_t)n_pad * 128 * 2 * 2; }
+namespace {
 
-cudaError_t tc_syrk_f32(float*, int, int, int, int, void*, const int*, int*, cudaStream_t) {
-  return cudaErrorNotSupported;
+constexpr int TB = 128;                  // tile rows / cols / K of one panel
+constexpr int kTileBytes = TB * TB * 2;  // one BF16 operand tile (32 KB)
+constexpr int kPackTile = 2 * kTileBytes;  // hi + lo
+constexpr long long kWaitLimit = 1LL << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait; returns false when the limit is hit
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (long long it = 0; it < kWaitLimit; it++) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (it > 64) __nanosleep(32);
+  }
+  return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// shared-memory matrix descriptor: K-major, no swizzle
+__device__ __forceinline__ uint64_t umma_desc(const void* p, uint32_t lbo, uint32_t sbo) {
+  const uint32_t a = smem_u32(p);
+  uint64_t d = 0;
+  d |= (uint64_t)((a >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+  return d;               // base offset 0, layout type 0 (no swizzle)
+}
+
+// instruction descriptor: kind::f16, A = B = BF16, D = F32, K-major, M = N = 128
+constexpr uint32_t kIdesc = (1u << 4)           // D format F32
+                            | (1u << 7)         // A format BF16
+                            | (1u << 10)        // B format BF16
+                            | ((TB >> 3) << 17) // N >> 3
+                            | ((TB >> 4) << 24);// M >> 4
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// ---------------------------------------------------------------------------
+// X (rows r0 .. r0 + nrows - 1, columns k*TB ..) -> packed hi / lo tiles.
+// One thread per (row, 8-column group).
+__global__ void tc_pack_kernel(const float* __restrict__ S, int ld, int k, int nrows,
+                               uint8_t* __restrict__ pack, const int* __restrict__ active) {
+  if (active && !*active) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nrows * 16) return;
+  const int r = (int)(t >> 4), h = (int)(t & 15);
+  const float* src = S + (size_t)((k + 1) * TB + r) * ld + (size_t)k * TB + 8 * h;
+  const float4 a = *reinterpret_cast<const float4*>(src);
+  const float4 b = *reinterpret_cast<const float4*>(src + 4);
+  const float x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+  __align__(16) __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    hi[i] = __float2bfloat16_rn(x[i]);
+    lo[i] = __float2bfloat16_rn(x[i] - __bfloat162float(hi[i]));
+  }
+  const int tile = r / TB, rr = r % TB, g = rr >> 3, ri = rr & 7;
+  const size_t off = (size_t)tile * kPackTile + (size_t)((16 * g + h) * 128 + ri * 16);
+  *reinterpret_cast<uint4*>(pack + off) = *reinterpret_cast<const uint4*>(hi);
+  *reinterpret_cast<uint4*>(pack + off + kTileBytes) = *reinterpret_cast<const uint4*>(lo);
+}
+
+// ---------------------------------------------------------------------------
+// 256 threads.  K = 128 in two chunks of 64 through one 64 KB operand buffer
+// (A hi, A lo, B hi, B lo: 16 KB each), so three CTAs fit on an SM and
+// overlap each other's copies, MMAs and epilogues.  The accumulator is
+// staged through shared memory so the read-modify-write of the FP32 C tile
+// is coalesced (a warp covers a 512-byte row).
+constexpr int kChunkK = 64;
+constexpr int kChunkTile = TB * kChunkK * 2;  // 16 KB: one operand half-tile
+constexpr int kStageLd = TB + 4;              // floats per staged accumulator row
+constexpr int kSmemBytes = TB * kStageLd * 4;  // 67,584 B >= 4 * 16 KB operands
+
+__global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int ld, int k, int t0, int nt,
+                                                      const uint8_t* __restrict__ pack,
+                                                      const int* __restrict__ active, int* __restrict__ status) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ __align__(8) uint64_t bar_load[2], bar_mma[2];
+  __shared__ uint32_t tmem_base;
+  __shared__ int ok_s;
+  if (active && !*active) return;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int q = blockIdx.x;
+  int I = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
+  while ((I + 1) * (I + 2) / 2 <= q) I++;
+  while (I * (I + 1) / 2 > q) I--;
+  const int J = q - I * (I + 1) / 2;
+  const bool diag = I == J;
+  const uint8_t* pa = pack + (size_t)(t0 + I - (k + 1)) * kPackTile;
+  const uint8_t* pb = pack + (size_t)(t0 + J - (k + 1)) * kPackTile;
+  uint8_t* sAh = smem;
+  uint8_t* sAl = smem + kChunkTile;
+  uint8_t* sBh = diag ? sAh : smem + 2 * kChunkTile;
+  uint8_t* sBl = diag ? sAl : smem + 3 * kChunkTile;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(TB));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    mbar_init(&bar_load[0], 1);
+    mbar_init(&bar_load[1], 1);
+    mbar_init(&bar_mma[0], 1);
+    mbar_init(&bar_mma[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem_d = tmem_base;
+
+  if (tid == 0) {
+    int ok = 1;
+    for (int c = 0; c < 2 && ok; c++) {
+      // a packed tile holds core matrices (g, h) at (16 g + h) * 128; chunk c
+      // covers h = 8c .. 8c + 7, copied as 16 rows of 8 core matrices (1 KB each)
+      const uint32_t bytes = (diag ? 2 : 4) * kChunkTile;
+      mbar_expect_tx(&bar_load[c], bytes);
+      for (int g = 0; g < 16; g++) {
+        const size_t src = (size_t)(16 * g + 8 * c) * 128;
+        const size_t dst = (size_t)g * 1024;
+        bulk_g2s(sAh + dst, pa + src, 1024, &bar_load[c]);
+        bulk_g2s(sAl + dst, pa + kTileBytes + src, 1024, &bar_load[c]);
+        if (!diag) {
+          bulk_g2s(sBh + dst, pb + src, 1024, &bar_load[c]);
+          bulk_g2s(sBl + dst, pb + kTileBytes + src, 1024, &bar_load[c]);
+        }
+      }
+      if (!mbar_wait(&bar_load[c], 0)) {
+        ok = 0;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      // chunk layout: core (g, h') at (8 g + h') * 128 -> LBO 128 B, SBO 1024 B
+      const uint8_t* as[3] = {sAh, sAh, sAl};
+      const uint8_t* bs[3] = {sBh, sBl, sBh};
+#pragma unroll
+      for (int p = 0; p < 3; p++) {
+#pragma unroll
+        for (int s2 = 0; s2 < kChunkK / 16; s2++) {
+          const uint64_t da = umma_desc(as[p] + s2 * 256, 128, 1024);
+          const uint64_t db = umma_desc(bs[p] + s2 * 256, 128, 1024);
+          umma_bf16(tmem_d, da, db, (c > 0 || p > 0 || s2 > 0) ? 1u : 0u);
+        }
+      }
+      umma_commit(&bar_mma[c]);
+      // the operand buffer is reused by the next chunk: wait for these MMAs
+      if (!mbar_wait(&bar_mma[c], 0)) ok = 0;
+    }
+    ok_s = ok;
+    if (!ok) atomicOr(status, ST_SPIN_TIMEOUT);
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const int ok = ok_s;
+  float* stage = reinterpret_cast<float*>(smem);  // operands are consumed: reuse
+  if (ok) {
+    // warps w and w + 4 share TMEM lanes 32 (w % 4) ..; they split the columns
+    const int row = 32 * (warp & 3) + lane;
+    const int cbase = 64 * (warp >> 2);
+#pragma unroll 1
+    for (int c = 0; c < 2; c++) {
+      float d[32];
+      tmem_ld32(tmem_d + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(cbase + 32 * c), d);
+      float4* dst = reinterpret_cast<float4*>(stage + row * kStageLd + cbase + 32 * c);
+#pragma unroll
+      for (int i = 0; i < 8; i++) dst[i] = make_float4(d[4 * i], d[4 * i + 1], d[4 * i + 2], d[4 * i + 3]);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(TB));
+  }
+  if (ok) {
+    // coalesced read-modify-write: warp w takes rows w, w + 8, ...; lane = 4 columns
+    float* base = S + (size_t)((t0 + I) * TB) * ld + (size_t)(t0 + J) * TB + 4 * lane;
+#pragma unroll 4
+    for (int r = warp; r < TB; r += 8) {
+      float4 v = *reinterpret_cast<float4*>(base + (size_t)r * ld);
+      const float4 dd = *reinterpret_cast<const float4*>(stage + r * kStageLd + 4 * lane);
+      const int col = 4 * lane;
+      if (!diag || col + 0 <= r) v.x -= dd.x;
+      if (!diag || col + 1 <= r) v.y -= dd.y;
+      if (!diag || col + 2 <= r) v.z -= dd.z;
+      if (!diag || col + 3 <= r) v.w -= dd.w;
+      *reinterpret_cast<float4*>(base + (size_t)r * ld) = v;
+    }
+  }
+}
+
+}  // namespace
+
+size_t tc_syrk_scratch_bytes(int n_pad) { return (size_t)(n_pad / TB + 1) * kPackTile; }
+
+cudaError_t tc_syrk_f32(float* S, int ld, int k, int t0, int nt, void* scratch, const int* active, int* status,
+                        cudaStream_t st) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(tc_syrk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  const int nrows = nt * TB;  // rows of the trailing part (t0 == k + 1)
+  const long long nthr = (long long)nrows * 16;
+  tc_pack_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>(S, ld, k, nrows, static_cast<uint8_t*>(scratch),
+                                                                  active);
+  tc_syrk_kernel<<<nt * (nt + 1) / 2, 256, kSmemBytes, st>>>(S, ld, k, t0, nt,
+                                                                  static_cast<const uint8_t*>(scratch), active,
+                                                                  status);
+  return cudaGetLastError();
 }
 
 }  // namespace nl

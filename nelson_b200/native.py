@@ -80,7 +80,8 @@ EXPORTS = [
     "nl_compute_increment", "nl_get_increment", "nl_inc_sqnorm", "nl_get_schur", "nl_oplus", "nl_backup",
     "nl_rollback", "nl_max_abs_b", "nl_chi2", "nl_rho", "nl_lm_solve", "nl_gn_solve", "nl_phase_timings",
     "nl_kernel_launches", "nl_solver_create", "nl_solver_destroy", "nl_solver_set_hessian",
-    "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_status_string", "nl_version",
+    "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_selftest_tc_update", "nl_status_string",
+    "nl_version",
 ]
 
 _lib = None
@@ -111,6 +112,7 @@ def load(build_if_missing: bool = True):
     L.nl_gn_solve.argtypes = [vp, C.POINTER(GNSettings), C.POINTER(SolveReport), vp, i]
     L.nl_solver_create.argtypes = [C.POINTER(SolverDesc), vp, vp, vp, C.POINTER(vp)]
     L.nl_solver_compute_increment.argtypes = [vp, d, d, vp, vp, C.POINTER(i)]
+    L.nl_selftest_tc_update.argtypes = [i, C.c_ulonglong, i, C.POINTER(d)]
     for name in EXPORTS:  # fails loudly if the library lacks an entry point
         if name not in ("nl_status_string", "nl_version"):
             getattr(L, name).restype = C.c_int
@@ -305,3 +307,11 @@ class BAProblemGPU:
         v = C.c_longlong()
         self._c(self.L.nl_kernel_launches(self.h, C.byref(v)), "nl_kernel_launches")
         return v.value
+
+
+def selftest_tc_update(ntiles=8, seed=1, device=0) -> float:
+    """Max relative difference between the tensor-core and CUDA-core trailing updates."""
+    L = load()
+    err = C.c_double()
+    _chk(L, L.nl_selftest_tc_update(ntiles, seed, device, C.byref(err)), "nl_selftest_tc_update")
+    return err.value

@@ -109,7 +109,7 @@ def test_lm_trace_matches_oracle(Orc, cfg, scale, prec):
     # final parameters
     cu_o, pt_o = o.get_params()
     cu_g, pt_g = g.get_params()
-    assert rel(pt_g, pt_o) < (1e-8 if prec == N.PREC_FP64 else 1e-3)
+    assert rel(pt_g, pt_o) < (1e-6 if prec == N.PREC_FP64 else 1e-3)  # gauge-free problem
     g.close()
 
 

@@ -43,9 +43,9 @@ template <typename T>
 static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S, int ld, int k,
                                                                 double* __restrict__ Linv, int* __restrict__ status,
                                                                 const int* __restrict__ active) {
-  __shared__ double Lcol[NB][4];   // L of block column jb, rows >= 4 jb
-  __shared__ double Xrow[4][NB];   // X of block row jb, columns <= 4 jb + 3
-  __shared__ double Di[4][4];      // inv(L_jb,jb)
+  __shared__ double Lcol[2][NB][4];  // L of block column jb, rows >= 4 jb (double-buffered)
+  __shared__ double Xrow[2][4][NB];  // X of block row jb, columns <= 4 jb + 3
+  __shared__ double Di[2][4][4];     // inv(L_jb,jb)
   __shared__ int bad;
   if (active && !*active) return;
   const int tid = threadIdx.x;
@@ -70,23 +70,26 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
     }
   __syncthreads();
   for (int jb = 0; jb < NB / 4; jb++) {
-    // (1) factor + invert the diagonal 4x4 block
+    const int buf = jb & 1;
+    // (1) factor + invert the diagonal 4x4 block (one rsqrt per column,
+    //     multiplications only: Di[i][i] = 1 / L_ii is that rsqrt)
     if (own && R == jb && C == jb) {
       bool fail = false;
+      double rs[4];
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         double d = a[j][j];
 #pragma unroll
         for (int l = 0; l < j; l++) d -= a[j][l] * a[j][l];
         fail |= !(d > 0.0) || !isfinite(d);
-        const double p = sqrt(fmax(d, 1e-300));
-        a[j][j] = p;
+        rs[j] = rsqrt(fmax(d, 1e-300));
+        a[j][j] = d * rs[j];
 #pragma unroll
         for (int i = j + 1; i < 4; i++) {
           double v = a[i][j];
 #pragma unroll
           for (int l = 0; l < j; l++) v -= a[i][l] * a[j][l];
-          a[i][j] = v / p;
+          a[i][j] = v * rs[j];
         }
       }
       if (fail) bad = 1;
@@ -95,23 +98,25 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
       for (int c = 0; c < 4; c++)
 #pragma unroll
         for (int i = 0; i < 4; i++) {
-          double v = (i == c) ? 1.0 : 0.0;
+          if (i < c) {
+            di[i][c] = 0.0;
+          } else if (i == c) {
+            di[i][c] = rs[i];
+          } else {
+            double v = 0.0;
 #pragma unroll
-          for (int l = 0; l < i; l++) v -= a[i][l] * di[l][c];
-          di[i][c] = (i >= c) ? v / a[i][i] : 0.0;
+            for (int l = c; l < i; l++) v -= a[i][l] * di[l][c];
+            di[i][c] = v * rs[i];
+          }
         }
 #pragma unroll
       for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int c = 0; c < 4; c++) {
-          Di[i][c] = di[i][c];
-          if (c <= i) a[i][c] = a[i][c];
-          else a[i][c] = 0.0;
+          Di[buf][i][c] = di[i][c];
+          if (c > i) a[i][c] = 0.0;
+          Lcol[buf][r0 + i][c] = a[i][c];
         }
-#pragma unroll
-      for (int u = 0; u < 4; u++)
-#pragma unroll
-        for (int v = 0; v < 4; v++) Lcol[r0 + u][v] = a[u][v];
     }
     __syncthreads();
     // (2) block column jb of L, block row jb of X
@@ -123,13 +128,13 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
         for (int v = 0; v < 4; v++) {
           double s = 0.0;
 #pragma unroll
-          for (int w = 0; w <= v; w++) s += a[u][w] * Di[v][w];
+          for (int w = 0; w <= v; w++) s += a[u][w] * Di[buf][v][w];
           l[v] = s;
         }
 #pragma unroll
         for (int v = 0; v < 4; v++) {
           a[u][v] = l[v];
-          Lcol[r0 + u][v] = l[v];
+          Lcol[buf][r0 + u][v] = l[v];
         }
       }
     }
@@ -141,26 +146,26 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
         for (int u = 0; u < 4; u++) {
           double s = 0.0;
 #pragma unroll
-          for (int w = 0; w <= u; w++) s += Di[u][w] * x[w][v];
+          for (int w = 0; w <= u; w++) s += Di[buf][u][w] * x[w][v];
           xx[u] = s;
         }
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           x[u][v] = xx[u];
-          Xrow[u][c0 + v] = xx[u];
+          Xrow[buf][u][c0 + v] = xx[u];
         }
       }
     }
     __syncthreads();
-    // (3) updates
+    // (3) updates; the next step writes the other buffers, so no barrier here
     if (own && C > jb) {
 #pragma unroll
       for (int w = 0; w < 4; w++) {
         double lr[4], lc[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-          lr[u] = Lcol[r0 + u][w];
-          lc[u] = Lcol[c0 + u][w];
+          lr[u] = Lcol[buf][r0 + u][w];
+          lc[u] = Lcol[buf][c0 + u][w];
         }
 #pragma unroll
         for (int u = 0; u < 4; u++)
@@ -173,8 +178,8 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
         double lr[4], xr[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-          lr[u] = Lcol[r0 + u][w];
-          xr[u] = Xrow[w][c0 + u];
+          lr[u] = Lcol[buf][r0 + u][w];
+          xr[u] = Xrow[buf][w][c0 + u];
         }
 #pragma unroll
         for (int u = 0; u < 4; u++)
@@ -182,8 +187,8 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
           for (int v = 0; v < 4; v++) x[u][v] -= lr[u] * xr[v];
       }
     }
-    __syncthreads();
   }
+  __syncthreads();
   if (tid == 0 && bad) atomicOr(status, ST_CHOL_FAIL);
   double* out = Linv + (size_t)k * NB * NB;
   if (own) {

@@ -19,6 +19,8 @@
 //                    xV_p = Vinv_p (-bV_p - sum W' xU).
 #pragma once
 
+#include <type_traits>
+
 #include "nl_common.cuh"
 
 namespace nl {
@@ -137,18 +139,34 @@ static __global__ void __launch_bounds__(NT) wvinv_bs_kernel(SchurDev d, const T
 
 // ---------------------------------------------------------------------------
 // One warp per output block (i <= j); lanes own the BC*BC outputs round-robin.
-// Operands of up to PB pairs are staged in per-warp shared memory.
+// Batches of PB pairs: lane l < 2 np loads one block UID (Y_a for l < np,
+// W_b above), the operands move as 16-byte vectors (blocks are padded to 16
+// bytes) and are re-laid in shared memory with rows padded to 4, so each
+// 3-term row product reads two vectors.
+template <typename T>
+struct Vec4;
+template <>
+struct Vec4<float> {
+  using type = float4;
+};
+template <>
+struct Vec4<double> {
+  using type = double4;
+};
+
 template <typename T, int BC, int WARPS>
 static __global__ void __launch_bounds__(WARPS * 32) schur_kernel(SchurDev d, const T* __restrict__ U,
-                                                            const T* __restrict__ Y, const T* __restrict__ W,
-                                                            const double* __restrict__ lam, T* __restrict__ S,
-                                                            T* __restrict__ S0, const int* __restrict__ active) {
+                                                                   const T* __restrict__ Y, const T* __restrict__ W,
+                                                                   const double* __restrict__ lam, T* __restrict__ S,
+                                                                   T* __restrict__ S0, const int* __restrict__ active) {
   constexpr int LW = Layout<T, BC>::W;
   constexpr int LU = Layout<T, BC>::U;
-  constexpr int PB = 4;                     // pairs staged per step
-  constexpr int NO = (BC * BC + 31) / 32;   // outputs per lane
-  constexpr int OP = BC * 3;                // operand size
-  __shared__ T sh[WARPS][PB][2][OP + 1];
+  constexpr int PB = 8;                          // pairs per batch
+  constexpr int NO = (BC * BC + 31) / 32;        // outputs per lane
+  constexpr int EPV = 16 / (int)sizeof(T);       // elements per 16-byte vector
+  constexpr int VB = LW / EPV;                   // vectors per block
+  using V16 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  __shared__ __align__(16) T sh[WARPS][2][PB][BC][4];
   if (active && !*active) return;
   const double rel = lam[0], abs = lam[1];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -165,11 +183,34 @@ static __global__ void __launch_bounds__(WARPS * 32) schur_kernel(SchurDev d, co
     const long long p0 = d.s_pair_ptr[b], p1 = d.s_pair_ptr[b + 1];
     for (long long pp = p0; pp < p1; pp += PB) {
       const int np = (int)min((long long)PB, p1 - pp);
-      // stage operands: Y[a] and W[b] of np pairs
-      for (int t = lane; t < np * 2 * OP; t += 32) {
-        const int q = t / (2 * OP), rem = t - q * 2 * OP, which = rem / OP, e = rem - which * OP;
-        const int uid = which == 0 ? d.pair_a[pp + q] : d.pair_b[pp + q];
-        sh[warp][q][which][e] = (which == 0 ? Y : W)[(size_t)uid * LW + e];
+      int uid = 0;
+      if (lane < np) uid = d.pair_a[pp + lane];
+      else if (lane < 2 * np) uid = d.pair_b[pp + lane - np];
+      // stage 2 np blocks of VB vectors each
+      V16 v[(2 * PB * VB + 31) / 32];
+#pragma unroll
+      for (int t = 0; t < (2 * PB * VB + 31) / 32; t++) {
+        const int u = lane + 32 * t;
+        const int blk = u / VB, part = u - blk * VB;
+        const int src_uid = __shfl_sync(0xffffffffu, uid, blk & 31);
+        if (blk < 2 * np) {
+          const T* base = (blk < np ? Y : W) + (size_t)src_uid * LW;
+          v[t] = *reinterpret_cast<const V16*>(base + part * EPV);
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < (2 * PB * VB + 31) / 32; t++) {
+        const int u = lane + 32 * t;
+        const int blk = u / VB, part = u - blk * VB;
+        if (blk < 2 * np) {
+          const int which = blk < np ? 0 : 1, q = blk < np ? blk : blk - np;
+          const T* e = reinterpret_cast<const T*>(&v[t]);
+#pragma unroll
+          for (int m = 0; m < EPV; m++) {
+            const int idx = part * EPV + m;  // element of the BC x 3 block
+            if (idx < BC * 3) sh[warp][which][q][idx / 3][idx % 3] = e[m];
+          }
+        }
       }
       __syncwarp();
 #pragma unroll
@@ -179,8 +220,8 @@ static __global__ void __launch_bounds__(WARPS * 32) schur_kernel(SchurDev d, co
           const int r = o / BC, cc = o - r * BC;
           T s = (T)0;
           for (int q = 0; q < np; q++) {
-            const T* ya = sh[warp][q][0] + r * 3;
-            const T* wb = sh[warp][q][1] + cc * 3;
+            const T* ya = sh[warp][0][q][r];
+            const T* wb = sh[warp][1][q][cc];
             s += ya[0] * wb[0] + ya[1] * wb[1] + ya[2] * wb[2];
           }
           acc[k] -= s;

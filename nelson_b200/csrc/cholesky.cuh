@@ -270,18 +270,35 @@ static __global__ void __launch_bounds__(256) trsm_kernel(T* __restrict__ S, int
 // C_IJ -= X_I X_J' with X = columns [k NB, (k+1) NB).  Used as the portable
 // reference of the tensor-core kernel and for small problems.
 template <typename T>
+__device__ inline void syrk_cc_tile(T* __restrict__ S, int ld, int k, int gI, int gJ);
+
+template <typename T>
 static __global__ void __launch_bounds__(256) syrk_cc_kernel(T* __restrict__ S, int ld, int k, int t0, int nt,
                                                       const int* __restrict__ active) {
-  constexpr int KC = 16;
-  __shared__ T As[KC][NB + 4];
-  __shared__ T Bs[KC][NB + 4];
   if (active && !*active) return;
   const int q = blockIdx.x;
   int I = (int)((sqrt(8.0 * q + 1.0) - 1.0) * 0.5);
   while ((I + 1) * (I + 2) / 2 <= q) I++;
   while (I * (I + 1) / 2 > q) I--;
   const int J = q - I * (I + 1) / 2;
-  const int rA = (t0 + I) * NB, rB = (t0 + J) * NB, kc = k * NB;
+  syrk_cc_tile<T>(S, ld, k, t0 + I, t0 + J);
+}
+
+// one output tile (gI, gJ), gI >= gJ
+template <typename T>
+static __global__ void __launch_bounds__(256) syrk_cc_tile_kernel(T* __restrict__ S, int ld, int k, int gI, int gJ,
+                                                                  const int* __restrict__ active) {
+  if (active && !*active) return;
+  syrk_cc_tile<T>(S, ld, k, gI, gJ);
+}
+
+template <typename T>
+__device__ inline void syrk_cc_tile(T* __restrict__ S, int ld, int k, int gI, int gJ) {
+  constexpr int KC = 16;
+  __shared__ T As[KC][NB + 4];
+  __shared__ T Bs[KC][NB + 4];
+  const int I = gI, J = gJ;
+  const int rA = gI * NB, rB = gJ * NB, kc = k * NB;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   T acc[8][8];
 #pragma unroll

@@ -504,7 +504,12 @@ nl_status nl_create(const nl_problem_desc* d, nl_problem** out) {
   h->device = d->device;
   nl_status s;
   if ((s = select_device(h.get())) != NL_OK) return s;
-  NL_CUDA(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+  {
+    // the main stream carries the factorisation's critical path: highest priority
+    int lo = 0, hi = 0;
+    NL_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    NL_CUDA(cudaStreamCreateWithPriority(&h->st, cudaStreamNonBlocking, hi));
+  }
   NL_CUDA(cudaEventCreateWithFlags(&h->ev_a, cudaEventDisableTiming));
   NL_CUDA(cudaEventCreateWithFlags(&h->ev_b, cudaEventDisableTiming));
   NL_CUDA(cudaEventCreate(&h->ev_t0));
@@ -911,7 +916,11 @@ nl_status nl_solver_create(const nl_solver_desc* d, const int* u_rc, const int* 
   std::unique_ptr<nl_solver> s(new nl_solver());
   s->d = *d;
   NL_CUDA(cudaSetDevice(d->device));
-  NL_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  {
+    int lo = 0, hi = 0;
+    NL_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    NL_CUDA(cudaStreamCreateWithPriority(&s->st, cudaStreamNonBlocking, hi));
+  }
   if (d->precision == NL_PREC_FP64) {
     if (cublasCreate(&s->cublas) != CUBLAS_STATUS_SUCCESS) return NL_ERR_CUDA;
     cublasSetStream(s->cublas, s->st);

@@ -128,7 +128,10 @@ class SchurCoreT final : public SchurCore {
     NL_TRY(S_.alloc(sizeof(T) * (size_t)ld_ * ld_));
     need_s0_ = refine_sweeps > 0 || keep_schur;
     if (need_s0_) NL_TRY(S0_.alloc(sizeof(T) * (size_t)ld_ * ld_));
-    if (sizeof(T) == 4 && use_tc) NL_TRY(tcs_.alloc(tc_syrk_scratch_bytes(ld_)));
+    if (sizeof(T) == 4 && use_tc) {
+      tcs_half_ = (tc_syrk_scratch_bytes(ld_) + 255) / 256 * 256;
+      NL_TRY(tcs_.alloc(2 * tcs_half_));
+    }
     NL_TRY(upload(v_uid_, st.v_uid, st_));
     NL_TRY(upload(w_row_ptr_, w_row_ptr, st_));
     NL_TRY(upload(w_col_, st.w_c, st_));
@@ -179,6 +182,21 @@ class SchurCoreT final : public SchurCore {
     NL_CUDA(cudaFuncSetAttribute(trsv_bwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsvSmem));
     if (!ev_[0]) {
       for (auto& e : ev_) NL_CUDA(cudaEventCreate(&e));
+      NL_CUDA(cudaEventCreateWithFlags(&ev_panel_, cudaEventDisableTiming));
+      NL_CUDA(cudaEventCreateWithFlags(&ev_b_, cudaEventDisableTiming));
+      {
+        // the side stream (bulk trailing updates) yields SMs to the critical path
+        int lo = 0, hi = 0;
+        NL_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        NL_CUDA(cudaStreamCreateWithPriority(&st2_, cudaStreamNonBlocking, lo));
+      }
+      if (cublas_) {
+        if (cublasCreate(&cublas2_) != CUBLAS_STATUS_SUCCESS) return NL_ERR_CUDA;
+        nl_status ws = ws2_.alloc(64u << 20);
+        if (ws != NL_OK) return ws;
+        cublasSetWorkspace(cublas2_, ws2_.p, ws2_.bytes);
+        cublasSetStream(cublas2_, st2_);
+      }
     }
     return NL_OK;
   }
@@ -195,55 +213,122 @@ class SchurCoreT final : public SchurCore {
     return NL_OK;
   }
 
+  // Right-looking blocked Cholesky with look-ahead.  After panel k is
+  // factored (diagonal tile + TRSM below it), its trailing update is split:
+  //   update A(k): block column k+1 (tiles (I, k+1), I >= k+1), main stream;
+  //   update B(k): the triangle of tiles >= k+2, side stream,
+  // so the factorisation of panel k+1 (which needs only A(k)) overlaps B(k).
+  // A(k) waits for B(k-1) (both touch block column k+1); B(k) follows B(k-1)
+  // on the side stream and waits for panel k.  The BF16 pack of panel k is
+  // double-buffered.
+  nl_status launch_update(int k, int t0, int nt, bool col_only, cudaStream_t st, int* status, const int* active) {
+    if (nt <= 0) return NL_OK;
+    if (sizeof(T) == 8 && precision_ == NL_PREC_FP64 && cublas_) {
+      // Row-major lower storage = column-major upper.  X = rows >= r0 of
+      // panel k; the column-major view of S is M(a, b) = S[b][a].
+      double* Sd = reinterpret_cast<double*>(S_.p);
+      const double alpha = -1.0, beta = 1.0;
+      const size_t r0 = (size_t)t0 * NB, kc = (size_t)k * NB;
+      const int n_rem = ld_ - (int)r0;
+      // each stream has its own handle (and workspace)
+      cublasHandle_t hb = (st == st_) ? cublas_ : cublas2_;
+      if (cublasSetStream(hb, st) != CUBLAS_STATUS_SUCCESS) return NL_ERR_CUDA;
+      if (col_only) {
+        // M(c0.., r0..) -= Pc' Pr : C (128 x n_rem) with A = M(kc.., c0..), B = M(kc.., r0..)
+        if (cublasDgemm(hb, CUBLAS_OP_T, CUBLAS_OP_N, NB, n_rem, NB, &alpha, Sd + r0 * ld_ + kc, ld_,
+                        Sd + r0 * ld_ + kc, ld_, &beta, Sd + r0 * ld_ + r0, ld_) != CUBLAS_STATUS_SUCCESS)
+          return NL_ERR_CUDA;
+      } else {
+        if (cublasDsyrk(hb, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, n_rem, NB, &alpha, Sd + r0 * ld_ + kc, ld_,
+                        &beta, Sd + r0 * ld_ + r0, ld_) != CUBLAS_STATUS_SUCCESS)
+          return NL_ERR_CUDA;
+      }
+    } else if (sizeof(T) == 4 && use_tc) {
+      NL_CUDA(tc_update_f32(reinterpret_cast<float*>(S_.p), ld_, k, t0, nt, col_only ? 1 : 0,
+                            static_cast<uint8_t*>(tcs_.p) + (size_t)(k & 1) * tcs_half_, active, status, st));
+      launches++;
+    } else {
+      if (col_only) {
+        // column block as a triangle of 1 plus rows below: reuse the tile kernel per row tile
+        for (int I = 0; I < nt; I++)
+          syrk_cc_tile_kernel<T><<<1, 256, 0, st>>>(S_.as<T>(), ld_, k, t0 + I, t0, active);
+        launches += nt;
+      } else {
+        syrk_cc_kernel<T><<<nt * (nt + 1) / 2, 256, 0, st>>>(S_.as<T>(), ld_, k, t0, nt, active);
+        launches++;
+      }
+    }
+    return NL_OK;
+  }
+
+  nl_status factor_panel(int k, int* status, const int* active) {
+    potrf_diag_kernel<T><<<1, PT, kPotrfSmem, st_>>>(S_.as<T>(), ld_, k, Linv_.as<double>(), status, active);
+    launches++;
+    const int below = ld_ - (k + 1) * NB;
+    if (below > 0) {
+      trsm_kernel<T><<<cdiv(below, TRSM_ROWS), 256, trsm_smem<T>(), st_>>>(S_.as<T>(), ld_, k, below,
+                                                                            Linv_.as<double>(), active);
+      launches++;
+      if (sizeof(T) == 4 && use_tc) {
+        NL_CUDA(tc_pack_f32(reinterpret_cast<const float*>(S_.p), ld_, k, below,
+                            static_cast<uint8_t*>(tcs_.p) + (size_t)(k & 1) * tcs_half_, active, st_));
+        launches++;
+      }
+    }
+    return NL_OK;
+  }
+
   nl_status enqueue_factor(int* status, const int* active) {
     const bool tm = timing && !active;
-    if (tm && (int)upd_ev_.size() < 2 * ntiles_) {
-      for (size_t i = upd_ev_.size(); i < (size_t)2 * ntiles_; i++) {
+    if (tm && (int)upd_ev_.size() < 4 * ntiles_) {
+      for (size_t i = upd_ev_.size(); i < (size_t)4 * ntiles_; i++) {
         cudaEvent_t e;
         NL_CUDA(cudaEventCreate(&e));
         upd_ev_.push_back(e);
       }
     }
-    int nupd = 0;
     double upd_flop = 0;
-    for (int k = 0; k < ntiles_; k++) {
-      potrf_diag_kernel<T><<<1, PT, kPotrfSmem, st_>>>(S_.as<T>(), ld_, k, Linv_.as<double>(), status, active);
-      launches++;
+    nl_status r;
+    if ((r = factor_panel(0, status, active)) != NL_OK) return r;
+    bool pending_b = false;
+    for (int k = 0; k + 1 < ntiles_; k++) {
       const int below = ld_ - (k + 1) * NB;
-      if (below <= 0) break;
-      trsm_kernel<T><<<cdiv(below, TRSM_ROWS), 256, trsm_smem<T>(), st_>>>(S_.as<T>(), ld_, k, below,
-                                                                            Linv_.as<double>(), active);
-      launches++;
-      const int t0 = k + 1, nt = ntiles_ - t0;
-      if (tm) NL_CUDA(cudaEventRecord(upd_ev_[2 * nupd], st_));
-      upd_flop += (double)NB * below * (below + 1);  // 2 * NB * below (below + 1) / 2
-      if (sizeof(T) == 8 && precision_ == NL_PREC_FP64 && cublas_) {
-        // FP64 comparison path: cuBLAS DSYRK on the trailing matrix.  Row-major
-        // lower storage is column-major upper; the panel X (below x NB, row-major)
-        // is the column-major NB x below matrix A, and C -= A' A.
-        const double alpha = -1.0, beta = 1.0;
-        double* Sd = reinterpret_cast<double*>(S_.p);
-        const size_t r0 = (size_t)t0 * NB;
-        if (cublasDsyrk(cublas_, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, below, NB, &alpha, Sd + r0 * ld_ + (size_t)k * NB,
-                        ld_, &beta, Sd + r0 * ld_ + r0, ld_) != CUBLAS_STATUS_SUCCESS)
-          return NL_ERR_CUDA;
-      } else if (sizeof(T) == 4 && use_tc) {
-        NL_CUDA(tc_syrk_f32(reinterpret_cast<float*>(S_.p), ld_, k, t0, nt, tcs_.p, active, status, st_));
-        launches += 2;
+      upd_flop += (double)NB * below * (below + 1);
+      // panel k is factored and packed
+      NL_CUDA(cudaEventRecord(ev_panel_, st_));
+      // A(k): block column k+1, after B(k-1)
+      if (pending_b) NL_CUDA(cudaStreamWaitEvent(st_, ev_b_, 0));
+      if (tm) NL_CUDA(cudaEventRecord(upd_ev_[4 * k], st_));
+      if ((r = launch_update(k, k + 1, ntiles_ - k - 1, true, st_, status, active)) != NL_OK) return r;
+      if (tm) NL_CUDA(cudaEventRecord(upd_ev_[4 * k + 1], st_));
+      // B(k): tiles >= k+2 on the side stream
+      if (k + 2 < ntiles_) {
+        NL_CUDA(cudaStreamWaitEvent(st2_, ev_panel_, 0));
+        if (tm) NL_CUDA(cudaEventRecord(upd_ev_[4 * k + 2], st2_));
+        if ((r = launch_update(k, k + 2, ntiles_ - k - 2, false, st2_, status, active)) != NL_OK) return r;
+        if (tm) NL_CUDA(cudaEventRecord(upd_ev_[4 * k + 3], st2_));
+        NL_CUDA(cudaEventRecord(ev_b_, st2_));
+        pending_b = true;
       } else {
-        syrk_cc_kernel<T><<<nt * (nt + 1) / 2, 256, 0, st_>>>(S_.as<T>(), ld_, k, t0, nt, active);
-        launches++;
+        pending_b = false;
       }
-      if (tm) NL_CUDA(cudaEventRecord(upd_ev_[2 * nupd + 1], st_));
-      nupd++;
+      if ((r = factor_panel(k + 1, status, active)) != NL_OK) return r;
     }
+    if (pending_b) NL_CUDA(cudaStreamWaitEvent(st_, ev_b_, 0));
+    if (cublas_) cublasSetStream(cublas_, st_);
     if (tm) {
-      NL_CUDA(cudaEventSynchronize(upd_ev_[2 * nupd - 1 < 0 ? 0 : 2 * nupd - 1]));
+      NL_CUDA(cudaStreamSynchronize(st_));
       float tot = 0;
-      for (int i = 0; i < nupd; i++) {
+      int nupd = 0;
+      for (int k = 0; k + 1 < ntiles_; k++) {
         float ms = 0;
-        cudaEventElapsedTime(&ms, upd_ev_[2 * i], upd_ev_[2 * i + 1]);
+        cudaEventElapsedTime(&ms, upd_ev_[4 * k], upd_ev_[4 * k + 1]);
         tot += ms;
+        if (k + 2 < ntiles_) {
+          cudaEventElapsedTime(&ms, upd_ev_[4 * k + 2], upd_ev_[4 * k + 3]);
+          tot += ms;
+        }
+        nupd++;
       }
       times.update_ms = tot;
       times.update_launches = nupd;
@@ -405,7 +490,26 @@ class SchurCoreT final : public SchurCore {
   DevBuf U_, V_, W_, Y_, Vinv_, bU_, bV_, bS_, incU_, incV_, y_, r_, dx_, part_, Linv_, flags_, S_, S0_, tcs_;
   DevBuf v_uid_, w_row_ptr_, w_col_, w_row_, w_col_ptr_, w_col_uid_, u_diag_, s_i_, s_j_, s_uuid_, s_ptr_, pa_, pb_;
   cudaEvent_t ev_[7] = {};
+  cudaEvent_t ev_panel_ = nullptr, ev_b_ = nullptr;
+  cudaStream_t st2_ = nullptr;  // side stream of the look-ahead factorisation
+  cublasHandle_t cublas2_ = nullptr;
+  DevBuf ws2_;
+  size_t tcs_half_ = 0;
   std::vector<cudaEvent_t> upd_ev_;
+
+ public:
+  ~SchurCoreT() override {
+    if (cublas2_) cublasDestroy(cublas2_);
+    if (st2_) {
+      cudaStreamSynchronize(st2_);
+      cudaStreamDestroy(st2_);
+    }
+    for (auto e : ev_)
+      if (e) cudaEventDestroy(e);
+    if (ev_panel_) cudaEventDestroy(ev_panel_);
+    if (ev_b_) cudaEventDestroy(ev_b_);
+    for (auto e : upd_ev_) cudaEventDestroy(e);
+  }
 };
 
 }  // namespace

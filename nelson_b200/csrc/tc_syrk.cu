@@ -161,7 +161,7 @@ constexpr int kStageLd = TB + 4;              // floats per staged accumulator r
 constexpr int kSmemBytes = TB * kStageLd * 4;  // 67,584 B >= 4 * 16 KB operands
 
 __global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int ld, int k, int t0, int nt,
-                                                      const uint8_t* __restrict__ pack,
+                                                      int col_only, const uint8_t* __restrict__ pack,
                                                       const int* __restrict__ active, int* __restrict__ status) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ __align__(8) uint64_t bar_load[2], bar_mma[2];
@@ -170,10 +170,16 @@ __global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int
   if (active && !*active) return;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int q = blockIdx.x;
-  int I = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
-  while ((I + 1) * (I + 2) / 2 <= q) I++;
-  while (I * (I + 1) / 2 > q) I--;
-  const int J = q - I * (I + 1) / 2;
+  int I, J;
+  if (col_only) {
+    I = q;
+    J = 0;
+  } else {
+    I = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
+    while ((I + 1) * (I + 2) / 2 <= q) I++;
+    while (I * (I + 1) / 2 > q) I--;
+    J = q - I * (I + 1) / 2;
+  }
   const bool diag = I == J;
   const uint8_t* pa = pack + (size_t)(t0 + I - (k + 1)) * kPackTile;
   const uint8_t* pb = pack + (size_t)(t0 + J - (k + 1)) * kPackTile;
@@ -283,22 +289,36 @@ __global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int
 
 size_t tc_syrk_scratch_bytes(int n_pad) { return (size_t)(n_pad / TB + 1) * kPackTile; }
 
-cudaError_t tc_syrk_f32(float* S, int ld, int k, int t0, int nt, void* scratch, const int* active, int* status,
-                        cudaStream_t st) {
-  static bool attr_set = false;
-  if (!attr_set) {
+cudaError_t tc_pack_f32(const float* S, int ld, int k, int nrows, void* pack, const int* active, cudaStream_t st) {
+  const long long nthr = (long long)nrows * 16;
+  if (nthr <= 0) return cudaSuccess;
+  tc_pack_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>(S, ld, k, nrows, static_cast<uint8_t*>(pack),
+                                                                  active);
+  return cudaGetLastError();
+}
+
+cudaError_t tc_update_f32(float* S, int ld, int k, int t0, int nt, int col_only, const void* pack,
+                          const int* active, int* status, cudaStream_t st) {
+  static int attr_dev = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
     cudaError_t e = cudaFuncSetAttribute(tc_syrk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
     if (e != cudaSuccess) return e;
-    attr_set = true;
+    attr_dev = dev;
   }
-  const int nrows = nt * TB;  // rows of the trailing part (t0 == k + 1)
-  const long long nthr = (long long)nrows * 16;
-  tc_pack_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>(S, ld, k, nrows, static_cast<uint8_t*>(scratch),
-                                                                  active);
-  tc_syrk_kernel<<<nt * (nt + 1) / 2, 256, kSmemBytes, st>>>(S, ld, k, t0, nt,
-                                                                  static_cast<const uint8_t*>(scratch), active,
-                                                                  status);
+  const int grid = col_only ? nt : nt * (nt + 1) / 2;
+  if (grid <= 0) return cudaSuccess;
+  tc_syrk_kernel<<<grid, 256, kSmemBytes, st>>>(S, ld, k, t0, nt, col_only, static_cast<const uint8_t*>(pack),
+                                                active, status);
   return cudaGetLastError();
+}
+
+cudaError_t tc_syrk_f32(float* S, int ld, int k, int t0, int nt, void* scratch, const int* active, int* status,
+                        cudaStream_t st) {
+  cudaError_t e = tc_pack_f32(S, ld, k, nt * TB, scratch, active, st);
+  if (e != cudaSuccess) return e;
+  return tc_update_f32(S, ld, k, t0, nt, 0, scratch, active, status, st);
 }
 
 }  // namespace nl

@@ -8,6 +8,13 @@ namespace nl {
 // the current panel split into BF16 hi/lo halves in UMMA canonical layout.
 size_t tc_syrk_scratch_bytes(int n_pad);
 
+// Pack rows (k+1)*128 .. (k+1)*128 + nrows - 1 of panel k into `pack`.
+cudaError_t tc_pack_f32(const float* S, int ld, int k, int nrows, void* pack, const int* active, cudaStream_t st);
+// Update with a packed panel: col_only = 1 updates tiles (t0 .. t0+nt-1, t0),
+// col_only = 0 the lower triangle of tiles t0 .. t0+nt-1.
+cudaError_t tc_update_f32(float* S, int ld, int k, int t0, int nt, int col_only, const void* pack,
+                          const int* active, int* status, cudaStream_t st);
+
 // S[I][J] -= X_I X_J' for the lower 128x128 tiles I >= J of the trailing
 // matrix (tiles t0 .. t0 + nt - 1), X = columns [k*128, (k+1)*128) of S
 // (FP32, row-major, leading dimension ld).  The product runs as three BF16

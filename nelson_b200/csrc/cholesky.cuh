@@ -209,13 +209,15 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
 }
 
 // ---------------------------------------------------------------------------
-// L_ik = A_ik inv(L_kk)' for 64-row slabs below the diagonal tile.  256
-// threads: row group g = tid / 64 (16 rows), columns p and 127 - p (balanced
-// against the triangular inverse).
+// L_ik = A_ik inv(L_kk)' for 64-row slabs below the diagonal tile, as a
+// register-tiled product: X (64 x 128) = A (64 x 128) Linv' (128 x 128).
+// 256 threads, thread (ty, tx) computes rows ty*4 .. ty*4+3 (ty < 16) and
+// columns tx + 16 j (tx < 16, j < 8); A and Linv are staged in shared memory
+// in the working precision, K-major, and read as broadcasts / strided rows.
 constexpr int TRSM_ROWS = 64;
 template <typename T>
 constexpr size_t trsm_smem() {
-  return sizeof(T) * ((size_t)NB * (NB + 1) + (size_t)TRSM_ROWS * NB);
+  return sizeof(T) * ((size_t)NB * (NB + 1) + (size_t)NB * (TRSM_ROWS + 1));
 }
 
 template <typename T>
@@ -223,8 +225,8 @@ static __global__ void __launch_bounds__(256) trsm_kernel(T* __restrict__ S, int
                                                           const double* __restrict__ Linv,
                                                           const int* __restrict__ active) {
   extern __shared__ unsigned char smraw[];
-  T* sL = reinterpret_cast<T*>(smraw);  // NB x (NB + 1), Linv in T
-  T* sX = sL + NB * (NB + 1);            // TRSM_ROWS x NB rows of A
+  T* sL = reinterpret_cast<T*>(smraw);      // sL[l][j] = Linv[j][l], (NB + 1) stride
+  T* sA = sL + NB * (NB + 1);               // sA[l][r] = A[r][l], (TRSM_ROWS + 1) stride
   if (active && !*active) return;
   const int tid = threadIdx.x;
   const int r0 = (k + 1) * NB + blockIdx.x * TRSM_ROWS;
@@ -232,35 +234,38 @@ static __global__ void __launch_bounds__(256) trsm_kernel(T* __restrict__ S, int
   if (nr <= 0) return;
   const double* Li = Linv + (size_t)k * NB * NB;
   for (int i = tid; i < NB * NB; i += 256) {
-    const int r = i / NB, c = i - r * NB;
-    sL[r * (NB + 1) + c] = (T)Li[i];
+    const int j = i / NB, l = i - j * NB;
+    sL[l * (NB + 1) + j] = (T)Li[i];
   }
   for (int i = tid; i < TRSM_ROWS * NB; i += 256) {
-    const int r = i / NB, c = i - r * NB;
-    sX[i] = r < nr ? S[(size_t)(r0 + r) * ld + (size_t)k * NB + c] : (T)0;
+    const int r = i / NB, l = i - r * NB;
+    sA[l * (TRSM_ROWS + 1) + r] = r < nr ? S[(size_t)(r0 + r) * ld + (size_t)k * NB + l] : (T)0;
   }
   __syncthreads();
-  const int g = tid >> 6, p = tid & 63;
-  const int j0 = p, j1 = NB - 1 - p;
-  T a0[16], a1[16];
+  const int ty = tid >> 4, tx = tid & 15;
+  T acc[4][8];
 #pragma unroll
-  for (int r = 0; r < 16; r++) a0[r] = a1[r] = (T)0;
-  for (int l = 0; l <= j1; l++) {
-    const T l0 = l <= j0 ? sL[j0 * (NB + 1) + l] : (T)0;
-    const T l1 = sL[j1 * (NB + 1) + l];
+  for (int u = 0; u < 4; u++)
 #pragma unroll
-    for (int r = 0; r < 16; r++) {
-      const T x = sX[(g * 16 + r) * NB + l];
-      a0[r] += x * l0;
-      a1[r] += x * l1;
-    }
+    for (int v = 0; v < 8; v++) acc[u][v] = (T)0;
+#pragma unroll 4
+  for (int l = 0; l < NB; l++) {
+    T a[4], b[8];
+#pragma unroll
+    for (int u = 0; u < 4; u++) a[u] = sA[l * (TRSM_ROWS + 1) + ty * 4 + u];
+#pragma unroll
+    for (int v = 0; v < 8; v++) b[v] = sL[l * (NB + 1) + tx + 16 * v];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int v = 0; v < 8; v++) acc[u][v] += a[u] * b[v];
   }
 #pragma unroll
-  for (int r = 0; r < 16; r++) {
-    const int rr = g * 16 + r;
+  for (int u = 0; u < 4; u++) {
+    const int rr = ty * 4 + u;
     if (rr < nr) {
-      S[(size_t)(r0 + rr) * ld + (size_t)k * NB + j0] = a0[r];
-      S[(size_t)(r0 + rr) * ld + (size_t)k * NB + j1] = a1[r];
+#pragma unroll
+      for (int v = 0; v < 8; v++) S[(size_t)(r0 + rr) * ld + (size_t)k * NB + tx + 16 * v] = acc[u][v];
     }
   }
 }

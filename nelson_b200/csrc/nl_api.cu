@@ -522,7 +522,7 @@ nl_status nl_create(const nl_problem_desc* d, nl_problem** out) {
   }
   h->core = make_schur_core(d->precision, d->bc, h->cublas);
   if (!h->core) return NL_ERR_UNSUPPORTED;
-  h->core->refine_sweeps = d->refine_sweeps >= 0 ? d->refine_sweeps : (d->precision == NL_PREC_MIXED ? 2 : 0);
+  h->core->refine_sweeps = d->refine_sweeps >= 0 ? d->refine_sweeps : (d->precision == NL_PREC_MIXED ? 1 : 0);
   h->core->keep_schur = (long long)d->nc_var * d->bc <= 4096 ? 1 : 0;
   h->core->use_tc = d->precision == NL_PREC_MIXED ? 1 : 0;
   const int nc_all = d->nc_var + d->nc_fix, np_all = d->np_var + d->np_fix;
@@ -930,7 +930,7 @@ nl_status nl_solver_create(const nl_solver_desc* d, const int* u_rc, const int* 
   }
   s->core = make_schur_core(d->precision, d->bu, s->cublas);
   if (!s->core) return NL_ERR_UNSUPPORTED;
-  s->core->refine_sweeps = d->refine_sweeps >= 0 ? d->refine_sweeps : (d->precision == NL_PREC_MIXED ? 2 : 0);
+  s->core->refine_sweeps = d->refine_sweeps >= 0 ? d->refine_sweeps : (d->precision == NL_PREC_MIXED ? 1 : 0);
   s->core->keep_schur = 0;
   s->core->use_tc = d->precision == NL_PREC_MIXED ? 1 : 0;
   SchurStructure ss;

@@ -188,6 +188,13 @@ __global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int
   uint8_t* sBh = diag ? sAh : smem + 2 * kChunkTile;
   uint8_t* sBl = diag ? sAl : smem + 3 * kChunkTile;
 
+  // start pulling the output tile into L2 now; the epilogue reads it last
+  {
+    const float* crow0 = S + (size_t)((t0 + I) * TB) * ld + (size_t)(t0 + J) * TB;
+    if (tid < TB)
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(crow0 + (size_t)tid * ld), "r"(TB * 4)
+                   : "memory");
+  }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
                  "r"(TB));

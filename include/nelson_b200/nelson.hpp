@@ -1,0 +1,448 @@
+// nelson.hpp -- header-only C++ classes over the C ABI of nelson_b200.h, in
+// the shapes nelson's own code uses, so that a nelson user swaps the solver
+// id and the section type and keeps the rest of the program:
+//
+//   nelson                                          nelson_b200
+//   DoubleSection<..., EdgeBinaryUV projection>     BASection
+//     (nelson/DoubleSection.h:24-330)
+//   SolverCholeskySchur (SolverCholeskySchur.h)     SolverCholeskySchurCuda
+//   LevenbergMarquardt<Solver> (LevenbergMarquardt.h/.hpp)
+//                                                   LevenbergMarquardt<Solver>
+//   GaussNewton<Solver> (GaussNewton.h/.hpp)        GaussNewton<Solver>
+//   LevenbergMarquardtSettings / GaussNewtonSettings  same names and defaults
+//
+// LevenbergMarquardt::solve / GaussNewton::solve below restate the
+// reference's control flow (nelson/LevenbergMarquardt.hpp:36-146,
+// nelson/GaussNewton.hpp:32-127) over the problem and solver concepts, one
+// C-ABI call per step; solveOnDevice() runs the same loop entirely on the GPU
+// (nl_lm_solve / nl_gn_solve) and is what a production caller uses.
+//
+// Errors: every failing C-ABI call throws nelson_b200::Error carrying the
+// nl_status.  A Cholesky failure of the reduced system is not an error: it is
+// the `false` return of computeIncrement, as in the reference.
+#ifndef NELSON_B200_NELSON_HPP
+#define NELSON_B200_NELSON_HPP
+
+#include <algorithm>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../nelson_b200.h"
+
+namespace nelson_b200 {
+
+class Error : public std::runtime_error {
+ public:
+  Error(nl_status s, const std::string& what)
+      : std::runtime_error(what + ": " + nl_status_string(s)), status_(s) {}
+  nl_status status() const { return status_; }
+
+ private:
+  nl_status status_;
+};
+
+inline void check(nl_status s, const char* what) {
+  if (s != NL_OK) throw Error(s, what);
+}
+
+// NodeType / NodeId (nelson/EdgeInterface.h:35-55): an id of a variable or of
+// a fixed parameter block.
+enum class NodeType { Variable, Fixed };
+struct NodeId {
+  int id = 0;
+  NodeType type = NodeType::Variable;
+  NodeId() = default;
+  explicit NodeId(int i, NodeType t = NodeType::Variable) : id(i), type(t) {}
+  static NodeId fixed(int i) { return NodeId(i, NodeType::Fixed); }
+};
+
+// nelson/LevenbergMarquardt.h:18-34, defaults nelson/LevenbergMarquardt.cpp:6-19.
+struct LevenbergMarquardtSettings {
+  int maxNumIt = 100;
+  int maxNumSubIt = 10;
+  int minNumIt = 0;
+  double epsBVector = 1e-15;
+  double epsIncSquare = 1e-30;
+  double epsChi2 = 1e-15;
+  double tau = 1e-3;
+  double penaltyV = 2.0;
+  double initV = 2.0;
+  double maxScaleFactor = 2.0 / 3.0;
+  double minScaleFactor = 1.0 / 3.0;
+  nl_lm_settings c() const {
+    return nl_lm_settings{maxNumIt, maxNumSubIt, minNumIt, epsBVector, epsIncSquare, epsChi2,
+                          tau, penaltyV, initV, maxScaleFactor, minScaleFactor};
+  }
+};
+
+// nelson/GaussNewton.h:18-30, defaults nelson/GaussNewton.cpp:12-22.
+struct GaussNewtonSettings {
+  int maxNumIt = 100;
+  int minNumIt = 0;
+  double epsBVector = 1e-15;
+  double epsIncSquare = 1e-30;
+  double epsChi2 = 1e-15;
+  double absLambda = 0.0;
+  double relLambda = 0.0;
+  nl_gn_settings c() const {
+    return nl_gn_settings{maxNumIt, minNumIt, epsBVector, epsIncSquare, epsChi2, absLambda,
+                          relLambda};
+  }
+};
+
+// nelson/LevenbergMarquardt.h:36-44 (GaussNewton uses the first six).
+enum class TerminationReason {
+  SuccessAtStart = NL_SUCCESS_AT_START,
+  SuccessSmallIncrement = NL_SUCCESS_SMALL_INCREMENT,
+  SuccessEpsB = NL_SUCCESS_EPS_B,
+  SuccessSmallResiduals = NL_SUCCESS_SMALL_RESIDUALS,
+  SolverFailure = NL_SOLVER_FAILURE,
+  MaxIterationReached = NL_MAX_ITERATION_REACHED,
+  MaxSubIterationReached = NL_MAX_SUBITERATION_REACHED
+};
+
+// One record per sub-iteration (the content of LevenbergMarquardtStats,
+// nelson/LevenbergMarquardt.h:57-85, plus damping and gain ratio).
+struct IterationRecord {
+  int it, subit;
+  double chi2, mu, rho, incSquaredNorm;
+  bool solverOk, accepted;
+};
+
+// ---------------------------------------------------------------------------
+// BASection: a DoubleSection of cameras (U, 6 or 9 parameters) and points
+// (V, 3 parameters) joined by the projection EdgeBinaryUV, resident on one
+// GPU.  Call order as in the reference: construct (parametersReady), addEdge
+// ..., optionally setUser2InternalIndexesU, structureReady, then solve.
+class BASection {
+ public:
+  BASection(int bc, int numCameras, int numPoints, int numFixedCameras = 0,
+            int numFixedPoints = 0, int precision = NL_PREC_MIXED, double f = 500.0,
+            double cx = 320.0, double cy = 240.0, int device = 0, int refineSweeps = -1) {
+    nl_problem_desc d{};
+    d.bc = bc;
+    d.nc_var = numCameras;
+    d.nc_fix = numFixedCameras;
+    d.np_var = numPoints;
+    d.np_fix = numFixedPoints;
+    d.precision = precision;
+    d.f = f;
+    d.cx = cx;
+    d.cy = cy;
+    d.refine_sweeps = refineSweeps;
+    d.device = device;
+    check(nl_create(&d, &h_), "nl_create");
+    desc_ = d;
+  }
+  ~BASection() {
+    if (h_) nl_destroy(h_);
+  }
+  BASection(const BASection&) = delete;
+  BASection& operator=(const BASection&) = delete;
+  BASection(BASection&& o) noexcept : h_(std::exchange(o.h_, nullptr)), desc_(o.desc_) {}
+
+  nl_problem* handle() const { return h_; }
+  int cameraBlockSize() const { return desc_.bc; }
+  int numParametersU() const { return desc_.nc_var; }
+  int numParametersV() const { return desc_.np_var; }
+
+  // Cameras: axis-angle[3], t[3] (, f, k1, k2), variable cameras then fixed;
+  // points: xyz, variable then fixed.
+  void setParameters(const std::vector<double>& cams, const std::vector<double>& pts) {
+    const size_t nc = size_t(desc_.nc_var + desc_.nc_fix), np = size_t(desc_.np_var + desc_.np_fix);
+    if (cams.size() != nc * desc_.bc || pts.size() != np * 3)
+      throw Error(NL_ERR_ARG, "setParameters: sizes");
+    check(nl_set_params(h_, cams.data(), pts.data()), "nl_set_params");
+  }
+  void getParameters(std::vector<double>& cams, std::vector<double>& pts) const {
+    cams.resize(size_t(desc_.nc_var + desc_.nc_fix) * desc_.bc);
+    pts.resize(size_t(desc_.np_var + desc_.np_fix) * 3);
+    check(nl_get_params(h_, cams.data(), pts.data()), "nl_get_params");
+  }
+  // DoubleSection::parametersReady (nelson/DoubleSection.hpp:67-80): the
+  // parameter counts are fixed by the constructor; kept for call-order parity.
+  void parametersReady() {}
+
+  // DoubleSection::addEdge(NodeId, NodeId, EdgeBinaryUV*) (DoubleSection.hpp:338-365),
+  // with the projection edge given by its observation (and optional weight).
+  void addEdge(NodeId cam, NodeId pt, double u, double v, double weight = 1.0) {
+    cam_.push_back(cam.id);
+    camFixed_.push_back(cam.type == NodeType::Fixed);
+    pt_.push_back(pt.id);
+    ptFixed_.push_back(pt.type == NodeType::Fixed);
+    obs_.push_back(u);
+    obs_.push_back(v);
+    w_.push_back(weight);
+  }
+  // DoubleSection::setUser2InternalIndexesU (nelson/DoubleSection.hpp:23-27).
+  void setUser2InternalIndexesU(const std::vector<int>& perm) {
+    if (perm.size() != size_t(desc_.nc_var)) throw Error(NL_ERR_ARG, "setUser2InternalIndexesU");
+    check(nl_set_user2internal_u(h_, perm.data()), "nl_set_user2internal_u");
+  }
+  // DoubleSection::structureReady (nelson/DoubleSection.hpp:83-246).
+  void structureReady() {
+    const bool weighted = std::any_of(w_.begin(), w_.end(), [](double x) { return x != 1.0; });
+    check(nl_add_ba_edges(h_, int(cam_.size()), cam_.data(), camFixed_.data(), pt_.data(),
+                          ptFixed_.data(), obs_.data(), weighted ? w_.data() : nullptr),
+          "nl_add_ba_edges");
+    check(nl_structure_ready(h_), "nl_structure_ready");
+    std::vector<int>().swap(cam_);
+    std::vector<int>().swap(camFixed_);
+    std::vector<int>().swap(pt_);
+    std::vector<int>().swap(ptFixed_);
+    std::vector<double>().swap(obs_);
+    std::vector<double>().swap(w_);
+  }
+
+  // ---- the problem concept used by LevenbergMarquardt / GaussNewton ----
+  // DoubleSection::update(bool) (nelson/DoubleSection.hpp:452-467).
+  void update(bool computeHessian) {
+    double c;
+    check(nl_update(h_, computeHessian ? 1 : 0, &c), "nl_update");
+  }
+  // hessian().chi2() / hessian().maxAbsValBVect() (nelson/HessianBase.h).
+  class HessianView {
+   public:
+    explicit HessianView(nl_problem* h) : h_(h) {}
+    double chi2() const {
+      double c;
+      check(nl_chi2(h_, &c), "nl_chi2");
+      return c;
+    }
+    double maxAbsValBVect() const {
+      double b;
+      check(nl_max_abs_b(h_, &b), "nl_max_abs_b");
+      return b;
+    }
+
+   private:
+    nl_problem* h_;
+  };
+  HessianView hessian() const { return HessianView(h_); }
+  // oplus with the solver's increment vector (the increment stays on the device).
+  void oplus() { check(nl_oplus(h_), "nl_oplus"); }
+  void backupSolution() { check(nl_backup(h_), "nl_backup"); }
+  void rollbackSolution() { check(nl_rollback(h_), "nl_rollback"); }
+  // computeRhoChi2Change (nelson/DoubleSection.hpp:469-480), on the current
+  // increment: (oldChi2 - chi2) / (inc' (mu inc - b)).
+  double computeRhoChi2Change(double mu, double oldChi2) const {
+    double r;
+    check(nl_rho(h_, mu, oldChi2, &r), "nl_rho");
+    return r;
+  }
+
+ private:
+  nl_problem* h_ = nullptr;
+  nl_problem_desc desc_{};
+  std::vector<int> cam_, camFixed_, pt_, ptFixed_;
+  std::vector<double> obs_, w_;
+};
+
+// ---------------------------------------------------------------------------
+// The Solver concept (nelson/SolverCholeskySchur.h:96-115) on a BASection's
+// device-resident Hessian.
+class SolverCholeskySchurCuda {
+ public:
+  void init(BASection& p) {
+    p_ = &p;
+    check(nl_solver_init(p.handle()), "nl_solver_init");
+  }
+  double maxAbsHDiag() const {
+    double m;
+    check(nl_max_abs_hdiag(p_->handle(), &m), "nl_max_abs_hdiag");
+    return m;
+  }
+  // computeIncrement(H, b, relLambda, absLambda) (SolverCholeskySchur.hpp:91-157):
+  // false when a damped block or the reduced system is not positive definite
+  // (the increment is then zero).
+  bool computeIncrement(double relLambda, double absLambda) {
+    int ok = 0;
+    check(nl_compute_increment(p_->handle(), relLambda, absLambda, &ok), "nl_compute_increment");
+    return ok != 0;
+  }
+  double incrementVectorSquaredNorm() const {
+    double s;
+    check(nl_inc_sqnorm(p_->handle(), &s), "nl_inc_sqnorm");
+    return s;
+  }
+  void incrementVector(std::vector<double>& incU, std::vector<double>& incV) const {
+    incU.resize(size_t(p_->numParametersU()) * p_->cameraBlockSize());
+    incV.resize(size_t(p_->numParametersV()) * 3);
+    check(nl_get_increment(p_->handle(), incU.data(), incV.data()), "nl_get_increment");
+  }
+  nl_phase_times timeStats() const {
+    nl_phase_times t{};
+    check(nl_phase_timings(p_->handle(), &t), "nl_phase_timings");
+    return t;
+  }
+
+ private:
+  BASection* p_ = nullptr;
+};
+
+// ---------------------------------------------------------------------------
+// LevenbergMarquardt<Solver> (nelson/LevenbergMarquardt.h:46-118).
+template <class Solver = SolverCholeskySchurCuda>
+class LevenbergMarquardt {
+ public:
+  LevenbergMarquardtSettings& settings() { return settings_; }
+  const std::vector<IterationRecord>& stats() const { return stats_; }
+  int numIterations() const { return iter_; }
+  Solver& solver() { return solver_; }
+
+  // nelson/LevenbergMarquardt.hpp:36-146, one C-ABI call per step.
+  TerminationReason solve(BASection& P) {
+    const auto& s = settings_;
+    stats_.clear();
+    iter_ = -1;
+    solver_.init(P);
+    P.update(true);
+    push(-1, -1, P.hessian().chi2(), 0, 0, 0, true, true);
+    if (P.hessian().maxAbsValBVect() <= s.epsBVector) return TerminationReason::SuccessAtStart;
+    P.backupSolution();
+    double oldChi2 = P.hessian().chi2();
+    double mu = s.tau * solver_.maxAbsHDiag();
+    double v = s.initV;
+    iter_ = 0;
+    while (iter_ < s.maxNumIt) {
+      int subiter = 0;
+      bool repeat;
+      do {
+        const double muUsed = mu;
+        const bool ok = solver_.computeIncrement(0.0, mu);
+        const double inc = solver_.incrementVectorSquaredNorm();
+        if (ok && iter_ >= s.minNumIt && inc <= s.epsIncSquare) {
+          push(iter_, subiter, P.hessian().chi2(), muUsed, 0, inc, true, false);
+          return TerminationReason::SuccessSmallIncrement;
+        }
+        double rho = -1, chi2 = -1;
+        if (ok) {
+          P.oplus();
+          P.update(false);
+          chi2 = P.hessian().chi2();
+          rho = P.computeRhoChi2Change(mu, oldChi2);
+        }
+        const bool accepted = ok && rho > 0;
+        push(iter_, subiter, chi2, muUsed, rho, inc, ok, accepted);
+        if (accepted) {
+          if (iter_ > s.minNumIt && P.hessian().maxAbsValBVect() <= s.epsBVector)
+            return TerminationReason::SuccessEpsB;
+          if (iter_ > s.minNumIt && chi2 < s.epsChi2) return TerminationReason::SuccessSmallResiduals;
+          const double fc = 2 * rho - 1;
+          mu *= std::max(s.minScaleFactor, std::min(s.maxScaleFactor, 1 - fc * fc * fc));
+          v = s.initV;
+        } else {
+          P.rollbackSolution();
+          mu *= v;
+          v *= s.penaltyV;
+        }
+        ++subiter;
+        if (subiter >= s.maxNumSubIt) return TerminationReason::MaxSubIterationReached;
+        repeat = !accepted;
+      } while (repeat);
+      P.update(true);
+      P.backupSolution();
+      oldChi2 = P.hessian().chi2();
+      ++iter_;
+    }
+    return TerminationReason::MaxIterationReached;
+  }
+
+  // The same loop with every step on the device (nl_lm_solve).
+  TerminationReason solveOnDevice(BASection& P, nl_solve_report* report = nullptr) {
+    const nl_lm_settings c = settings_.c();
+    nl_solve_report rep{};
+    std::vector<double> tr(size_t(settings_.maxNumIt + 1) * (settings_.maxNumSubIt + 1) *
+                           NL_TRACE_STRIDE);
+    check(nl_lm_solve(P.handle(), &c, &rep, tr.data(), int(tr.size() / NL_TRACE_STRIDE)),
+          "nl_lm_solve");
+    stats_.clear();
+    for (int k = 0; k < rep.n_trace; k++) {
+      const double* t = &tr[size_t(k) * NL_TRACE_STRIDE];
+      stats_.push_back({int(t[0]), int(t[1]), t[2], t[3], t[4], t[5], t[6] != 0, t[7] != 0});
+    }
+    iter_ = rep.iterations;
+    if (report) *report = rep;
+    return TerminationReason(rep.reason);
+  }
+
+ private:
+  void push(int it, int sub, double chi2, double mu, double rho, double inc, bool ok, bool acc) {
+    stats_.push_back({it, sub, chi2, mu, rho, inc, ok, acc});
+  }
+  LevenbergMarquardtSettings settings_;
+  Solver solver_;
+  std::vector<IterationRecord> stats_;
+  int iter_ = -1;
+};
+
+// GaussNewton<Solver> (nelson/GaussNewton.h:43-96).
+template <class Solver = SolverCholeskySchurCuda>
+class GaussNewton {
+ public:
+  GaussNewtonSettings& settings() { return settings_; }
+  const std::vector<IterationRecord>& stats() const { return stats_; }
+  int numIterations() const { return iter_; }
+
+  // nelson/GaussNewton.hpp:32-127.
+  TerminationReason solve(BASection& P) {
+    const auto& s = settings_;
+    stats_.clear();
+    iter_ = -1;
+    solver_.init(P);
+    P.update(true);
+    stats_.push_back({-1, 0, P.hessian().chi2(), 0, 0, 0, true, true});
+    if (P.hessian().maxAbsValBVect() <= s.epsBVector) return TerminationReason::SuccessAtStart;
+    iter_ = 0;
+    while (iter_ < s.maxNumIt) {
+      const bool ok = solver_.computeIncrement(s.relLambda, s.absLambda);
+      const double inc = solver_.incrementVectorSquaredNorm();
+      if (!ok) {
+        stats_.push_back({iter_, 0, -1, 0, 0, inc, false, false});
+        return TerminationReason::SolverFailure;
+      }
+      if (iter_ >= s.minNumIt && inc <= s.epsIncSquare) {
+        stats_.push_back({iter_, 0, P.hessian().chi2(), 0, 0, inc, true, false});
+        return TerminationReason::SuccessSmallIncrement;
+      }
+      P.oplus();
+      P.update(true);
+      const double chi2 = P.hessian().chi2();
+      stats_.push_back({iter_, 0, chi2, 0, 0, inc, true, true});
+      if (iter_ > s.minNumIt && P.hessian().maxAbsValBVect() <= s.epsBVector)
+        return TerminationReason::SuccessEpsB;
+      if (iter_ > s.minNumIt && chi2 < s.epsChi2) return TerminationReason::SuccessSmallResiduals;
+      ++iter_;
+    }
+    return TerminationReason::MaxIterationReached;
+  }
+
+  TerminationReason solveOnDevice(BASection& P, nl_solve_report* report = nullptr) {
+    const nl_gn_settings c = settings_.c();
+    nl_solve_report rep{};
+    std::vector<double> tr(size_t(settings_.maxNumIt + 2) * NL_TRACE_STRIDE);
+    check(nl_gn_solve(P.handle(), &c, &rep, tr.data(), int(tr.size() / NL_TRACE_STRIDE)),
+          "nl_gn_solve");
+    stats_.clear();
+    for (int k = 0; k < rep.n_trace; k++) {
+      const double* t = &tr[size_t(k) * NL_TRACE_STRIDE];
+      stats_.push_back({int(t[0]), int(t[1]), t[2], t[3], t[4], t[5], t[6] != 0, t[7] != 0});
+    }
+    iter_ = rep.iterations;
+    if (report) *report = rep;
+    return TerminationReason(rep.reason);
+  }
+
+ private:
+  GaussNewtonSettings settings_;
+  Solver solver_;
+  std::vector<IterationRecord> stats_;
+  int iter_ = -1;
+};
+
+}  // namespace nelson_b200
+
+#endif

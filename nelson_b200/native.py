@@ -315,3 +315,50 @@ def selftest_tc_update(ntiles=8, seed=1, device=0) -> float:
     err = C.c_double()
     _chk(L, L.nl_selftest_tc_update(ntiles, seed, device, C.byref(err)), "nl_selftest_tc_update")
     return err.value
+
+
+class SchurSolverGPU:
+    """Solver-only drop-in: SolverCholeskySchur on a Hessian assembled by the
+    caller (U any pattern in upper CSC order, V block diagonal 3x3, W CSR),
+    i.e. init / maxAbsHDiag / computeIncrement of nelson/SolverCholeskySchur.hpp:44-157."""
+
+    def __init__(self, bu, nu, nv, u_rc, v_rc, w_rc, precision=PREC_FP64, refine_sweeps=-1, device=0):
+        self.L = load()
+        self.bu, self.nu, self.nv = bu, nu, nv
+        u_rc = np.ascontiguousarray(u_rc, np.int32).reshape(-1, 2)
+        v_rc = np.ascontiguousarray(v_rc, np.int32).reshape(-1, 2)
+        w_rc = np.ascontiguousarray(w_rc, np.int32).reshape(-1, 2)
+        d = SolverDesc(bu=bu, nu=nu, nv=nv, nU=len(u_rc), nV=len(v_rc), nW=len(w_rc), precision=precision,
+                       refine_sweeps=refine_sweeps, device=device)
+        h = C.c_void_p()
+        _chk(self.L, self.L.nl_solver_create(C.byref(d), _p(u_rc), _p(v_rc), _p(w_rc), C.byref(h)),
+             "nl_solver_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.nl_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_hessian(self, U, V, W, bU, bV):
+        a = [np.ascontiguousarray(x, np.float64) for x in (U, V, W, bU, bV)]
+        _chk(self.L, self.L.nl_solver_set_hessian(self.h, *[_p(x) for x in a]), "nl_solver_set_hessian")
+
+    def max_abs_hdiag(self):
+        v = C.c_double()
+        _chk(self.L, self.L.nl_solver_max_abs_hdiag(self.h, C.byref(v)), "nl_solver_max_abs_hdiag")
+        return v.value
+
+    def compute_increment(self, rel, abs_):
+        du = np.zeros(self.nu * self.bu)
+        dv = np.zeros(self.nv * 3)
+        ok = C.c_int()
+        _chk(self.L, self.L.nl_solver_compute_increment(self.h, rel, abs_, _p(du), _p(dv), C.byref(ok)),
+             "nl_solver_compute_increment")
+        return bool(ok.value), du, dv

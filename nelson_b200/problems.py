@@ -312,3 +312,19 @@ def add_uniform_noise(lp: LinearProblem, sigma: float, rng) -> None:
     parameters (testDoubleSectionSchurCommon.h:347-354)."""
     lp.u[:lp.nu_var] += rng.uniform(-sigma, sigma, size=(lp.nu_var, lp.bu))
     lp.v[:lp.nv_var] += rng.uniform(-sigma, sigma, size=(lp.nv_var, lp.bv))
+
+
+def with_fixed_nodes(p: BAProblem, ncf: int, npf: int = 0) -> BAProblem:
+    """The last `ncf` cameras and `npf` points become fixed nodes
+    (NodeType::Fixed): parameters keep their order (variable blocks first,
+    then fixed), edges refer to fixed blocks by their index among the fixed
+    ones.  Holding two cameras fixed removes the similarity gauge of BA."""
+    ncv, npv = p.nc_var - ncf, p.np_var - npf
+    cf = (p.cam_idx >= ncv).astype(np.int32)
+    pf = (p.pt_idx >= npv).astype(np.int32)
+    return BAProblem(bc=p.bc, cams=p.cams, pts=p.pts, nc_var=ncv, np_var=npv,
+                     cam_idx=np.where(cf == 1, p.cam_idx - ncv, p.cam_idx).astype(np.int32),
+                     pt_idx=np.where(pf == 1, p.pt_idx - npv, p.pt_idx).astype(np.int32),
+                     obs=p.obs, weight=p.weight, cam_fixed=cf, pt_fixed=pf, nc_fix=ncf, np_fix=npf,
+                     f=p.f, cx=p.cx, cy=p.cy, cams_true=p.cams_true, pts_true=p.pts_true,
+                     name=p.name + "+fixed", meta=dict(p.meta))

@@ -208,6 +208,37 @@ nl_status nl_solver_compute_increment(nl_solver* s, double rel_lambda, double ab
  * (No counterpart in the reference: it checks the B200 kernel itself.) */
 nl_status nl_selftest_tc_update(int ntiles, unsigned long long seed, int device, double* max_rel_err);
 
+/* ---- cost without any device allocation ---------------------------------- */
+/* No counterpart in the reference.  The FP64 cost chi2 = sum_e w_e |r_e|^2 of
+ * the projection edges (the value nl_update reports), for callers that must
+ * not allocate device memory while they run: a program whose memory pool owns
+ * the whole device, a real-time loop that keeps the allocator out of its
+ * frames, a host context where allocation calls are forbidden.  It creates no
+ * handle and calls no allocator; every input and the output are the caller's
+ * device buffers:
+ *   d_cam_state  cameras in the device state layout of nl_get_camera_state
+ *                (16 doubles: R[9] row-major, t[3], f, k1, k2, pad);
+ *   d_pts        points, 3 doubles each;
+ *   d_edge_cam / d_edge_pt  per edge, the camera / point row in those arrays;
+ *   d_obs        per edge the measured pixel (2 doubles); d_weight per-edge
+ *                weights or NULL for 1;
+ *   f            focal length of 6-parameter cameras (bc = 6); cx, cy the
+ *                principal point;
+ *   d_chi2       one double, written on `stream` (a cudaStream_t, 0 = the
+ *                default stream); the call returns after enqueueing.
+ * Its scratch (32 KB of partial sums) is a fixed array inside the library,
+ * present on every GPU that loads it until the process exits.  At most
+ * NL_NOALLOC_MAX_EDGES edges; larger ne is rejected with NL_ERR_ARG.  The
+ * first call on a device looks up that array's address (with that device
+ * current); make it before any stream capture.  All calls share the array:
+ * calls whose work overlaps on the GPU (other streams, other threads) race and
+ * must be serialised by the caller. */
+#define NL_NOALLOC_MAX_EDGES 16777216
+nl_status nl_ba_cost_noalloc(int bc, int ne, const double* d_cam_state, const double* d_pts,
+                             const int* d_edge_cam, const int* d_edge_pt, const double* d_obs,
+                             const double* d_weight, double f, double cx, double cy, double* d_chi2,
+                             void* stream);
+
 const char* nl_status_string(int status);
 /* Library build identification: "nelson_b200 <version> sm_100a". */
 const char* nl_version(void);

@@ -80,7 +80,8 @@ EXPORTS = [
     "nl_compute_increment", "nl_get_increment", "nl_inc_sqnorm", "nl_get_schur", "nl_oplus", "nl_backup",
     "nl_rollback", "nl_max_abs_b", "nl_chi2", "nl_rho", "nl_lm_solve", "nl_gn_solve", "nl_phase_timings",
     "nl_kernel_launches", "nl_solver_create", "nl_solver_destroy", "nl_solver_set_hessian",
-    "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_selftest_tc_update", "nl_status_string",
+    "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_selftest_tc_update", "nl_ba_cost_noalloc",
+    "nl_status_string",
     "nl_version",
 ]
 
@@ -113,6 +114,7 @@ def load(build_if_missing: bool = True):
     L.nl_solver_create.argtypes = [C.POINTER(SolverDesc), vp, vp, vp, C.POINTER(vp)]
     L.nl_solver_compute_increment.argtypes = [vp, d, d, vp, vp, C.POINTER(i)]
     L.nl_selftest_tc_update.argtypes = [i, C.c_ulonglong, i, C.POINTER(d)]
+    L.nl_ba_cost_noalloc.argtypes = [i, i, vp, vp, vp, vp, vp, vp, d, d, d, vp, vp]
     for name in EXPORTS:  # fails loudly if the library lacks an entry point
         if name not in ("nl_status_string", "nl_version"):
             getattr(L, name).restype = C.c_int

@@ -263,24 +263,25 @@ def main():
     mu = 1e-3 * gm.max_abs_hdiag()
     gm.compute_increment(0.0, mu)
     pt = gm.phase_times()
-    # The trailing update after panel k is a rank-128 update of the (T-k-1)-tile
-    # lower trailing triangle: every 128x128 FP32 tile is read and written once
-    # (128 KB), the two BF16 panels come from L2.  Its arithmetic intensity is
-    # 32 flop/B, so the kernel is HBM-bound; the algorithmic bytes per launch are
-    # those tile read-modify-writes.
-    ntiles = -(-(prob.nc_var * prob.bc) // 128)
-    tile_rmw = sum(m * (m + 1) // 2 for m in range(ntiles))
-    alg_bytes = tile_rmw * 128 * 128 * 4 * 2
-    nlaunch = 2 * (ntiles - 1) - 1  # block column k+1, then the rest, per panel
+    # The trailing update is a rank-K update (K = 256 for the paired panels of
+    # the tensor-core schedule, 128 for the look-ahead column): every updated
+    # 128x128 FP32 tile is read and written once per launch (128 KB) while the
+    # BF16 panels come from L2 -- 32-64 flop per byte, so the kernel is
+    # HBM-bound.  update_bytes are those tile read-modify-writes.
+    alg_bytes = pt["update_bytes"]
+    nlaunch = max(pt["update_launches"], 1)
     upd_s = pt["update_ms"] * 1e-3
     ach = alg_bytes / upd_s / 1e9 if upd_s > 0 else None
     traffic = profiled_traffic()
+    traffic_launch = None
+    if traffic and traffic.get("bytes_per_tile_update"):
+        traffic_launch = traffic["bytes_per_tile_update"] * (alg_bytes / (128 * 128 * 4 * 2)) / nlaunch
     tfl = pt["update_flop"] / upd_s / 1e12 if upd_s > 0 else None
-    roofline = {"bound": "hbm", "kernel": "tc_syrk_kernel: Cholesky trailing update of S (tcgen05, rank-128)",
+    roofline = {"bound": "hbm", "kernel": "tc_syrk_kernel: Cholesky trailing update of S (tcgen05, split-BF16x3)",
                 "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": (ach / hbm) if ach else None,
                 "peak_source": f"{peak_src} HBM copy bandwidth",
                 "algorithmic_bytes_per_launch": alg_bytes / nlaunch, "launches_per_factorisation": nlaunch,
-                "traffic": (traffic or {}).get("bytes_per_launch_full_size"),
+                "traffic": traffic_launch,
                 "traffic_source": (traffic or {}).get("source"),
                 "tensor": {"achieved_tflops": tfl, "peak_tflops": bf16,
                            "frac": (tfl / bf16) if tfl else None,

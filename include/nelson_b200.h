@@ -92,7 +92,9 @@ typedef struct {
   float eval_ms;     /* last update(true) */
   float update_ms;   /* device time of the trailing updates inside factor_ms */
   int update_launches;
-  double update_flop; /* algorithmic flops of those updates (2 * multiply-adds) */
+  double update_flop;  /* algorithmic flops of those updates (2 * multiply-adds) */
+  double update_bytes; /* algorithmic bytes of those updates: each updated
+                          128 x 128 tile read and written once per launch */
 } nl_phase_times;
 
 /* ---- problem: device-resident BA section -------------------------------- */
@@ -173,6 +175,35 @@ nl_status nl_lm_solve(nl_problem* h, const nl_lm_settings* s, nl_solve_report* r
 /* GaussNewton<Solver>::solve (nelson/GaussNewton.hpp:32-127). */
 nl_status nl_gn_solve(nl_problem* h, const nl_gn_settings* s, nl_solve_report* rep,
                       double* trace, int trace_cap);
+
+/* ---- adjoint of a converged solve (implicit-function theorem) ------------ */
+/* No counterpart in the reference (it has no differentiation).  At a
+ * converged solution x* (the local gradient J'W r vanishes) and for a loss
+ * L(x*) with gradient dL/dx, computes
+ *     mu = H^-1 dL/dx          (H: exact Hessian of the cost at x*, FP64
+ *                               Hessian-vector products incl. second-order terms)
+ *     dL/dz_e = w_e J_e mu_e   (observations, 2 per edge)
+ *     dL/dw_e = -(J_e mu_e) . r_e   (per-edge weights)
+ * mu is found by `sweeps` rounds of iterative refinement preconditioned by
+ * the Schur factorisation of J'WJ at x* (factored once, reused each round).
+ * H must be non-singular: hold the gauge (e.g. two cameras as fixed nodes).
+ * Inputs, host memory: dL_dcams (variable cameras in user order, camera
+ * tangent [dw, dt (, df, dk1, dk2)]) and dL_dpts (variable points, xyz);
+ * either may be NULL for zero.  Outputs (any may be NULL): g_obs (2 per edge)
+ * and g_weight (1 per edge) in the order the edges were added; mu_cams /
+ * mu_pts in the layout of the inputs.  The gradient w.r.t. the initial
+ * parameters of a converged solve is zero and is not returned.  On return the
+ * Hessian blocks are those of x* and the gradient vector b is overwritten:
+ * call nl_update(h, 1, ...) before reading b-dependent quantities. */
+typedef struct {
+  int ok;               /* 1 when every factorisation / solve succeeded */
+  int sweeps;           /* refinement rounds after the first solve */
+  double grad_norm;     /* |dL/dx| */
+  double residual_norm; /* |dL/dx - H mu| after the last round */
+  double device_ms;     /* device time of the adjoint */
+} nl_adjoint_report;
+nl_status nl_adjoint(nl_problem* h, const double* dL_dcams, const double* dL_dpts, int sweeps, double* g_obs,
+                     double* g_weight, double* mu_cams, double* mu_pts, nl_adjoint_report* rep);
 
 nl_status nl_phase_timings(nl_problem* h, nl_phase_times* out);
 /* Number of kernels of this library launched on the handle since creation. */

@@ -43,8 +43,12 @@ template <typename T>
 static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S, int ld, int k,
                                                                 double* __restrict__ Linv, int* __restrict__ status,
                                                                 const int* __restrict__ active) {
-  __shared__ double Lcol[2][NB][4];  // L of block column jb, rows >= 4 jb (double-buffered)
-  __shared__ double Xrow[2][4][NB];  // X of block row jb, columns <= 4 jb + 3
+  // L of block column jb (row 4 b + u, column w at Lc[.][w][u][b]) and X of
+  // block row jb (row u, column 4 b + v at Xr[.][u][v][b]), double-buffered.
+  // Block index innermost: a warp's owners read consecutive block indices, so
+  // the loads of the rank-4 update are free of bank conflicts.
+  __shared__ double Lc[2][4][4][NB / 4];
+  __shared__ double Xr[2][4][4][NB / 4];
   __shared__ double Di[2][4][4];     // inv(L_jb,jb)
   __shared__ int bad;
   if (active && !*active) return;
@@ -115,7 +119,7 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
         for (int c = 0; c < 4; c++) {
           Di[buf][i][c] = di[i][c];
           if (c > i) a[i][c] = 0.0;
-          Lcol[buf][r0 + i][c] = a[i][c];
+          Lc[buf][c][i][jb] = a[i][c];
         }
     }
     __syncthreads();
@@ -134,7 +138,7 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
 #pragma unroll
         for (int v = 0; v < 4; v++) {
           a[u][v] = l[v];
-          Lcol[buf][r0 + u][v] = l[v];
+          Lc[buf][v][u][R] = l[v];
         }
       }
     }
@@ -152,7 +156,7 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           x[u][v] = xx[u];
-          Xrow[buf][u][c0 + v] = xx[u];
+          Xr[buf][u][v][C] = xx[u];
         }
       }
     }
@@ -164,8 +168,8 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
         double lr[4], lc[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-          lr[u] = Lcol[buf][r0 + u][w];
-          lc[u] = Lcol[buf][c0 + u][w];
+          lr[u] = Lc[buf][w][u][R];
+          lc[u] = Lc[buf][w][u][C];
         }
 #pragma unroll
         for (int u = 0; u < 4; u++)
@@ -178,8 +182,8 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
         double lr[4], xr[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-          lr[u] = Lcol[buf][r0 + u][w];
-          xr[u] = Xrow[buf][w][c0 + u];
+          lr[u] = Lc[buf][w][u][R];
+          xr[u] = Xr[buf][w][u][C];
         }
 #pragma unroll
         for (int u = 0; u < 4; u++)
@@ -232,14 +236,32 @@ static __global__ void __launch_bounds__(256) trsm_kernel(T* __restrict__ S, int
   const int r0 = (k + 1) * NB + blockIdx.x * TRSM_ROWS;
   const int nr = min(TRSM_ROWS, (k + 1) * NB + nrows_below - r0);
   if (nr <= 0) return;
+  // staging: 16 independent loads in flight per thread before the stores
   const double* Li = Linv + (size_t)k * NB * NB;
-  for (int i = tid; i < NB * NB; i += 256) {
-    const int j = i / NB, l = i - j * NB;
-    sL[l * (NB + 1) + j] = (T)Li[i];
+#pragma unroll 1
+  for (int i0 = tid; i0 < NB * NB; i0 += 256 * 16) {
+    double v[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) v[u] = __ldg(Li + i0 + 256 * u);
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      const int i = i0 + 256 * u, j = i / NB, l = i - j * NB;
+      sL[l * (NB + 1) + j] = (T)v[u];
+    }
   }
-  for (int i = tid; i < TRSM_ROWS * NB; i += 256) {
-    const int r = i / NB, l = i - r * NB;
-    sA[l * (TRSM_ROWS + 1) + r] = r < nr ? S[(size_t)(r0 + r) * ld + (size_t)k * NB + l] : (T)0;
+#pragma unroll 1
+  for (int i0 = tid; i0 < TRSM_ROWS * NB; i0 += 256 * 16) {
+    T v[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      const int i = i0 + 256 * u, r = i / NB, l = i - r * NB;
+      v[u] = r < nr ? S[(size_t)(r0 + r) * ld + (size_t)k * NB + l] : (T)0;
+    }
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      const int i = i0 + 256 * u, r = i / NB, l = i - r * NB;
+      sA[l * (TRSM_ROWS + 1) + r] = v[u];
+    }
   }
   __syncthreads();
   const int ty = tid >> 4, tx = tid & 15;

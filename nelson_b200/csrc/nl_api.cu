@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "ba_kernels.cuh"
+#include "adjoint.cuh"
 #include "schur_core.cuh"
 
 using namespace nl;
@@ -60,6 +61,7 @@ struct nl_problem {
   double lam_host[2] = {0, 0};
   DevBuf d_lam;
   long long launches = 0;
+  DevBuf adj_vec, adj_slot2int, adj_out;  // adjoint work (allocated on first nl_adjoint)
   cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
   float eval_ms = 0;
   int have_jac = 0;
@@ -871,6 +873,132 @@ nl_status nl_gn_solve(nl_problem* h, const nl_gn_settings* st, nl_solve_report* 
   s.initV = 1;
   s.penaltyV = 1;
   return run_solver(h, s, rep, trace, trace_cap, std::max(st->maxNumIt, 0) + 2);
+}
+
+}  // extern "C"
+
+namespace {
+
+template <int BC>
+void enqueue_hv(nl_problem* h, const double* vU, const double* vV, double* outU, double* outV) {
+  if (h->nci > 0) hv_cam_kernel<BC, 128><<<h->nci, 128, 0, h->st>>>(h->ba, vU, vV, outU);
+  if (h->desc.np_var > 0)
+    hv_pt_kernel<BC><<<cdiv(h->desc.np_var, 128), 128, 0, h->st>>>(h->ba, h->adj_slot2int.as<int>(), vU, vV, outV);
+  h->launches += 2;
+}
+
+template <typename T>
+void enqueue_neg_to_b(nl_problem* h, const double* res, int nU, int nV3) {
+  if (nU > 0) neg_to_b_kernel<T><<<cdiv(nU, 256), 256, 0, h->st>>>(res, nU, (T*)h->core->dbU());
+  if (nV3 > 0) neg_to_b_kernel<T><<<cdiv(nV3, 256), 256, 0, h->st>>>(res + nU, nV3, (T*)h->core->dbV());
+  h->launches += 2;
+}
+
+}  // namespace
+
+extern "C" {
+
+nl_status nl_adjoint(nl_problem* h, const double* dL_dcams, const double* dL_dpts, int sweeps, double* g_obs,
+                     double* g_weight, double* mu_cams, double* mu_pts, nl_adjoint_report* rep) {
+  NL_CHECK_READY(h);
+  if (sweeps < 0 || sweeps > 64) return NL_ERR_ARG;
+  NL_CUDA(cudaSetDevice(h->device));
+  const int bc = h->desc.bc, nci = h->nci, npv = h->desc.np_var, ncv = h->desc.nc_var;
+  const int nU = nci * bc, nV3 = 3 * npv, ntot = nU + nV3;
+  const int ne = (int)h->e_cam.size();
+  nl_status s;
+  if (!h->adj_vec.p) {
+    // [g | res | hv | mu], FP64, internal camera order then points
+    if ((s = h->adj_vec.alloc(sizeof(double) * 4 * (size_t)std::max(ntot, 1))) != NL_OK) return s;
+    std::vector<int> s2i(h->nc_all(), -1);
+    for (int u = 0; u < ncv; u++) s2i[u] = h->perm[u];
+    if ((s = upload(h->adj_slot2int, s2i, h->st)) != NL_OK) return s;
+    if ((s = h->adj_out.alloc(sizeof(double) * 3 * (size_t)std::max(ne, 1))) != NL_OK) return s;
+  }
+  double* g = h->adj_vec.as<double>();
+  double* res = g + ntot;
+  double* hv = res + ntot;
+  double* mu = hv + ntot;
+  std::vector<double> gh(ntot, 0.0);
+  if (dL_dcams)
+    for (int u = 0; u < ncv; u++)
+      for (int i = 0; i < bc; i++) gh[(size_t)h->perm[u] * bc + i] = dL_dcams[(size_t)u * bc + i];
+  if (dL_dpts) std::copy(dL_dpts, dL_dpts + nV3, gh.begin() + nU);
+  double gnorm = 0;
+  for (double x : gh) gnorm += x * x;
+  gnorm = std::sqrt(gnorm);
+  NL_CUDA(cudaEventRecord(h->ev_t0, h->st));
+  if (ntot > 0) {
+    NL_CUDA(cudaMemcpyAsync(g, gh.data(), sizeof(double) * ntot, cudaMemcpyHostToDevice, h->st));
+    NL_CUDA(cudaMemcpyAsync(res, g, sizeof(double) * ntot, cudaMemcpyDeviceToDevice, h->st));
+    NL_CUDA(cudaMemsetAsync(mu, 0, sizeof(double) * ntot, h->st));
+  }
+  // J'WJ at x* (and the cost); its factorisation preconditions the exact Hessian
+  if ((s = enqueue_eval(h, true, h->scal, h->scal + 1, nullptr)) != NL_OK) return s;
+  h->host_pin[16] = 0.0;
+  h->host_pin[17] = 0.0;
+  NL_CUDA(cudaMemcpyAsync(h->d_lam.p, h->host_pin + 16, 2 * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  NL_CUDA(cudaMemsetAsync(h->status, 0, sizeof(int), h->st));
+  const bool f64 = h->desc.precision == NL_PREC_FP64;
+  for (int it = 0; it <= sweeps; it++) {
+    if (f64)
+      enqueue_neg_to_b<double>(h, res, nU, nV3);
+    else
+      enqueue_neg_to_b<float>(h, res, nU, nV3);
+    s = it == 0 ? h->core->enqueue_increment(h->d_lam.as<double>(), h->status, nullptr)
+                : h->core->enqueue_resolve(h->status);
+    if (s != NL_OK) return s;
+    if (nU > 0) acc_kernel<<<cdiv(nU, 256), 256, 0, h->st>>>(mu, h->core->incU, nU);
+    if (nV3 > 0) acc_kernel<<<cdiv(nV3, 256), 256, 0, h->st>>>(mu + nU, h->core->incV, nV3);
+    if (bc == 9)
+      enqueue_hv<9>(h, mu, mu + nU, hv, hv + nU);
+    else
+      enqueue_hv<6>(h, mu, mu + nU, hv, hv + nU);
+    if (ntot > 0) resid_kernel<<<cdiv(ntot, 256), 256, 0, h->st>>>(g, hv, ntot, res);
+    h->launches += 3;
+  }
+  double* dobs = h->adj_out.as<double>();
+  double* dw = dobs + 2 * (size_t)ne;
+  if ((g_obs || g_weight) && ne > 0) {
+    if (bc == 9)
+      vjp_edge_kernel<9><<<cdiv(ne, 128), 128, 0, h->st>>>(h->ba, h->d_eorder.as<int>(), h->adj_slot2int.as<int>(),
+                                                            mu, mu + nU, dobs, dw);
+    else
+      vjp_edge_kernel<6><<<cdiv(ne, 128), 128, 0, h->st>>>(h->ba, h->d_eorder.as<int>(), h->adj_slot2int.as<int>(),
+                                                            mu, mu + nU, dobs, dw);
+    h->launches++;
+  }
+  NL_CUDA(cudaGetLastError());
+  NL_CUDA(cudaEventRecord(h->ev_t1, h->st));
+  std::vector<double> rh(ntot), muh(ntot);
+  if (ntot > 0) {
+    NL_CUDA(cudaMemcpyAsync(rh.data(), res, sizeof(double) * ntot, cudaMemcpyDeviceToHost, h->st));
+    NL_CUDA(cudaMemcpyAsync(muh.data(), mu, sizeof(double) * ntot, cudaMemcpyDeviceToHost, h->st));
+  }
+  if (g_obs && ne > 0) NL_CUDA(cudaMemcpyAsync(g_obs, dobs, sizeof(double) * 2 * ne, cudaMemcpyDeviceToHost, h->st));
+  if (g_weight && ne > 0) NL_CUDA(cudaMemcpyAsync(g_weight, dw, sizeof(double) * ne, cudaMemcpyDeviceToHost, h->st));
+  NL_CUDA(cudaMemcpyAsync(h->host_pin + 20, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  int st = 0;
+  memcpy(&st, h->host_pin + 20, sizeof(int));
+  double rnorm = 0;
+  for (double x : rh) rnorm += x * x;
+  if (mu_cams)
+    for (int u = 0; u < ncv; u++)
+      for (int i = 0; i < bc; i++) mu_cams[(size_t)u * bc + i] = muh[(size_t)h->perm[u] * bc + i];
+  if (mu_pts) std::copy(muh.begin() + nU, muh.end(), mu_pts);
+  if (rep) {
+    rep->ok = st == 0 ? 1 : 0;
+    rep->sweeps = sweeps;
+    rep->grad_norm = gnorm;
+    rep->residual_norm = std::sqrt(rnorm);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev_t0, h->ev_t1);
+    rep->device_ms = ms;
+  }
+  if (st & ST_SPIN_TIMEOUT) return NL_ERR_TIMEOUT;
+  if (st) return NL_ERR_NOT_SPD;
+  return NL_OK;
 }
 
 nl_status nl_phase_timings(nl_problem* h, nl_phase_times* out) {

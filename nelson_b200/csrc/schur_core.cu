@@ -130,7 +130,7 @@ class SchurCoreT final : public SchurCore {
     if (need_s0_) NL_TRY(S0_.alloc(sizeof(T) * (size_t)ld_ * ld_));
     if (sizeof(T) == 4 && use_tc) {
       tcs_half_ = (tc_syrk_scratch_bytes(ld_) + 255) / 256 * 256;
-      NL_TRY(tcs_.alloc(2 * tcs_half_));
+      NL_TRY(tcs_.alloc(kPackSlots * tcs_half_));
     }
     NL_TRY(upload(v_uid_, st.v_uid, st_));
     NL_TRY(upload(w_row_ptr_, w_row_ptr, st_));
@@ -244,8 +244,8 @@ class SchurCoreT final : public SchurCore {
           return NL_ERR_CUDA;
       }
     } else if (sizeof(T) == 4 && use_tc) {
-      NL_CUDA(tc_update_f32(reinterpret_cast<float*>(S_.p), ld_, k, t0, nt, col_only ? 1 : 0,
-                            static_cast<uint8_t*>(tcs_.p) + (size_t)(k & 1) * tcs_half_, active, status, st));
+      NL_CUDA(tc_update_f32(reinterpret_cast<float*>(S_.p), ld_, k, t0, nt, col_only ? 1 : 0, pack_slot(k), nullptr,
+                            active, status, st));
       launches++;
     } else {
       if (col_only) {
@@ -271,14 +271,102 @@ class SchurCoreT final : public SchurCore {
       launches++;
       if (sizeof(T) == 4 && use_tc) {
         NL_CUDA(tc_pack_f32(reinterpret_cast<const float*>(S_.p), ld_, k, below,
-                            static_cast<uint8_t*>(tcs_.p) + (size_t)(k & 1) * tcs_half_, active, st_));
+                            pack_slot(k), active, st_));
         launches++;
       }
     }
     return NL_OK;
   }
 
+  uint8_t* pack_slot(int k) const { return static_cast<uint8_t*>(tcs_.p) + (size_t)(k % kPackSlots) * tcs_half_; }
+
+  // Tensor-core schedule: panels in pairs, so the bulk of the trailing update
+  // has K = 256 and every trailing tile is read and written once per pair
+  // instead of once per panel.  Per pair (k, k + 1):
+  //   A1  block column k+1 with panel k (K = 128), main stream;
+  //   panel k+1 (diagonal factor, TRSM, pack);
+  //   A2  block columns k+2, k+3 with panels k, k+1 (K = 256), main stream,
+  //       after B of the previous pair (both touch those columns);
+  //   B   tiles of block columns >= k+4 (K = 256), side stream, after the
+  //       packs of the pair and after the previous B;
+  //   panel k+2.
+  // Packs live in kPackSlots = 4 slots (k mod 4): the next pair writes the
+  // other two while B still reads this pair's.
+  nl_status enqueue_factor_pairs(int* status, const int* active) {
+    const bool tm = timing && !active;
+    const int nT = ntiles_;
+    if (tm && (int)upd_ev_.size() < 6 * nT) {
+      for (size_t i = upd_ev_.size(); i < (size_t)6 * nT; i++) {
+        cudaEvent_t e;
+        NL_CUDA(cudaEventCreate(&e));
+        upd_ev_.push_back(e);
+      }
+    }
+    float* S = reinterpret_cast<float*>(S_.p);
+    double upd_flop = 0, upd_bytes = 0;
+    int nev = 0, nupd = 0;
+    auto tiles_of = [](int nt, int ncols) {
+      if (ncols <= 0) return (double)nt * (nt + 1) / 2;
+      double t = 0;
+      for (int j = 0; j < ncols && j < nt; j++) t += nt - j;
+      return t;
+    };
+    auto upd = [&](int k, bool pair, int t0, int nt, int ncols, cudaStream_t st) -> nl_status {
+      if (nt <= 0) return NL_OK;
+      if (tm) NL_CUDA(cudaEventRecord(upd_ev_[nev], st));
+      NL_CUDA(tc_update_f32(S, ld_, k, t0, nt, ncols, pack_slot(k), pair ? pack_slot(k + 1) : nullptr, active,
+                            status, st));
+      if (tm) NL_CUDA(cudaEventRecord(upd_ev_[nev + 1], st));
+      nev += 2;
+      nupd++;
+      launches++;
+      upd_bytes += tiles_of(nt, ncols) * (double)NB * NB * sizeof(float) * 2;
+      return NL_OK;
+    };
+    for (int k = 0; k + 1 < nT; k++) {
+      const double below = (double)ld_ - (double)(k + 1) * NB;
+      upd_flop += (double)NB * below * (below + 1);
+    }
+    nl_status r;
+    if ((r = factor_panel(0, status, active)) != NL_OK) return r;
+    bool pending_b = false;
+    for (int k = 0; k + 1 < nT; k += 2) {
+      // panel k is factored and packed; block column k+1 has every update but panel k's
+      if ((r = upd(k, false, k + 1, nT - k - 1, 1, st_)) != NL_OK) return r;  // A1
+      if ((r = factor_panel(k + 1, status, active)) != NL_OK) return r;
+      if (k + 2 >= nT) break;
+      NL_CUDA(cudaEventRecord(ev_panel_, st_));
+      if (pending_b) NL_CUDA(cudaStreamWaitEvent(st_, ev_b_, 0));
+      if ((r = upd(k, true, k + 2, nT - k - 2, 2, st_)) != NL_OK) return r;  // A2
+      if (k + 4 < nT) {
+        NL_CUDA(cudaStreamWaitEvent(st2_, ev_panel_, 0));
+        if ((r = upd(k, true, k + 4, nT - k - 4, 0, st2_)) != NL_OK) return r;  // B
+        NL_CUDA(cudaEventRecord(ev_b_, st2_));
+        pending_b = true;
+      } else {
+        pending_b = false;
+      }
+      if ((r = factor_panel(k + 2, status, active)) != NL_OK) return r;
+    }
+    if (pending_b) NL_CUDA(cudaStreamWaitEvent(st_, ev_b_, 0));
+    if (tm) {
+      NL_CUDA(cudaStreamSynchronize(st_));
+      float tot = 0;
+      for (int i = 0; i < nev; i += 2) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, upd_ev_[i], upd_ev_[i + 1]);
+        tot += ms;
+      }
+      times.update_ms = tot;
+      times.update_launches = nupd;
+      times.update_flop = upd_flop;
+      times.update_bytes = upd_bytes;
+    }
+    return NL_OK;
+  }
+
   nl_status enqueue_factor(int* status, const int* active) {
+    if (sizeof(T) == 4 && use_tc) return enqueue_factor_pairs(status, active);
     const bool tm = timing && !active;
     if (tm && (int)upd_ev_.size() < 4 * ntiles_) {
       for (size_t i = upd_ev_.size(); i < (size_t)4 * ntiles_; i++) {
@@ -333,6 +421,9 @@ class SchurCoreT final : public SchurCore {
       times.update_ms = tot;
       times.update_launches = nupd;
       times.update_flop = upd_flop;
+      double tiles = 0;
+      for (int m = 1; m < ntiles_; m++) tiles += (double)m * (m + 1) / 2;
+      times.update_bytes = tiles * (double)NB * NB * sizeof(T) * 2;
     }
     return NL_OK;
   }
@@ -390,6 +481,30 @@ class SchurCoreT final : public SchurCore {
       times.backsub_ms = ms[5];
       cudaEventElapsedTime(&times.total_ms, ev_[0], ev_[6]);
     }
+    return NL_OK;
+  }
+
+  nl_status enqueue_resolve(int* status) override {
+    if (nci_ > 0)
+      wvinv_bs_kernel<T, BC, 128><<<nci_, 128, 0, st_>>>(d_, W_.as<T>(), Vinv_.as<T>(), Y_.as<T>(), bU_.as<T>(),
+                                                         bV_.as<T>(), bS_.as<double>(), nullptr);
+    launches++;
+    nl_status s = enqueue_solve(bS_.as<double>(), incU, status, nullptr);
+    if (s != NL_OK) return s;
+    for (int it = 0; it < refine_sweeps && need_s0_; it++) {
+      symv_partial_kernel<T, kSymvChunks><<<dim3(ntiles_, kSymvChunks), SV, 0, st_>>>(
+          S0_.as<T>(), ld_, ntiles_, incU, part_.as<double>(), nullptr);
+      resid_finalize_kernel<kSymvChunks><<<cdiv(ld_, 256), 256, 0, st_>>>(part_.as<double>(), bS_.as<double>(), ld_,
+                                                                          r_.as<double>(), nullptr);
+      if ((s = enqueue_solve(r_.as<double>(), dx_.as<double>(), status, nullptr)) != NL_OK) return s;
+      axpy_kernel<<<cdiv(ld_, 256), 256, 0, st_>>>(incU, dx_.as<double>(), ld_, nullptr);
+      launches += 3;
+    }
+    zero_if_failed_kernel<<<cdiv(ld_, 256), 256, 0, st_>>>(incU, ld_, status, nullptr);
+    backsub_kernel<T, BC><<<cdiv(std::max(np_, 1), 128), 128, 0, st_>>>(d_, W_.as<T>(), Vinv_.as<T>(), bV_.as<T>(),
+                                                                      incU, incV, status, nullptr);
+    launches += 2;
+    NL_CUDA(cudaGetLastError());
     return NL_OK;
   }
 
@@ -495,6 +610,7 @@ class SchurCoreT final : public SchurCore {
   cublasHandle_t cublas2_ = nullptr;
   DevBuf ws2_;
   size_t tcs_half_ = 0;
+  static constexpr int kPackSlots = 4;
   std::vector<cudaEvent_t> upd_ev_;
 
  public:

@@ -79,6 +79,10 @@ class SchurCore {
   virtual nl_status setup(const SchurStructure& st, cudaStream_t stream) = 0;
   // computeIncrement with lam = device (rel, abs); `active` predicates every kernel.
   virtual nl_status enqueue_increment(const double* lam, int* status, const int* active) = 0;
+  // Solve with the factorisation of the last enqueue_increment for the
+  // current bU / bV (same V^-1, W V^-1 and factor of S): incU / incV get
+  // -(J'WJ + damping)^-1 b.
+  virtual nl_status enqueue_resolve(int* status) = 0;
   virtual nl_status enqueue_hdiag(double* out) = 0;
   virtual nl_status enqueue_maxabs_b(double* out, const int* active) = 0;
   virtual nl_status enqueue_inc_dot(const LmDev* s, double* part, int* nparts) = 0;

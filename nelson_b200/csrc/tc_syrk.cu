@@ -11,8 +11,9 @@
 //                  core (m-group g, k-group h) at byte (16 g + h) * 128, i.e.
 //                  LBO (K step) = 128 B, SBO (M step) = 2048 B.
 // tc_syrk_kernel   one CTA per lower 128x128 output tile: bulk-copies the
-//                  packed operands (cp.async.bulk + mbarrier) in two K chunks,
-//                  one thread issues 24 tcgen05.mma (M = N = 128, K = 16,
+//                  packed operands (cp.async.bulk + mbarrier) in K chunks of
+//                  64 (K = 128 for one panel, 256 for a pair of panels),
+//                  one thread issues 12 tcgen05.mma per chunk (M = N = 128, K = 16,
 //                  kind::f16, BF16 in, FP32 accumulate in TMEM) for
 //                  hi*hi + hi*lo + lo*hi and commits to an mbarrier; eight
 //                  warps read the accumulator with tcgen05.ld (32x32b), stage
@@ -161,28 +162,36 @@ constexpr int kStageLd = TB + 4;              // floats per staged accumulator r
 constexpr int kSmemBytes = TB * kStageLd * 4;  // 67,584 B >= 4 * 16 KB operands
 
 __global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int ld, int k, int t0, int nt,
-                                                      int col_only, const uint8_t* __restrict__ pack,
+                                                      int ncols, const uint8_t* __restrict__ pack,
+                                                      const uint8_t* __restrict__ pack2,
                                                       const int* __restrict__ active, int* __restrict__ status) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ __align__(8) uint64_t bar_load[2], bar_mma[2];
+  __shared__ __align__(8) uint64_t bar_load[4], bar_mma[4];
   __shared__ uint32_t tmem_base;
   __shared__ int ok_s;
   if (active && !*active) return;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int q = blockIdx.x;
+  int q = blockIdx.x;
   int I, J;
-  if (col_only) {
-    I = q;
+  if (ncols > 0) {
+    // the first ncols tile columns of the trailing triangle: column j holds
+    // tiles j .. nt - 1
     J = 0;
+    while (q >= nt - J) {
+      q -= nt - J;
+      J++;
+    }
+    I = J + q;
   } else {
     I = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
     while ((I + 1) * (I + 2) / 2 <= q) I++;
     while (I * (I + 1) / 2 > q) I--;
     J = q - I * (I + 1) / 2;
   }
+  // K = 128 (panel k) or 256 (panels k and k + 1): chunks of 64, chunks 2, 3
+  // from the pack of panel k + 1 (whose rows start one tile lower)
+  const int nch = pack2 ? 4 : 2;
   const bool diag = I == J;
-  const uint8_t* pa = pack + (size_t)(t0 + I - (k + 1)) * kPackTile;
-  const uint8_t* pb = pack + (size_t)(t0 + J - (k + 1)) * kPackTile;
   uint8_t* sAh = smem;
   uint8_t* sAl = smem + kChunkTile;
   uint8_t* sBh = diag ? sAh : smem + 2 * kChunkTile;
@@ -201,10 +210,10 @@ __global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    mbar_init(&bar_load[0], 1);
-    mbar_init(&bar_load[1], 1);
-    mbar_init(&bar_mma[0], 1);
-    mbar_init(&bar_mma[1], 1);
+    for (int c = 0; c < 4; c++) {
+      mbar_init(&bar_load[c], 1);
+      mbar_init(&bar_mma[c], 1);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
@@ -214,13 +223,17 @@ __global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int
 
   if (tid == 0) {
     int ok = 1;
-    for (int c = 0; c < 2 && ok; c++) {
+    for (int c = 0; c < nch && ok; c++) {
       // a packed tile holds core matrices (g, h) at (16 g + h) * 128; chunk c
-      // covers h = 8c .. 8c + 7, copied as 16 rows of 8 core matrices (1 KB each)
+      // covers h = 8 (c & 1) .. + 7, copied as 16 rows of 8 core matrices (1 KB each)
+      const uint8_t* pk = c < 2 ? pack : pack2;
+      const int first = c < 2 ? k + 1 : k + 2;  // first tile row of that pack
+      const uint8_t* pa = pk + (size_t)(t0 + I - first) * kPackTile;
+      const uint8_t* pb = pk + (size_t)(t0 + J - first) * kPackTile;
       const uint32_t bytes = (diag ? 2 : 4) * kChunkTile;
       mbar_expect_tx(&bar_load[c], bytes);
       for (int g = 0; g < 16; g++) {
-        const size_t src = (size_t)(16 * g + 8 * c) * 128;
+        const size_t src = (size_t)(16 * g + 8 * (c & 1)) * 128;
         const size_t dst = (size_t)g * 1024;
         bulk_g2s(sAh + dst, pa + src, 1024, &bar_load[c]);
         bulk_g2s(sAl + dst, pa + kTileBytes + src, 1024, &bar_load[c]);
@@ -304,7 +317,7 @@ cudaError_t tc_pack_f32(const float* S, int ld, int k, int nrows, void* pack, co
   return cudaGetLastError();
 }
 
-cudaError_t tc_update_f32(float* S, int ld, int k, int t0, int nt, int col_only, const void* pack,
+cudaError_t tc_update_f32(float* S, int ld, int k, int t0, int nt, int ncols, const void* pack, const void* pack2,
                           const int* active, int* status, cudaStream_t st) {
   static int attr_dev = -1;
   int dev = 0;
@@ -314,10 +327,16 @@ cudaError_t tc_update_f32(float* S, int ld, int k, int t0, int nt, int col_only,
     if (e != cudaSuccess) return e;
     attr_dev = dev;
   }
-  const int grid = col_only ? nt : nt * (nt + 1) / 2;
+  int grid = 0;
+  if (ncols > 0) {
+    for (int j = 0; j < ncols && j < nt; j++) grid += nt - j;
+  } else {
+    grid = nt * (nt + 1) / 2;
+  }
   if (grid <= 0) return cudaSuccess;
-  tc_syrk_kernel<<<grid, 256, kSmemBytes, st>>>(S, ld, k, t0, nt, col_only, static_cast<const uint8_t*>(pack),
-                                                active, status);
+  tc_syrk_kernel<<<grid, 256, kSmemBytes, st>>>(S, ld, k, t0, nt, ncols > nt ? nt : ncols,
+                                                static_cast<const uint8_t*>(pack),
+                                                static_cast<const uint8_t*>(pack2), active, status);
   return cudaGetLastError();
 }
 
@@ -325,7 +344,7 @@ cudaError_t tc_syrk_f32(float* S, int ld, int k, int t0, int nt, void* scratch, 
                         cudaStream_t st) {
   cudaError_t e = tc_pack_f32(S, ld, k, nt * TB, scratch, active, st);
   if (e != cudaSuccess) return e;
-  return tc_update_f32(S, ld, k, t0, nt, 0, scratch, active, status, st);
+  return tc_update_f32(S, ld, k, t0, nt, 0, scratch, nullptr, active, status, st);
 }
 
 }  // namespace nl

@@ -65,7 +65,12 @@ class SolveReport(C.Structure):
 class PhaseTimes(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("vinv_ms", "wvinv_bs_ms", "schur_ms", "factor_ms", "solve_ms",
                                           "backsub_ms", "total_ms", "eval_ms", "update_ms")] + \
-        [("update_launches", C.c_int), ("update_flop", C.c_double)]
+        [("update_launches", C.c_int), ("update_flop", C.c_double), ("update_bytes", C.c_double)]
+
+
+class AdjointReport(C.Structure):
+    _fields_ = [("ok", C.c_int), ("sweeps", C.c_int), ("grad_norm", C.c_double), ("residual_norm", C.c_double),
+                ("device_ms", C.c_double)]
 
 
 class SolverDesc(C.Structure):
@@ -81,6 +86,7 @@ EXPORTS = [
     "nl_rollback", "nl_max_abs_b", "nl_chi2", "nl_rho", "nl_lm_solve", "nl_gn_solve", "nl_phase_timings",
     "nl_kernel_launches", "nl_solver_create", "nl_solver_destroy", "nl_solver_set_hessian",
     "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_selftest_tc_update", "nl_ba_cost_noalloc",
+    "nl_adjoint",
     "nl_status_string",
     "nl_version",
 ]
@@ -114,6 +120,7 @@ def load(build_if_missing: bool = True):
     L.nl_solver_create.argtypes = [C.POINTER(SolverDesc), vp, vp, vp, C.POINTER(vp)]
     L.nl_solver_compute_increment.argtypes = [vp, d, d, vp, vp, C.POINTER(i)]
     L.nl_selftest_tc_update.argtypes = [i, C.c_ulonglong, i, C.POINTER(d)]
+    L.nl_adjoint.argtypes = [vp, vp, vp, i, vp, vp, vp, vp, C.POINTER(AdjointReport)]
     L.nl_ba_cost_noalloc.argtypes = [i, i, vp, vp, vp, vp, vp, vp, d, d, d, vp, vp]
     for name in EXPORTS:  # fails loudly if the library lacks an entry point
         if name not in ("nl_status_string", "nl_version"):
@@ -299,6 +306,21 @@ class BAProblemGPU:
         tr = np.zeros((max(trace_cap, 1), TRACE_STRIDE))
         self._c(self.L.nl_gn_solve(self.h, C.byref(s), C.byref(rep), _p(tr), trace_cap), "nl_gn_solve")
         return REASONS[rep.reason], tr[:rep.n_trace].copy(), rep.iterations
+
+    def adjoint(self, dL_dpts=None, dL_dcams=None, sweeps=3, want_mu=False):
+        """Implicit-function adjoint at the current (converged) solution:
+        returns (dL/dobs (ne, 2), dL/dweight (ne,), report[, mu_cams, mu_pts])."""
+        g_obs = np.zeros((self.ne, 2))
+        g_w = np.zeros(self.ne)
+        mu_c = np.zeros((self.nc_var, self.bc)) if want_mu else None
+        mu_p = np.zeros((self.np_var, 3)) if want_mu else None
+        dc = None if dL_dcams is None else np.ascontiguousarray(dL_dcams, np.float64).reshape(self.nc_var, self.bc)
+        dp = None if dL_dpts is None else np.ascontiguousarray(dL_dpts, np.float64).reshape(self.np_var, 3)
+        rep = AdjointReport()
+        self._c(self.L.nl_adjoint(self.h, _p(dc), _p(dp), sweeps, _p(g_obs), _p(g_w), _p(mu_c), _p(mu_p),
+                                  C.byref(rep)), "nl_adjoint")
+        r = {n: getattr(rep, n) for n, _ in AdjointReport._fields_}
+        return (g_obs, g_w, r, mu_c, mu_p) if want_mu else (g_obs, g_w, r)
 
     def phase_times(self):
         t = PhaseTimes()

@@ -130,3 +130,28 @@ def test_gn_matches_oracle(Orc, prec):
     for a, b in zip(tr_o, tr_g):
         assert abs(a[2] - b[2]) <= tol * a[2]
     g.close()
+
+
+@pytest.mark.parametrize("prec", [N.PREC_FP64, N.PREC_MIXED])
+@pytest.mark.parametrize("cfg,scale", [(1, 0.5), (2, 0.1)])
+def test_increment_multi_tile(Orc, cfg, scale, prec):
+    """Reduced systems of 8 (even) and 11 (odd) 128-wide tiles, so every step
+    of the blocked factorisation runs: the look-ahead column updates, the
+    paired-panel (K = 256) trailing updates of the tensor-core schedule and
+    the look-back triangular solves."""
+    p = make_config(cfg, scale)
+    o = Orc.Oracle.from_ba(p)
+    g = N.BAProblemGPU.from_ba(p, precision=prec)
+    assert -(-p.nc_var * p.bc // 128) >= 8
+    o.update(True)
+    g.update(True)
+    for mu_rel in (1e-3, 1e-6):
+        mu = mu_rel * o.max_abs_hdiag()
+        assert o.compute_increment(0.0, mu) and g.compute_increment(0.0, mu)
+        du_o, dv_o = o.increment()
+        du_g, dv_g = g.increment()
+        # at mu = 1e-6 max diag the gauge-free system is nearly singular: an
+        # FP32 factor with one FP64 refinement sweep holds the increment to 1e-3
+        itol = 1e-10 if prec == N.PREC_FP64 else (MIXED_INC_TOL if mu_rel >= 1e-3 else 1e-3)
+        assert rel(du_g, du_o) < itol and rel(dv_g, dv_o) < itol, (mu_rel, rel(du_g, du_o), rel(dv_g, dv_o))
+    g.close()

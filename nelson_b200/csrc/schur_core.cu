@@ -89,6 +89,11 @@ class SchurCoreT final : public SchurCore {
         }
     for (int q = 0; q < nU_; q++) s_uuid[bid[(size_t)st.u_r[q] * nci_ + st.u_c[q]]] = q;
     nS_ = (int)s_i.size();
+    // Schur work order: output blocks by pair count, heaviest first
+    std::vector<int> s_order(std::max(nS_, 1), 0);
+    for (int b = 0; b < nS_; b++) s_order[b] = b;
+    std::stable_sort(s_order.begin(), s_order.begin() + nS_,
+                     [&](int x, int y) { return s_ptr[x + 1] - s_ptr[x] > s_ptr[y + 1] - s_ptr[y]; });
     std::vector<int> pa(std::max<long long>(npairs, 1)), pb(std::max<long long>(npairs, 1));
     {
       std::vector<long long> fill(s_ptr.begin(), s_ptr.end() - 1);
@@ -142,6 +147,8 @@ class SchurCoreT final : public SchurCore {
     NL_TRY(upload(s_i_, s_i, st_));
     NL_TRY(upload(s_j_, s_j, st_));
     NL_TRY(upload(s_uuid_, s_uuid, st_));
+    NL_TRY(upload(s_order_, s_order, st_));
+    NL_TRY(sched_.alloc(sizeof(int) * 4));
     NL_TRY(upload(s_ptr_, s_ptr, st_));
     NL_TRY(upload(pa_, pa, st_));
     NL_TRY(upload(pb_, pb, st_));
@@ -440,9 +447,11 @@ class SchurCoreT final : public SchurCore {
     NL_CUDA(cudaMemsetAsync(S_.p, 0, S_.bytes, st_));
     if (need_s0_) NL_CUDA(cudaMemsetAsync(S0_.p, 0, S0_.bytes, st_));
     {
-      const int grid = std::max(1, std::min(cdiv(nS_, kSchurWarps), 148 * 16));
+      const int grid = std::max(1, std::min(cdiv(nS_, kSchurWarps), 148 * 8));
+      NL_CUDA(cudaMemsetAsync(sched_.p, 0, sizeof(int), st_));
       schur_kernel<T, BC, kSchurWarps><<<grid, kSchurWarps * 32, 0, st_>>>(
-          d_, U_.as<T>(), Y_.as<T>(), W_.as<T>(), lam, S_.as<T>(), need_s0_ ? S0_.as<T>() : nullptr, active);
+          d_, U_.as<T>(), Y_.as<T>(), W_.as<T>(), lam, S_.as<T>(), need_s0_ ? S0_.as<T>() : nullptr,
+          s_order_.as<int>(), sched_.as<int>(), active);
       if (ld_ > n_)
         pad_identity_kernel<T><<<cdiv(ld_ - n_, 128), 128, 0, st_>>>(S_.as<T>(), need_s0_ ? S0_.as<T>() : nullptr, n_,
                                                                      ld_, active);
@@ -603,7 +612,8 @@ class SchurCoreT final : public SchurCore {
   bool need_s0_ = false;
   SchurDev d_{};
   DevBuf U_, V_, W_, Y_, Vinv_, bU_, bV_, bS_, incU_, incV_, y_, r_, dx_, part_, Linv_, flags_, S_, S0_, tcs_;
-  DevBuf v_uid_, w_row_ptr_, w_col_, w_row_, w_col_ptr_, w_col_uid_, u_diag_, s_i_, s_j_, s_uuid_, s_ptr_, pa_, pb_;
+  DevBuf v_uid_, w_row_ptr_, w_col_, w_row_, w_col_ptr_, w_col_uid_, u_diag_, s_i_, s_j_, s_uuid_, s_ptr_, pa_, pb_, s_order_,
+      sched_;
   cudaEvent_t ev_[7] = {};
   cudaEvent_t ev_panel_ = nullptr, ev_b_ = nullptr;
   cudaStream_t st2_ = nullptr;  // side stream of the look-ahead factorisation

@@ -154,98 +154,142 @@ struct Vec4<double> {
   using type = double4;
 };
 
+// A staged row of a BC x 3 block (padded to 4 elements, 16-byte aligned).
+__device__ __forceinline__ void load_row3(const float* p, float& a, float& b, float& c) {
+  const float4 v = *reinterpret_cast<const float4*>(p);
+  a = v.x;
+  b = v.y;
+  c = v.z;
+}
+__device__ __forceinline__ void load_row3(const double* p, double& a, double& b, double& c) {
+  const double2 v = *reinterpret_cast<const double2*>(p);
+  a = v.x;
+  b = v.y;
+  c = p[2];
+}
+
+// One warp per output block, blocks taken heaviest-first from a work counter
+// (`order` lists them by pair count, descending), so the long diagonal blocks
+// start early and the tail is short; each block is still summed by one warp
+// in pair order, so S does not depend on the schedule.  Lane l < NSTR owns a
+// 1 x SW strip (row r, columns c0 .. c0 + SW - 1) of the BC x BC block.
+// Per batch of PB pairs the warp stages Y_a and W_b (rows padded to 4) in
+// shared memory and already issues the global loads of the next batch, so
+// their latency overlaps this batch's FMAs.  The batch's products are summed
+// before they are subtracted (blocked summation: a diagonal block sums
+// thousands of pairs in the working precision).
 template <typename T, int BC, int WARPS>
-static __global__ void __launch_bounds__(WARPS * 32) schur_kernel(SchurDev d, const T* __restrict__ U,
-                                                                   const T* __restrict__ Y, const T* __restrict__ W,
-                                                                   const double* __restrict__ lam, T* __restrict__ S,
-                                                                   T* __restrict__ S0, const int* __restrict__ active) {
+static __global__ void __launch_bounds__(WARPS * 32, 2) schur_kernel(SchurDev d, const T* __restrict__ U,
+                                                                      const T* __restrict__ Y, const T* __restrict__ W,
+                                                                      const double* __restrict__ lam, T* __restrict__ S,
+                                                                      T* __restrict__ S0, const int* __restrict__ order,
+                                                                      int* __restrict__ counter,
+                                                                      const int* __restrict__ active) {
   constexpr int LW = Layout<T, BC>::W;
   constexpr int LU = Layout<T, BC>::U;
-  constexpr int PB = 8;                          // pairs per batch
-  constexpr int NO = (BC * BC + 31) / 32;        // outputs per lane
-  constexpr int EPV = 16 / (int)sizeof(T);       // elements per 16-byte vector
-  constexpr int VB = LW / EPV;                   // vectors per block
+  constexpr int PB = 8;                                            // pairs per batch
+  constexpr int SW = (BC % 3 == 0) ? 3 : ((BC % 2 == 0) ? 2 : 1);  // strip width
+  constexpr int NSTR = BC * BC / SW;                               // strips (<= 32)
+  constexpr int EPV = 16 / (int)sizeof(T);                         // elements per 16-byte vector
+  constexpr int VB = LW / EPV;                                     // vectors per block
+  constexpr int NV = (2 * PB * VB + 31) / 32;                      // staged vectors per lane
   using V16 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  static_assert(NSTR <= 32, "one strip per lane");
   __shared__ __align__(16) T sh[WARPS][2][PB][BC][4];
   if (active && !*active) return;
   const double rel = lam[0], abs = lam[1];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nwarps = gridDim.x * WARPS;
-  for (int b = blockIdx.x * WARPS + warp; b < d.nS; b += nwarps) {
+  const int r = lane / (BC / SW), c0 = (lane % (BC / SW)) * SW;
+  const bool own = lane < NSTR;
+  T(*sy)[BC][4] = sh[warp][0];
+  T(*sw)[BC][4] = sh[warp][1];
+  for (;;) {
+    int idx = 0;
+    if (lane == 0) idx = atomicAdd(counter, 1);
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+    if (idx >= d.nS) break;
+    const int b = order[idx];
     const int bi = d.s_i[b], bj = d.s_j[b], uu = d.s_uuid[b];
-    T acc[NO];
+    T acc[SW];
 #pragma unroll
-    for (int k = 0; k < NO; k++) {
-      const int o = lane + 32 * k;
-      acc[k] = (T)0;
-      if (o < BC * BC && uu >= 0) acc[k] = U[(size_t)uu * LU + o];
-    }
+    for (int s2 = 0; s2 < SW; s2++)
+      acc[s2] = (own && uu >= 0) ? U[(size_t)uu * LU + r * BC + c0 + s2] : (T)0;
     const long long p0 = d.s_pair_ptr[b], p1 = d.s_pair_ptr[b + 1];
-    for (long long pp = p0; pp < p1; pp += PB) {
-      const int np = (int)min((long long)PB, p1 - pp);
+    // batch loader: lanes 0..np-1 fetch pair_a, np..2np-1 pair_b, then the
+    // 2 np blocks are read as VB 16-byte vectors each
+    V16 v[NV];
+    int np = 0;
+    auto load_batch = [&](long long pp) {
+      np = (int)min((long long)PB, p1 - pp);
       int uid = 0;
-      if (lane < np) uid = d.pair_a[pp + lane];
-      else if (lane < 2 * np) uid = d.pair_b[pp + lane - np];
-      // stage 2 np blocks of VB vectors each
-      V16 v[(2 * PB * VB + 31) / 32];
+      if (lane < np) uid = __ldg(d.pair_a + pp + lane);
+      else if (lane < 2 * np) uid = __ldg(d.pair_b + pp + lane - np);
 #pragma unroll
-      for (int t = 0; t < (2 * PB * VB + 31) / 32; t++) {
+      for (int t = 0; t < NV; t++) {
         const int u = lane + 32 * t;
         const int blk = u / VB, part = u - blk * VB;
         const int src_uid = __shfl_sync(0xffffffffu, uid, blk & 31);
         if (blk < 2 * np) {
           const T* base = (blk < np ? Y : W) + (size_t)src_uid * LW;
-          v[t] = *reinterpret_cast<const V16*>(base + part * EPV);
+          v[t] = __ldg(reinterpret_cast<const V16*>(base + part * EPV));
         }
       }
+    };
+    if (p0 < p1) load_batch(p0);
+    for (long long pp = p0; pp < p1; pp += PB) {
+      const int cur = np;
+      // registers -> shared memory (rows padded to 4)
 #pragma unroll
-      for (int t = 0; t < (2 * PB * VB + 31) / 32; t++) {
+      for (int t = 0; t < NV; t++) {
         const int u = lane + 32 * t;
         const int blk = u / VB, part = u - blk * VB;
-        if (blk < 2 * np) {
-          const int which = blk < np ? 0 : 1, q = blk < np ? blk : blk - np;
+        if (blk < 2 * cur) {
+          T(*dst)[4] = blk < cur ? sy[blk] : sw[blk - cur];
           const T* e = reinterpret_cast<const T*>(&v[t]);
 #pragma unroll
           for (int m = 0; m < EPV; m++) {
-            const int idx = part * EPV + m;  // element of the BC x 3 block
-            if (idx < BC * 3) sh[warp][which][q][idx / 3][idx % 3] = e[m];
+            const int el = part * EPV + m;  // element of the BC x 3 block
+            if (el < BC * 3) dst[el / 3][el % 3] = e[m];
           }
         }
       }
       __syncwarp();
+      if (pp + PB < p1) load_batch(pp + PB);  // in flight during the FMAs below
+      if (own) {
+        T part[SW];
 #pragma unroll
-      for (int k = 0; k < NO; k++) {
-        const int o = lane + 32 * k;
-        if (o < BC * BC) {
-          const int r = o / BC, cc = o - r * BC;
-          T s = (T)0;
-          for (int q = 0; q < np; q++) {
-            const T* ya = sh[warp][0][q][r];
-            const T* wb = sh[warp][1][q][cc];
-            s += ya[0] * wb[0] + ya[1] * wb[1] + ya[2] * wb[2];
+        for (int s2 = 0; s2 < SW; s2++) part[s2] = (T)0;
+        for (int q = 0; q < cur; q++) {
+          T y0, y1, y2;
+          load_row3(sy[q][r], y0, y1, y2);
+#pragma unroll
+          for (int s2 = 0; s2 < SW; s2++) {
+            T w0, w1, w2;
+            load_row3(sw[q][c0 + s2], w0, w1, w2);
+            part[s2] += y0 * w0 + y1 * w1 + y2 * w2;
           }
-          acc[k] -= s;
         }
+#pragma unroll
+        for (int s2 = 0; s2 < SW; s2++) acc[s2] -= part[s2];
       }
       __syncwarp();
     }
     // damping on the diagonal of diagonal blocks, then the store (lower storage:
     // S_lower[j*BC + c][i*BC + r] = S_ij[r][c])
-    const int ud = (bi == bj) ? d.u_diag_uid[bi] : -1;
+    if (own) {
+      const int ud = (bi == bj) ? d.u_diag_uid[bi] : -1;
 #pragma unroll
-    for (int k = 0; k < NO; k++) {
-      const int o = lane + 32 * k;
-      if (o < BC * BC) {
-        const int r = o / BC, cc = o - r * BC;
-        T v = acc[k];
+      for (int s2 = 0; s2 < SW; s2++) {
+        const int cc = c0 + s2;
+        T val = acc[s2];
         if (bi == bj && r == cc && (rel != 0.0 || abs != 0.0)) {
           const double udg = ud >= 0 ? (double)U[(size_t)ud * LU + r * BC + r] : 0.0;
-          v = (T)((double)v + rel * udg + abs);
+          val = (T)((double)val + rel * udg + abs);
         }
-        const size_t idx = (size_t)(bj * BC + cc) * d.ld + (size_t)(bi * BC + r);
+        const size_t o = (size_t)(bj * BC + cc) * d.ld + (size_t)(bi * BC + r);
         if (bi != bj || cc >= r) {
-          S[idx] = v;
-          if (S0) S0[idx] = v;
+          S[o] = val;
+          if (S0) S0[o] = val;
         }
       }
     }

@@ -6,19 +6,22 @@
 // (SolverCholeskyEigenDense::factorize, nelson/SolverCholeskyDense.hpp:15-18).
 //
 // tc_pack_kernel   splits X into BF16 hi = bf16(x) and lo = bf16(x - hi) and
-//                  stores each 128-row tile in the UMMA canonical K-major
+//                  stores each 128-row tile as four K-chunks of 32 columns,
+//                  each chunk (8 KB) contiguous in the UMMA canonical K-major
 //                  no-swizzle layout: 8x8 core matrices (128 contiguous bytes),
-//                  core (m-group g, k-group h) at byte (16 g + h) * 128, i.e.
-//                  LBO (K step) = 128 B, SBO (M step) = 2048 B.
-// tc_syrk_kernel   one CTA per lower 128x128 output tile: bulk-copies the
-//                  packed operands (cp.async.bulk + mbarrier) in K chunks of
-//                  64 (K = 128 for one panel, 256 for a pair of panels),
-//                  one thread issues 12 tcgen05.mma per chunk (M = N = 128, K = 16,
-//                  kind::f16, BF16 in, FP32 accumulate in TMEM) for
-//                  hi*hi + hi*lo + lo*hi and commits to an mbarrier; eight
-//                  warps read the accumulator with tcgen05.ld (32x32b), stage
-//                  it in shared memory and subtract it from the tile with
-//                  coalesced accesses.
+//                  core (m-group g, k-group h') at byte (4 g + h') * 128 of the
+//                  chunk, i.e. LBO (K step) = 128 B, SBO (M step) = 512 B.
+// tc_syrk_kernel   one CTA per lower 128x128 output tile.  One thread runs a
+//                  two-stage pipeline over the K-chunks (K = 128 for one
+//                  panel, 256 for a pair of panels): one cp.async.bulk per
+//                  operand chunk (A hi, A lo, B hi, B lo) lands on the
+//                  stage's mbarrier while the previous chunk's six
+//                  tcgen05.mma (M = N = 128, K = 16, kind::f16, BF16 in, FP32
+//                  accumulate in TMEM: hi*hi + hi*lo + lo*hi) run; each chunk
+//                  commits to the stage's MMA mbarrier, which frees the stage.
+//                  Eight warps then read the accumulator with tcgen05.ld
+//                  (32x32b), stage it in shared memory and subtract it from the
+//                  tile with coalesced accesses.
 // Every wait is bounded: on expiry the kernel records ST_SPIN_TIMEOUT, waits
 // (bounded) for what it issued, frees its TMEM and returns.
 #include <cuda_bf16.h>
@@ -34,6 +37,9 @@ namespace {
 constexpr int TB = 128;                  // tile rows / cols / K of one panel
 constexpr int kTileBytes = TB * TB * 2;  // one BF16 operand tile (32 KB)
 constexpr int kPackTile = 2 * kTileBytes;  // hi + lo
+constexpr int kChunkK = 32;                // K columns per pipeline chunk
+constexpr int kChunkBytes = TB * kChunkK * 2;  // one operand chunk: 8 KB
+constexpr int kChunksPerPanel = TB / kChunkK;  // 4
 constexpr long long kWaitLimit = 1LL << 22;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -145,7 +151,8 @@ __global__ void tc_pack_kernel(const float* __restrict__ S, int ld, int k, int n
     lo[i] = __float2bfloat16_rn(x[i] - __bfloat162float(hi[i]));
   }
   const int tile = r / TB, rr = r % TB, g = rr >> 3, ri = rr & 7;
-  const size_t off = (size_t)tile * kPackTile + (size_t)((16 * g + h) * 128 + ri * 16);
+  const int c = h >> 2, hh = h & 3;  // K-chunk of 32 columns, core column inside it
+  const size_t off = (size_t)tile * kPackTile + (size_t)c * kChunkBytes + (size_t)((4 * g + hh) * 128 + ri * 16);
   *reinterpret_cast<uint4*>(pack + off) = *reinterpret_cast<const uint4*>(hi);
   *reinterpret_cast<uint4*>(pack + off + kTileBytes) = *reinterpret_cast<const uint4*>(lo);
 }
@@ -156,17 +163,18 @@ __global__ void tc_pack_kernel(const float* __restrict__ S, int ld, int k, int n
 // overlap each other's copies, MMAs and epilogues.  The accumulator is
 // staged through shared memory so the read-modify-write of the FP32 C tile
 // is coalesced (a warp covers a 512-byte row).
-constexpr int kChunkK = 64;
-constexpr int kChunkTile = TB * kChunkK * 2;  // 16 KB: one operand half-tile
-constexpr int kStageLd = TB + 4;              // floats per staged accumulator row
-constexpr int kSmemBytes = TB * kStageLd * 4;  // 67,584 B >= 4 * 16 KB operands
+constexpr int kStageBytes = 4 * kChunkBytes;   // A hi, A lo, B hi, B lo of one chunk
+constexpr int kStages = 2;
+constexpr int kStageLd = TB + 4;               // floats per staged accumulator row
+constexpr int kSmemBytes = TB * kStageLd * 4;  // 67,584 B >= 2 stages x 32 KB operands
+static_assert(kStages * kStageBytes <= kSmemBytes, "operand stages alias the epilogue staging");
 
 __global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int ld, int k, int t0, int nt,
                                                       int ncols, const uint8_t* __restrict__ pack,
                                                       const uint8_t* __restrict__ pack2,
                                                       const int* __restrict__ active, int* __restrict__ status) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ __align__(8) uint64_t bar_load[4], bar_mma[4];
+  __shared__ __align__(8) uint64_t bar_load[2], bar_mma[2];
   __shared__ uint32_t tmem_base;
   __shared__ int ok_s;
   if (active && !*active) return;
@@ -188,14 +196,7 @@ __global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int
     while (I * (I + 1) / 2 > q) I--;
     J = q - I * (I + 1) / 2;
   }
-  // K = 128 (panel k) or 256 (panels k and k + 1): chunks of 64, chunks 2, 3
-  // from the pack of panel k + 1 (whose rows start one tile lower)
-  const int nch = pack2 ? 4 : 2;
   const bool diag = I == J;
-  uint8_t* sAh = smem;
-  uint8_t* sAl = smem + kChunkTile;
-  uint8_t* sBh = diag ? sAh : smem + 2 * kChunkTile;
-  uint8_t* sBl = diag ? sAl : smem + 3 * kChunkTile;
 
   // start pulling the output tile into L2 now; the epilogue reads it last
   {
@@ -210,9 +211,9 @@ __global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    for (int c = 0; c < 4; c++) {
-      mbar_init(&bar_load[c], 1);
-      mbar_init(&bar_mma[c], 1);
+    for (int st = 0; st < kStages; st++) {
+      mbar_init(&bar_load[st], 1);
+      mbar_init(&bar_mma[st], 1);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -223,45 +224,67 @@ __global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int
 
   if (tid == 0) {
     int ok = 1;
-    for (int c = 0; c < nch && ok; c++) {
-      // a packed tile holds core matrices (g, h) at (16 g + h) * 128; chunk c
-      // covers h = 8 (c & 1) .. + 7, copied as 16 rows of 8 core matrices (1 KB each)
-      const uint8_t* pk = c < 2 ? pack : pack2;
-      const int first = c < 2 ? k + 1 : k + 2;  // first tile row of that pack
-      const uint8_t* pa = pk + (size_t)(t0 + I - first) * kPackTile;
-      const uint8_t* pb = pk + (size_t)(t0 + J - first) * kPackTile;
-      const uint32_t bytes = (diag ? 2 : 4) * kChunkTile;
-      mbar_expect_tx(&bar_load[c], bytes);
-      for (int g = 0; g < 16; g++) {
-        const size_t src = (size_t)(16 * g + 8 * (c & 1)) * 128;
-        const size_t dst = (size_t)g * 1024;
-        bulk_g2s(sAh + dst, pa + src, 1024, &bar_load[c]);
-        bulk_g2s(sAl + dst, pa + kTileBytes + src, 1024, &bar_load[c]);
-        if (!diag) {
-          bulk_g2s(sBh + dst, pb + src, 1024, &bar_load[c]);
-          bulk_g2s(sBl + dst, pb + kTileBytes + src, 1024, &bar_load[c]);
-        }
+    const int nch = kChunksPerPanel * (pack2 ? 2 : 1);
+    // chunk c: stage c & 1, its (c >> 1)-th use of that stage
+    auto issue_load = [&](int c) {
+      uint8_t* st = smem + (size_t)(c & 1) * kStageBytes;
+      const int panel = c / kChunksPerPanel, cc = c % kChunksPerPanel;
+      const uint8_t* pk = panel == 0 ? pack : pack2;
+      const int first = k + 1 + panel;  // first tile row of that pack
+      const uint8_t* pa = pk + (size_t)(t0 + I - first) * kPackTile + (size_t)cc * kChunkBytes;
+      const uint8_t* pb = pk + (size_t)(t0 + J - first) * kPackTile + (size_t)cc * kChunkBytes;
+      mbar_expect_tx(&bar_load[c & 1], (diag ? 2 : 4) * kChunkBytes);
+      bulk_g2s(st, pa, kChunkBytes, &bar_load[c & 1]);
+      bulk_g2s(st + kChunkBytes, pa + kTileBytes, kChunkBytes, &bar_load[c & 1]);
+      if (!diag) {
+        bulk_g2s(st + 2 * kChunkBytes, pb, kChunkBytes, &bar_load[c & 1]);
+        bulk_g2s(st + 3 * kChunkBytes, pb + kTileBytes, kChunkBytes, &bar_load[c & 1]);
       }
-      if (!mbar_wait(&bar_load[c], 0)) {
+    };
+    int last_load = 0, last_commit = -1;
+    issue_load(0);
+    for (int c = 0; c < nch && ok; c++) {
+      if (c + 1 < nch) {
+        // stage (c + 1) & 1 was last read by the MMAs of chunk c - 1
+        if (c >= 1 && !mbar_wait(&bar_mma[(c + 1) & 1], ((c - 1) >> 1) & 1)) {
+          ok = 0;
+          break;
+        }
+        issue_load(c + 1);
+        last_load = c + 1;
+      }
+      if (!mbar_wait(&bar_load[c & 1], (c >> 1) & 1)) {
         ok = 0;
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      // chunk layout: core (g, h') at (8 g + h') * 128 -> LBO 128 B, SBO 1024 B
-      const uint8_t* as[3] = {sAh, sAh, sAl};
-      const uint8_t* bs[3] = {sBh, sBl, sBh};
+      const uint8_t* st = smem + (size_t)(c & 1) * kStageBytes;
+      const uint8_t* ah = st;
+      const uint8_t* al = st + kChunkBytes;
+      const uint8_t* bh = diag ? ah : st + 2 * kChunkBytes;
+      const uint8_t* bl = diag ? al : st + 3 * kChunkBytes;
+      const uint8_t* as[3] = {ah, ah, al};
+      const uint8_t* bs[3] = {bh, bl, bh};
 #pragma unroll
       for (int p = 0; p < 3; p++) {
 #pragma unroll
         for (int s2 = 0; s2 < kChunkK / 16; s2++) {
-          const uint64_t da = umma_desc(as[p] + s2 * 256, 128, 1024);
-          const uint64_t db = umma_desc(bs[p] + s2 * 256, 128, 1024);
+          // K = 16 = two core columns: 256 B along K; chunk SBO = 4 * 128 B
+          const uint64_t da = umma_desc(as[p] + s2 * 256, 128, 512);
+          const uint64_t db = umma_desc(bs[p] + s2 * 256, 128, 512);
           umma_bf16(tmem_d, da, db, (c > 0 || p > 0 || s2 > 0) ? 1u : 0u);
         }
       }
-      umma_commit(&bar_mma[c]);
-      // the operand buffer is reused by the next chunk: wait for these MMAs
-      if (!mbar_wait(&bar_mma[c], 0)) ok = 0;
+      umma_commit(&bar_mma[c & 1]);
+      last_commit = c;
+    }
+    // the last commit tracks every MMA issued before it
+    if (ok && !mbar_wait(&bar_mma[(nch - 1) & 1], ((nch - 1) >> 1) & 1)) ok = 0;
+    if (!ok) {
+      // a wait gave up: give what was issued a bounded chance to land before
+      // the shared memory and TMEM are reused / freed
+      if (last_commit >= 0) mbar_wait(&bar_mma[last_commit & 1], (last_commit >> 1) & 1);
+      mbar_wait(&bar_load[last_load & 1], (last_load >> 1) & 1);
     }
     ok_s = ok;
     if (!ok) atomicOr(status, ST_SPIN_TIMEOUT);

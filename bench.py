@@ -58,21 +58,34 @@ class Clocks:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.lines = []
+        self.lines = []  # (host time, csv line)
+        self.t0 = self.t1 = None
 
     def start(self):
+        """Start sampling every 20 ms; returns once the first sample is in (the
+        timed region is short, so nvidia-smi must already be running)."""
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            deadline = time.perf_counter() + 5.0
+            while not self.lines and time.perf_counter() < deadline:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def begin(self):
+        self.t0 = time.perf_counter()
+
+    def end(self):
+        self.t1 = time.perf_counter()
+        time.sleep(0.05)  # let the sample that covers the end arrive
 
     def stop(self):
         if self.proc is None:
@@ -82,9 +95,12 @@ class Clocks:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
+        t0 = self.t0 if self.t0 is not None else -1e30
+        t1 = self.t1 if self.t1 is not None else 1e30
+        inside = [ln for ts, ln in self.lines if t0 <= ts <= t1 + 0.03]
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in inside:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -97,7 +113,7 @@ class Clocks:
                 if v.lower().startswith("active"):
                     reasons.add(n)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "window_ms": round(1e3 * (t1 - t0), 1) if self.t0 is not None else None}
 
 
 def measured_peaks():
@@ -203,11 +219,13 @@ def main():
 
     # ---- timed: K LM iterations, mixed (the product) then FP64 ----
     clocks = Clocks(local)
+    clocks.start()
     launches0 = gm.kernel_launches()
     barrier()
-    clocks.start()
+    clocks.begin()
     r_m, tr_m, it_m, sub_m, rep_m = gm.lm_solve(N.LMSettings(maxNumIt=args.steps), trace_cap=4096, report=True)
     barrier()
+    clocks.end()
     ck = clocks.stop()
     launches = gm.kernel_launches() - launches0
     r_d, tr_d, it_d, sub_d, rep_d = gd.lm_solve(N.LMSettings(maxNumIt=args.steps), trace_cap=4096, report=True)

@@ -213,7 +213,8 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
 }
 
 // ---------------------------------------------------------------------------
-// L_ik = A_ik inv(L_kk)' for 64-row slabs below the diagonal tile, as a
+// L_ik = A_ik inv(L_kk)' for 64-row slabs of rows [row_begin, row_begin +
+// nrows) below the diagonal tile (absolute row indices), as a
 // register-tiled product: X (64 x 128) = A (64 x 128) Linv' (128 x 128).
 // 256 threads, thread (ty, tx) computes rows ty*4 .. ty*4+3 (ty < 16) and
 // columns tx + 16 j (tx < 16, j < 8); A and Linv are staged in shared memory
@@ -225,7 +226,7 @@ constexpr size_t trsm_smem() {
 }
 
 template <typename T>
-static __global__ void __launch_bounds__(256) trsm_kernel(T* __restrict__ S, int ld, int k, int nrows_below,
+static __global__ void __launch_bounds__(256) trsm_kernel(T* __restrict__ S, int ld, int k, int row_begin, int nrows,
                                                           const double* __restrict__ Linv,
                                                           const int* __restrict__ active) {
   extern __shared__ unsigned char smraw[];
@@ -233,8 +234,8 @@ static __global__ void __launch_bounds__(256) trsm_kernel(T* __restrict__ S, int
   T* sA = sL + NB * (NB + 1);               // sA[l][r] = A[r][l], (TRSM_ROWS + 1) stride
   if (active && !*active) return;
   const int tid = threadIdx.x;
-  const int r0 = (k + 1) * NB + blockIdx.x * TRSM_ROWS;
-  const int nr = min(TRSM_ROWS, (k + 1) * NB + nrows_below - r0);
+  const int r0 = row_begin + blockIdx.x * TRSM_ROWS;
+  const int nr = min(TRSM_ROWS, row_begin + nrows - r0);
   if (nr <= 0) return;
   // staging: 16 independent loads in flight per thread before the stores
   const double* Li = Linv + (size_t)k * NB * NB;

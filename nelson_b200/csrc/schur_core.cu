@@ -196,7 +196,10 @@ class SchurCoreT final : public SchurCore {
         int lo = 0, hi = 0;
         NL_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
         NL_CUDA(cudaStreamCreateWithPriority(&st2_, cudaStreamNonBlocking, lo));
+        // the auxiliary stream (panel work off the critical path) runs at the top priority
+        NL_CUDA(cudaStreamCreateWithPriority(&st3_, cudaStreamNonBlocking, hi));
       }
+      for (auto& e : dev_) NL_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
       if (cublas_) {
         if (cublasCreate(&cublas2_) != CUBLAS_STATUS_SUCCESS) return NL_ERR_CUDA;
         nl_status ws = ws2_.alloc(64u << 20);
@@ -251,8 +254,8 @@ class SchurCoreT final : public SchurCore {
           return NL_ERR_CUDA;
       }
     } else if (sizeof(T) == 4 && use_tc) {
-      NL_CUDA(tc_update_f32(reinterpret_cast<float*>(S_.p), ld_, k, t0, nt, col_only ? 1 : 0, pack_slot(k), nullptr,
-                            active, status, st));
+      NL_CUDA(tc_update_f32(reinterpret_cast<float*>(S_.p), ld_, k, t0, nt, col_only ? 1 : 0, 0, pack_slot(k),
+                            nullptr, active, status, st));
       launches++;
     } else {
       if (col_only) {
@@ -273,12 +276,11 @@ class SchurCoreT final : public SchurCore {
     launches++;
     const int below = ld_ - (k + 1) * NB;
     if (below > 0) {
-      trsm_kernel<T><<<cdiv(below, TRSM_ROWS), 256, trsm_smem<T>(), st_>>>(S_.as<T>(), ld_, k, below,
+      trsm_kernel<T><<<cdiv(below, TRSM_ROWS), 256, trsm_smem<T>(), st_>>>(S_.as<T>(), ld_, k, (k + 1) * NB, below,
                                                                             Linv_.as<double>(), active);
       launches++;
       if (sizeof(T) == 4 && use_tc) {
-        NL_CUDA(tc_pack_f32(reinterpret_cast<const float*>(S_.p), ld_, k, below,
-                            pack_slot(k), active, st_));
+        NL_CUDA(tc_pack_f32(reinterpret_cast<const float*>(S_.p), ld_, k, 0, below, pack_slot(k), active, st_));
         launches++;
       }
     }
@@ -289,21 +291,28 @@ class SchurCoreT final : public SchurCore {
 
   // Tensor-core schedule: panels in pairs, so the bulk of the trailing update
   // has K = 256 and every trailing tile is read and written once per pair
-  // instead of once per panel.  Per pair (k, k + 1):
-  //   A1  block column k+1 with panel k (K = 128), main stream;
-  //   panel k+1 (diagonal factor, TRSM, pack);
-  //   A2  block columns k+2, k+3 with panels k, k+1 (K = 256), main stream,
-  //       after B of the previous pair (both touch those columns);
-  //   B   tiles of block columns >= k+4 (K = 256), side stream, after the
-  //       packs of the pair and after the previous B;
-  //   panel k+2.
-  // Packs live in kPackSlots = 4 slots (k mod 4): the next pair writes the
-  // other two while B still reads this pair's.
+  // instead of once per panel, and the panel work split so that only the
+  // chain  potrf(j) -> TRSM + pack of row tile j+1 -> update of tile
+  // (j+1, j+1) -> potrf(j+1)  runs on the main stream; the rest of each step
+  // runs on the auxiliary stream (top priority) or, for the bulk update, on
+  // the side stream (lowest priority).  For the pair (k, k+1):
+  //   main  A1d  tile (k+1, k+1) with panel k (K = 128); potrf(k+1);
+  //         [wait A1r] TRSM + pack of row tile k+2 of panel k+1;
+  //         [wait B of the previous pair] A2d  tile (k+2, k+2) with panels
+  //         k, k+1 (K = 256); potrf(k+2); [wait A2r] TRSM + pack of row tile k+3
+  //   aux   A1r  block column k+1 below tile k+2 with panel k; TRSM + pack of
+  //         the rows below tile k+2 of panel k+1; [wait B] A2r  block columns
+  //         k+2 (below its diagonal) and k+3 with panels k, k+1; TRSM + pack of
+  //         the rows below tile k+3 of panel k+2
+  //   side  B    tiles of block columns >= k+4 with panels k, k+1.
+  // Packs live in kPackSlots = 4 slots (panel mod 4); B is the last reader of
+  // a pair's slots and the pair after next waits for it before repacking.
+  enum { EV_PACKF = 0, EV_POTRF, EV_A1R, EV_PACKR, EV_A2R, EV_B, EV_AUX };
   nl_status enqueue_factor_pairs(int* status, const int* active) {
     const bool tm = timing && !active;
     const int nT = ntiles_;
-    if (tm && (int)upd_ev_.size() < 6 * nT) {
-      for (size_t i = upd_ev_.size(); i < (size_t)6 * nT; i++) {
+    if (tm && (int)upd_ev_.size() < 10 * nT + 10) {
+      for (size_t i = upd_ev_.size(); i < (size_t)10 * nT + 10; i++) {
         cudaEvent_t e;
         NL_CUDA(cudaEventCreate(&e));
         upd_ev_.push_back(e);
@@ -312,50 +321,96 @@ class SchurCoreT final : public SchurCore {
     float* S = reinterpret_cast<float*>(S_.p);
     double upd_flop = 0, upd_bytes = 0;
     int nev = 0, nupd = 0;
-    auto tiles_of = [](int nt, int ncols) {
+    auto tiles_of = [](int nt, int ncols, int rb) {
       if (ncols <= 0) return (double)nt * (nt + 1) / 2;
       double t = 0;
-      for (int j = 0; j < ncols && j < nt; j++) t += nt - j;
+      for (int j = 0; j < ncols && j < nt; j++) t += std::max(0, nt - std::max(j, rb));
       return t;
     };
-    auto upd = [&](int k, bool pair, int t0, int nt, int ncols, cudaStream_t st) -> nl_status {
-      if (nt <= 0) return NL_OK;
+    auto upd = [&](int k, bool pair, int t0, int nt, int ncols, int rb, cudaStream_t st) -> nl_status {
+      if (nt <= 0 || tiles_of(nt, ncols, rb) <= 0) return NL_OK;
       if (tm) NL_CUDA(cudaEventRecord(upd_ev_[nev], st));
-      NL_CUDA(tc_update_f32(S, ld_, k, t0, nt, ncols, pack_slot(k), pair ? pack_slot(k + 1) : nullptr, active,
+      NL_CUDA(tc_update_f32(S, ld_, k, t0, nt, ncols, rb, pack_slot(k), pair ? pack_slot(k + 1) : nullptr, active,
                             status, st));
       if (tm) NL_CUDA(cudaEventRecord(upd_ev_[nev + 1], st));
       nev += 2;
       nupd++;
       launches++;
-      upd_bytes += tiles_of(nt, ncols) * (double)NB * NB * sizeof(float) * 2;
+      upd_bytes += tiles_of(nt, ncols, rb) * (double)NB * NB * sizeof(float) * 2;
       return NL_OK;
     };
+    // TRSM + pack of panel j's rows [r0, r0 + nrows) (absolute rows, tile aligned)
+    auto trsm_pack = [&](int j, int r0, int nrows, cudaStream_t st) -> nl_status {
+      if (nrows <= 0) return NL_OK;
+      trsm_kernel<T><<<cdiv(nrows, TRSM_ROWS), 256, trsm_smem<T>(), st>>>(S_.as<T>(), ld_, j, r0, nrows,
+                                                                           Linv_.as<double>(), active);
+      NL_CUDA(tc_pack_f32(reinterpret_cast<const float*>(S_.p), ld_, j, r0 - (j + 1) * NB, nrows, pack_slot(j),
+                          active, st));
+      launches += 2;
+      return NL_OK;
+    };
+    auto potrf = [&](int j) {
+      potrf_diag_kernel<T><<<1, PT, kPotrfSmem, st_>>>(S_.as<T>(), ld_, j, Linv_.as<double>(), status, active);
+      launches++;
+    };
+    auto rec = [&](int e, cudaStream_t st) { return cudaEventRecord(dev_[e], st); };
+    auto wait = [&](cudaStream_t st, int e) { return cudaStreamWaitEvent(st, dev_[e], 0); };
     for (int k = 0; k + 1 < nT; k++) {
       const double below = (double)ld_ - (double)(k + 1) * NB;
       upd_flop += (double)NB * below * (below + 1);
     }
     nl_status r;
-    if ((r = factor_panel(0, status, active)) != NL_OK) return r;
+    // panel 0
+    potrf(0);
+    if ((r = trsm_pack(0, NB, std::min(NB, ld_ - NB), st_)) != NL_OK) return r;
+    NL_CUDA(rec(EV_POTRF, st_));
+    NL_CUDA(wait(st3_, EV_POTRF));
+    if ((r = trsm_pack(0, 2 * NB, ld_ - 2 * NB, st3_)) != NL_OK) return r;
     bool pending_b = false;
     for (int k = 0; k + 1 < nT; k += 2) {
-      // panel k is factored and packed; block column k+1 has every update but panel k's
-      if ((r = upd(k, false, k + 1, nT - k - 1, 1, st_)) != NL_OK) return r;  // A1
-      if ((r = factor_panel(k + 1, status, active)) != NL_OK) return r;
+      // panel k is factored; row tile k+1 of it is packed (main), the rest
+      // is being packed on the aux stream
+      NL_CUDA(rec(EV_PACKF, st_));
+      if ((r = upd(k, false, k + 1, 1, 1, 0, st_)) != NL_OK) return r;  // A1d
+      NL_CUDA(wait(st3_, EV_PACKF));
+      if ((r = upd(k, false, k + 1, nT - k - 1, 1, 1, st3_)) != NL_OK) return r;  // A1r
+      NL_CUDA(rec(EV_A1R, st3_));
+      potrf(k + 1);
+      NL_CUDA(rec(EV_POTRF, st_));
+      NL_CUDA(wait(st3_, EV_POTRF));
+      if ((r = trsm_pack(k + 1, (k + 3) * NB, ld_ - (k + 3) * NB, st3_)) != NL_OK) return r;
+      NL_CUDA(rec(EV_PACKR, st3_));
+      NL_CUDA(wait(st_, EV_A1R));
+      if ((r = trsm_pack(k + 1, (k + 2) * NB, std::min(NB, ld_ - (k + 2) * NB), st_)) != NL_OK) return r;
       if (k + 2 >= nT) break;
-      NL_CUDA(cudaEventRecord(ev_panel_, st_));
-      if (pending_b) NL_CUDA(cudaStreamWaitEvent(st_, ev_b_, 0));
-      if ((r = upd(k, true, k + 2, nT - k - 2, 2, st_)) != NL_OK) return r;  // A2
+      // pair update: A2d on main, A2r on aux, B on the side stream
+      NL_CUDA(rec(EV_PACKF, st_));
+      if (pending_b) NL_CUDA(wait(st_, EV_B));
+      if ((r = upd(k, true, k + 2, 1, 1, 0, st_)) != NL_OK) return r;  // A2d
+      NL_CUDA(wait(st3_, EV_PACKF));
+      if (pending_b) NL_CUDA(wait(st3_, EV_B));
+      if ((r = upd(k, true, k + 2, nT - k - 2, 2, 1, st3_)) != NL_OK) return r;  // A2r
+      NL_CUDA(rec(EV_A2R, st3_));
       if (k + 4 < nT) {
-        NL_CUDA(cudaStreamWaitEvent(st2_, ev_panel_, 0));
-        if ((r = upd(k, true, k + 4, nT - k - 4, 0, st2_)) != NL_OK) return r;  // B
-        NL_CUDA(cudaEventRecord(ev_b_, st2_));
+        NL_CUDA(wait(st2_, EV_PACKF));
+        NL_CUDA(wait(st2_, EV_PACKR));
+        if ((r = upd(k, true, k + 4, nT - k - 4, 0, 0, st2_)) != NL_OK) return r;  // B
+        NL_CUDA(rec(EV_B, st2_));
         pending_b = true;
       } else {
         pending_b = false;
       }
-      if ((r = factor_panel(k + 2, status, active)) != NL_OK) return r;
+      potrf(k + 2);
+      NL_CUDA(rec(EV_POTRF, st_));
+      NL_CUDA(wait(st3_, EV_POTRF));
+      if ((r = trsm_pack(k + 2, (k + 4) * NB, ld_ - (k + 4) * NB, st3_)) != NL_OK) return r;
+      NL_CUDA(wait(st_, EV_A2R));
+      if ((r = trsm_pack(k + 2, (k + 3) * NB, std::min(NB, ld_ - (k + 3) * NB), st_)) != NL_OK) return r;
     }
-    if (pending_b) NL_CUDA(cudaStreamWaitEvent(st_, ev_b_, 0));
+    // join: the solves that follow read every tile and Linv
+    NL_CUDA(rec(EV_AUX, st3_));
+    NL_CUDA(wait(st_, EV_AUX));
+    if (pending_b) NL_CUDA(wait(st_, EV_B));
     if (tm) {
       NL_CUDA(cudaStreamSynchronize(st_));
       float tot = 0;
@@ -617,6 +672,8 @@ class SchurCoreT final : public SchurCore {
   cudaEvent_t ev_[7] = {};
   cudaEvent_t ev_panel_ = nullptr, ev_b_ = nullptr;
   cudaStream_t st2_ = nullptr;  // side stream of the look-ahead factorisation
+  cudaStream_t st3_ = nullptr;  // auxiliary stream of the tensor-core schedule
+  cudaEvent_t dev_[8] = {};     // dependency events of the tensor-core schedule
   cublasHandle_t cublas2_ = nullptr;
   DevBuf ws2_;
   size_t tcs_half_ = 0;
@@ -630,6 +687,12 @@ class SchurCoreT final : public SchurCore {
       cudaStreamSynchronize(st2_);
       cudaStreamDestroy(st2_);
     }
+    if (st3_) {
+      cudaStreamSynchronize(st3_);
+      cudaStreamDestroy(st3_);
+    }
+    for (auto e : dev_)
+      if (e) cudaEventDestroy(e);
     for (auto e : ev_)
       if (e) cudaEventDestroy(e);
     if (ev_panel_) cudaEventDestroy(ev_panel_);

@@ -25,6 +25,8 @@
 // Every wait is bounded: on expiry the kernel records ST_SPIN_TIMEOUT, waits
 // (bounded) for what it issued, frees its TMEM and returns.
 #include <cuda_bf16.h>
+
+#include <algorithm>
 #include <stdint.h>
 
 #include "nl_common.cuh"
@@ -132,14 +134,15 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
 }
 
 // ---------------------------------------------------------------------------
-// X (rows r0 .. r0 + nrows - 1, columns k*TB ..) -> packed hi / lo tiles.
+// X rows (k+1)*TB + r_first .. + nrows - 1 (columns k*TB ..) -> packed hi / lo
+// tiles; packed tile t holds rows (k+1+t)*TB ...
 // One thread per (row, 8-column group).
-__global__ void tc_pack_kernel(const float* __restrict__ S, int ld, int k, int nrows,
+__global__ void tc_pack_kernel(const float* __restrict__ S, int ld, int k, int r_first, int nrows,
                                uint8_t* __restrict__ pack, const int* __restrict__ active) {
   if (active && !*active) return;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)nrows * 16) return;
-  const int r = (int)(t >> 4), h = (int)(t & 15);
+  const int r = r_first + (int)(t >> 4), h = (int)(t & 15);
   const float* src = S + (size_t)((k + 1) * TB + r) * ld + (size_t)k * TB + 8 * h;
   const float4 a = *reinterpret_cast<const float4*>(src);
   const float4 b = *reinterpret_cast<const float4*>(src + 4);
@@ -170,7 +173,7 @@ constexpr int kSmemBytes = TB * kStageLd * 4;  // 67,584 B >= 2 stages x 32 KB o
 static_assert(kStages * kStageBytes <= kSmemBytes, "operand stages alias the epilogue staging");
 
 __global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int ld, int k, int t0, int nt,
-                                                      int ncols, const uint8_t* __restrict__ pack,
+                                                      int ncols, int rb, const uint8_t* __restrict__ pack,
                                                       const uint8_t* __restrict__ pack2,
                                                       const int* __restrict__ active, int* __restrict__ status) {
   extern __shared__ __align__(1024) uint8_t smem[];
@@ -183,13 +186,13 @@ __global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int
   int I, J;
   if (ncols > 0) {
     // the first ncols tile columns of the trailing triangle: column j holds
-    // tiles j .. nt - 1
+    // tiles max(j, rb) .. nt - 1
     J = 0;
-    while (q >= nt - J) {
-      q -= nt - J;
+    while (J + 1 < ncols && q >= nt - max(J, rb)) {
+      q -= nt - max(J, rb);
       J++;
     }
-    I = J + q;
+    I = max(J, rb) + q;
   } else {
     I = (int)((sqrtf(8.0f * q + 1.0f) - 1.0f) * 0.5f);
     while ((I + 1) * (I + 2) / 2 <= q) I++;
@@ -332,15 +335,17 @@ __global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int
 
 size_t tc_syrk_scratch_bytes(int n_pad) { return (size_t)(n_pad / TB + 1) * kPackTile; }
 
-cudaError_t tc_pack_f32(const float* S, int ld, int k, int nrows, void* pack, const int* active, cudaStream_t st) {
+cudaError_t tc_pack_f32(const float* S, int ld, int k, int r_first, int nrows, void* pack, const int* active,
+                        cudaStream_t st) {
   const long long nthr = (long long)nrows * 16;
   if (nthr <= 0) return cudaSuccess;
-  tc_pack_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>(S, ld, k, nrows, static_cast<uint8_t*>(pack),
-                                                                  active);
+  tc_pack_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>(S, ld, k, r_first, nrows,
+                                                                  static_cast<uint8_t*>(pack), active);
   return cudaGetLastError();
 }
 
-cudaError_t tc_update_f32(float* S, int ld, int k, int t0, int nt, int ncols, const void* pack, const void* pack2,
+cudaError_t tc_update_f32(float* S, int ld, int k, int t0, int nt, int ncols, int rb, const void* pack,
+                          const void* pack2,
                           const int* active, int* status, cudaStream_t st) {
   static int attr_dev = -1;
   int dev = 0;
@@ -352,12 +357,12 @@ cudaError_t tc_update_f32(float* S, int ld, int k, int t0, int nt, int ncols, co
   }
   int grid = 0;
   if (ncols > 0) {
-    for (int j = 0; j < ncols && j < nt; j++) grid += nt - j;
+    for (int j = 0; j < ncols && j < nt; j++) grid += nt - std::max(j, rb) > 0 ? nt - std::max(j, rb) : 0;
   } else {
     grid = nt * (nt + 1) / 2;
   }
   if (grid <= 0) return cudaSuccess;
-  tc_syrk_kernel<<<grid, 256, kSmemBytes, st>>>(S, ld, k, t0, nt, ncols > nt ? nt : ncols,
+  tc_syrk_kernel<<<grid, 256, kSmemBytes, st>>>(S, ld, k, t0, nt, ncols > nt ? nt : ncols, ncols > 0 ? rb : 0,
                                                 static_cast<const uint8_t*>(pack),
                                                 static_cast<const uint8_t*>(pack2), active, status);
   return cudaGetLastError();
@@ -365,9 +370,9 @@ cudaError_t tc_update_f32(float* S, int ld, int k, int t0, int nt, int ncols, co
 
 cudaError_t tc_syrk_f32(float* S, int ld, int k, int t0, int nt, void* scratch, const int* active, int* status,
                         cudaStream_t st) {
-  cudaError_t e = tc_pack_f32(S, ld, k, nt * TB, scratch, active, st);
+  cudaError_t e = tc_pack_f32(S, ld, k, 0, nt * TB, scratch, active, st);
   if (e != cudaSuccess) return e;
-  return tc_update_f32(S, ld, k, t0, nt, 0, scratch, nullptr, active, status, st);
+  return tc_update_f32(S, ld, k, t0, nt, 0, 0, scratch, nullptr, active, status, st);
 }
 
 }  // namespace nl

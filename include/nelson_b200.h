@@ -95,6 +95,10 @@ typedef struct {
   double update_flop;  /* algorithmic flops of those updates (2 * multiply-adds) */
   double update_bytes; /* algorithmic bytes of those updates: each updated
                           128 x 128 tile read and written once per launch */
+  float panel_ms;      /* summed device time of the diagonal-tile factorisations
+                          on the critical path (from their enqueue on the main
+                          stream, so including any wait for an SM) */
+  int panels;          /* number of those factorisations */
 } nl_phase_times;
 
 /* ---- problem: device-resident BA section -------------------------------- */

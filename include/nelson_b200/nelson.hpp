@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <fstream>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -441,6 +442,74 @@ class GaussNewton {
   Solver solver_;
   std::vector<IterationRecord> stats_;
   int iter_ = -1;
+};
+
+// ---------------------------------------------------------------------------
+// Problem files.
+// Problem / load: the visibility-list format of the reference's samples
+// (nelson/samples/Problems.h:4-12, Problems.cpp:8-30): "nCameras nPoints
+// nEdges" then nEdges (camera, point) pairs.  Returns false when the file
+// cannot be read, is truncated or holds an index out of range.
+struct Problem {
+  int nCameras = 0;
+  int nPoints = 0;
+  std::vector<std::pair<int, int>> edges;
+
+  bool load(const std::string& file) {
+    std::ifstream f(file);
+    if (!f.good()) return false;
+    int ne = 0;
+    if (!(f >> nCameras >> nPoints >> ne) || nCameras < 0 || nPoints < 0 || ne < 0) return false;
+    edges.resize(ne);
+    for (auto& e : edges) {
+      if (!(f >> e.first >> e.second)) return false;
+      if (e.first < 0 || e.first >= nCameras || e.second < 0 || e.second >= nPoints) return false;
+    }
+    return true;
+  }
+};
+
+// A BAL-style file: "num_cameras num_points num_observations", one
+// "camera point x y" line per observation, 9 parameters per camera (axis-angle,
+// t, f, k1, k2) and 3 per point.  Its pixels are -f d (P.x, P.y) / P.z about the
+// image centre; addToSection builds the equivalent BASection (9-parameter
+// cameras, principal point (0, 0), observations negated).
+struct BALData {
+  int nCameras = 0, nPoints = 0;
+  std::vector<int> cam, pt;
+  std::vector<double> obs;            // as in the file, 2 per observation
+  std::vector<double> cams, pts;      // 9 per camera, 3 per point
+
+  bool load(const std::string& file) {
+    std::ifstream f(file);
+    if (!f.good()) return false;
+    int ne = 0;
+    if (!(f >> nCameras >> nPoints >> ne) || nCameras < 0 || nPoints < 0 || ne < 0) return false;
+    cam.resize(ne);
+    pt.resize(ne);
+    obs.resize(2 * (size_t)ne);
+    for (int e = 0; e < ne; e++) {
+      if (!(f >> cam[e] >> pt[e] >> obs[2 * e] >> obs[2 * e + 1])) return false;
+      if (cam[e] < 0 || cam[e] >= nCameras || pt[e] < 0 || pt[e] >= nPoints) return false;
+    }
+    cams.resize(9 * (size_t)nCameras);
+    pts.resize(3 * (size_t)nPoints);
+    for (auto& v : cams)
+      if (!(f >> v)) return false;
+    for (auto& v : pts)
+      if (!(f >> v)) return false;
+    return true;
+  }
+
+  BASection toSection(int precision = NL_PREC_MIXED, int device = 0) const {
+    BASection ba(9, nCameras, nPoints, 0, 0, precision, 1.0, 0.0, 0.0, device);
+    ba.setParameters(cams, pts);
+    ba.parametersReady();
+    for (size_t e = 0; e < cam.size(); e++)
+      ba.addEdge(NodeId(cam[e]), NodeId(pt[e]), -obs[2 * e], -obs[2 * e + 1]);
+    ba.structureReady();
+    return ba;
+  }
 };
 
 }  // namespace nelson_b200

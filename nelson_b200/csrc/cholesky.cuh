@@ -23,37 +23,40 @@ constexpr long long kSpinLimit = 1LL << 24;  // bounded waits (~1 s worst case)
 
 // ---------------------------------------------------------------------------
 // One CTA (544 threads): factor the NB x NB diagonal tile of panel k in FP64
-// and build its inverse, both in registers.
-// Thread t owns 4x4 block (R, C), C <= R, of the lower triangle (528 blocks):
-// `a` holds A -> L, `x` holds B -> inv(L) for the same block position.  For
-// each block column jb (32 super-steps, three barriers each):
-//   (1) the owner of (jb, jb) factors its 4x4 block and inverts it;
-//   (2) owners of block column jb form L_R,jb = A_R,jb inv(L_jb,jb)' and
-//       publish it; owners of block row jb finish X_jb,C = inv(L_jb,jb) B_jb,C
-//       and publish it (right-looking forward substitution of L X = I);
-//   (3) owners right of jb apply the rank-4 update A -= L_R L_C'; owners
-//       below jb apply B_R,C -= L_R,jb X_jb,C.
-// L_kk is written back to S and inv(L_kk) (FP64, zeros above the diagonal)
-// to Linv.
+// and build its inverse, in registers.
+// Thread t owns 4x4 block (R, C), C <= R, of the lower triangle (528 blocks)
+// and one register block `t` for it: A until block column C is factored
+// (then L_R,C is written to S), afterwards B -> X = inv(L) (right-looking
+// forward substitution of L X = I).  For each block column jb (32 super-steps,
+// two barriers each):
+//   (1) the owner of (jb, jb) factors its 4x4 block and inverts it (Di);
+//   (2) owners of block column jb form L_R,jb = A_R,jb Di' and publish it;
+//       owners of block row jb finish X_jb,C = Di B_jb,C and publish it;
+//   (3) every block with jb < R applies one rank-4 update
+//       t -= L_R,jb Q_jb,C  with Q = L_C,jb' while jb < C (A part) and
+//       Q = X_jb,C once jb >= C (X part): the same instructions for both, so
+//       a warp never splits between the two.
+// L_kk is written to S and inv(L_kk) (FP64, zeros above the diagonal) to Linv.
 constexpr int PT = 544;
 constexpr int kTiles4 = (NB / 4) * (NB / 4 + 1) / 2;  // 528
 constexpr size_t kPotrfSmem = 0;
 
 template <typename T>
-static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S, int ld, int k,
+static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int ld, int k,
                                                                 double* __restrict__ Linv, int* __restrict__ status,
                                                                 const int* __restrict__ active) {
   // L of block column jb (row 4 b + u, column w at Lc[.][w][u][b]) and X of
-  // block row jb (row u, column 4 b + v at Xr[.][u][v][b]), double-buffered.
+  // block row jb (row w, column 4 b + u at Xr[.][w][u][b]), double-buffered.
   // Block index innermost: a warp's owners read consecutive block indices, so
   // the loads of the rank-4 update are free of bank conflicts.
   __shared__ double Lc[2][4][4][NB / 4];
   __shared__ double Xr[2][4][4][NB / 4];
-  __shared__ double Di[2][4][4];     // inv(L_jb,jb)
+  __shared__ double Di[2][4][4];  // inv(L_jb,jb)
   __shared__ int bad;
   if (active && !*active) return;
   const int tid = threadIdx.x;
   const size_t base = (size_t)k * NB * ld + (size_t)k * NB;
+  double* Lout = Linv + (size_t)k * NB * NB;
   if (tid == 0) bad = 0;
   int R = 0, C = 0;
   const bool own = tid < kTiles4;
@@ -64,14 +67,17 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
     C = tid - R * (R + 1) / 2;
   }
   const int r0 = 4 * R, c0 = 4 * C;
-  double a[4][4], x[4][4];
+  double t[4][4];
 #pragma unroll
   for (int u = 0; u < 4; u++)
 #pragma unroll
-    for (int v = 0; v < 4; v++) {
-      a[u][v] = (own && c0 + v <= r0 + u) ? (double)S[base + (size_t)(r0 + u) * ld + c0 + v] : 0.0;
-      x[u][v] = (own && R == C && u == v) ? 1.0 : 0.0;
-    }
+    for (int v = 0; v < 4; v++)
+      t[u][v] = (own && c0 + v <= r0 + u) ? (double)S[base + (size_t)(r0 + u) * ld + c0 + v] : 0.0;
+  // zero the strictly upper blocks of Linv (never written below)
+  for (int i = tid; i < NB * NB; i += PT) {
+    const int r = i / NB, c = i - r * NB;
+    if ((c >> 2) > (r >> 2)) Lout[i] = 0.0;
+  }
   __syncthreads();
   for (int jb = 0; jb < NB / 4; jb++) {
     const int buf = jb & 1;
@@ -82,49 +88,63 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
       double rs[4];
 #pragma unroll
       for (int j = 0; j < 4; j++) {
-        double d = a[j][j];
+        double d = t[j][j];
 #pragma unroll
-        for (int l = 0; l < j; l++) d -= a[j][l] * a[j][l];
+        for (int l = 0; l < j; l++) d -= t[j][l] * t[j][l];
         fail |= !(d > 0.0) || !isfinite(d);
         rs[j] = rsqrt(fmax(d, 1e-300));
-        a[j][j] = d * rs[j];
+        t[j][j] = d * rs[j];
 #pragma unroll
         for (int i = j + 1; i < 4; i++) {
-          double v = a[i][j];
+          double v = t[i][j];
 #pragma unroll
-          for (int l = 0; l < j; l++) v -= a[i][l] * a[j][l];
-          a[i][j] = v * rs[j];
+          for (int l = 0; l < j; l++) v -= t[i][l] * t[j][l];
+          t[i][j] = v * rs[j];
         }
       }
       if (fail) bad = 1;
-      double di[4][4];
-#pragma unroll
-      for (int c = 0; c < 4; c++)
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-          if (i < c) {
-            di[i][c] = 0.0;
-          } else if (i == c) {
-            di[i][c] = rs[i];
-          } else {
-            double v = 0.0;
-#pragma unroll
-            for (int l = c; l < i; l++) v -= a[i][l] * di[l][c];
-            di[i][c] = v * rs[i];
-          }
-        }
+      // L_jb,jb to S and the shared column
 #pragma unroll
       for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int c = 0; c < 4; c++) {
-          Di[buf][i][c] = di[i][c];
-          if (c > i) a[i][c] = 0.0;
-          Lc[buf][c][i][jb] = a[i][c];
+          const double l = c <= i ? t[i][c] : 0.0;
+          Lc[buf][c][i][jb] = l;
+          if (c <= i) S[base + (size_t)(r0 + i) * ld + c0 + c] = (T)l;
         }
+      // Di = inv(L_jb,jb) one column at a time; X_jb,jb = Di to Linv and the shared row
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        double dc[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          if (i < c) {
+            dc[i] = 0.0;
+          } else if (i == c) {
+            dc[i] = rs[i];
+          } else {
+            double v = 0.0;
+#pragma unroll
+            for (int l = c; l < i; l++) v -= t[i][l] * dc[l];
+            dc[i] = v * rs[i];
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          Di[buf][i][c] = dc[i];
+          Xr[buf][i][c][jb] = dc[i];
+          Lout[(size_t)(r0 + i) * NB + c0 + c] = dc[i];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) t[u][v] = 0.0;  // finished
     }
     __syncthreads();
-    // (2) block column jb of L, block row jb of X
+    // (2) block column jb of L (A part ends), block row jb of X (X part ends)
     if (own && C == jb && R > jb) {
+      // one row of L_R,jb = A_R,jb Di' at a time
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         double l[4];
@@ -132,17 +152,18 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
         for (int v = 0; v < 4; v++) {
           double s = 0.0;
 #pragma unroll
-          for (int w = 0; w <= v; w++) s += a[u][w] * Di[buf][v][w];
+          for (int w = 0; w <= v; w++) s += t[u][w] * Di[buf][v][w];
           l[v] = s;
         }
 #pragma unroll
         for (int v = 0; v < 4; v++) {
-          a[u][v] = l[v];
           Lc[buf][v][u][R] = l[v];
+          S[base + (size_t)(r0 + u) * ld + c0 + v] = (T)l[v];
+          t[u][v] = 0.0;  // the X block starts from zero below the diagonal
         }
       }
-    }
-    if (own && R == jb) {
+    } else if (own && R == jb && C < jb) {
+      // one column of X_jb,C = Di B_jb,C at a time
 #pragma unroll
       for (int v = 0; v < 4; v++) {
         double xx[4];
@@ -150,66 +171,38 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
         for (int u = 0; u < 4; u++) {
           double s = 0.0;
 #pragma unroll
-          for (int w = 0; w <= u; w++) s += Di[buf][u][w] * x[w][v];
+          for (int w = 0; w <= u; w++) s += Di[buf][u][w] * t[w][v];
           xx[u] = s;
         }
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-          x[u][v] = xx[u];
           Xr[buf][u][v][C] = xx[u];
+          Lout[(size_t)(r0 + u) * NB + c0 + v] = xx[u];
         }
       }
     }
     __syncthreads();
-    // (3) updates; the next step writes the other buffers, so no barrier here
-    if (own && C > jb) {
+    // (3) one rank-4 update per block below row jb; the next step writes the
+    //     other buffers, so no barrier here
+    if (own && jb < R) {
+      const double* q = (jb < C) ? &Lc[buf][0][0][0] : &Xr[buf][0][0][0];  // [w][v][b] either way
 #pragma unroll
       for (int w = 0; w < 4; w++) {
-        double lr[4], lc[4];
+        double pr[4], qc[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-          lr[u] = Lc[buf][w][u][R];
-          lc[u] = Lc[buf][w][u][C];
+          pr[u] = Lc[buf][w][u][R];
+          qc[u] = q[(w * 4 + u) * (NB / 4) + C];
         }
 #pragma unroll
         for (int u = 0; u < 4; u++)
 #pragma unroll
-          for (int v = 0; v < 4; v++) a[u][v] -= lr[u] * lc[v];
-      }
-    } else if (own && R > jb && C <= jb) {
-#pragma unroll
-      for (int w = 0; w < 4; w++) {
-        double lr[4], xr[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          lr[u] = Lc[buf][w][u][R];
-          xr[u] = Xr[buf][w][u][C];
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-#pragma unroll
-          for (int v = 0; v < 4; v++) x[u][v] -= lr[u] * xr[v];
+          for (int v = 0; v < 4; v++) t[u][v] -= pr[u] * qc[v];
       }
     }
   }
   __syncthreads();
   if (tid == 0 && bad) atomicOr(status, ST_CHOL_FAIL);
-  double* out = Linv + (size_t)k * NB * NB;
-  if (own) {
-#pragma unroll
-    for (int u = 0; u < 4; u++)
-#pragma unroll
-      for (int v = 0; v < 4; v++) {
-        const bool lower = c0 + v <= r0 + u;
-        out[(size_t)(r0 + u) * NB + c0 + v] = lower ? x[u][v] : 0.0;
-        if (lower) S[base + (size_t)(r0 + u) * ld + c0 + v] = (T)a[u][v];
-      }
-  }
-  // zero the strictly upper blocks of Linv
-  for (int i = tid; i < NB * NB; i += PT) {
-    const int r = i / NB, c = i - r * NB;
-    if ((c >> 2) > (r >> 2)) out[i] = 0.0;
-  }
 }
 
 // ---------------------------------------------------------------------------

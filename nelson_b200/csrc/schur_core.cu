@@ -311,7 +311,7 @@ class SchurCoreT final : public SchurCore {
   nl_status enqueue_factor_pairs(int* status, const int* active) {
     const bool tm = timing && !active;
     const int nT = ntiles_;
-    if (tm && (int)upd_ev_.size() < 10 * nT + 10) {
+    if (tm && (int)upd_ev_.size() < 10 * nT + 10) {  // [0, 8 nT): updates, [8 nT, 10 nT): potrf
       for (size_t i = upd_ev_.size(); i < (size_t)10 * nT + 10; i++) {
         cudaEvent_t e;
         NL_CUDA(cudaEventCreate(&e));
@@ -349,8 +349,13 @@ class SchurCoreT final : public SchurCore {
       launches += 2;
       return NL_OK;
     };
+    int npev = 0;
     auto potrf = [&](int j) {
+      const int e = 8 * nT + 2 * j;  // timing events after the update events
+      if (tm) cudaEventRecord(upd_ev_[e], st_);
       potrf_diag_kernel<T><<<1, PT, kPotrfSmem, st_>>>(S_.as<T>(), ld_, j, Linv_.as<double>(), status, active);
+      if (tm) cudaEventRecord(upd_ev_[e + 1], st_);
+      npev = j + 1;
       launches++;
     };
     auto rec = [&](int e, cudaStream_t st) { return cudaEventRecord(dev_[e], st); };
@@ -423,6 +428,14 @@ class SchurCoreT final : public SchurCore {
       times.update_launches = nupd;
       times.update_flop = upd_flop;
       times.update_bytes = upd_bytes;
+      float pt = 0;
+      for (int j = 0; j < npev; j++) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, upd_ev_[8 * nT + 2 * j], upd_ev_[8 * nT + 2 * j + 1]);
+        pt += ms;
+      }
+      times.panel_ms = pt;
+      times.panels = npev;
     }
     return NL_OK;
   }

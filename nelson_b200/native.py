@@ -65,7 +65,8 @@ class SolveReport(C.Structure):
 class PhaseTimes(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("vinv_ms", "wvinv_bs_ms", "schur_ms", "factor_ms", "solve_ms",
                                           "backsub_ms", "total_ms", "eval_ms", "update_ms")] + \
-        [("update_launches", C.c_int), ("update_flop", C.c_double), ("update_bytes", C.c_double)]
+        [("update_launches", C.c_int), ("update_flop", C.c_double), ("update_bytes", C.c_double),
+         ("panel_ms", C.c_float), ("panels", C.c_int)]
 
 
 class AdjointReport(C.Structure):

@@ -15,6 +15,7 @@ f, k1, k2.  Its increment is [dw, dt (, df, dk1, dk2)] with R <- exp(dw) R.
 """
 from __future__ import annotations
 
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -328,3 +329,97 @@ def with_fixed_nodes(p: BAProblem, ncf: int, npf: int = 0) -> BAProblem:
                      obs=p.obs, weight=p.weight, cam_fixed=cf, pt_fixed=pf, nc_fix=ncf, np_fix=npf,
                      f=p.f, cx=p.cx, cy=p.cy, cams_true=p.cams_true, pts_true=p.pts_true,
                      name=p.name + "+fixed", meta=dict(p.meta))
+
+
+# ---------------------------------------------------------------------------
+# Problem files.
+#
+# * Visibility lists in the format of the reference's Problem::load
+#   (nelson/samples/Problems.cpp:8-30): "nCameras nPoints nEdges" followed by
+#   nEdges whitespace-separated (camera, point) pairs.  `problem_from_pairs`
+#   builds a seeded synthetic BA problem on such a structure (the reference's
+#   sample does the same: random parameters on a given visibility list,
+#   nelson/samples/BASchurPerfomances.cpp:30-97).
+# * BAL-style files (header "num_cameras num_points num_observations", one
+#   "camera point x y" line per observation, then 9 parameters per camera:
+#   axis-angle, translation, f, k1, k2, then 3 per point).  Such files predict
+#   pixel = -f d (P.x, P.y) / P.z about the image centre; this library's model
+#   is f d (P.x, P.y) / P.z + (cx, cy), so a BAL problem loads with cx = cy = 0
+#   and negated observations (the same residual norms).
+
+def load_pairs(path: str):
+    """(n_cameras, n_points, cam_idx, pt_idx) of a visibility-list file."""
+    with open(path) as f:
+        tok = f.read().split()
+    if len(tok) < 3:
+        raise ValueError(f"{path}: missing header")
+    nc, npts, ne = int(tok[0]), int(tok[1]), int(tok[2])
+    if len(tok) < 3 + 2 * ne:
+        raise ValueError(f"{path}: {ne} edges announced, {(len(tok) - 3) // 2} present")
+    e = np.array(tok[3:3 + 2 * ne], dtype=np.int64).reshape(ne, 2)
+    if ne and (e[:, 0].min() < 0 or e[:, 0].max() >= nc or e[:, 1].min() < 0 or e[:, 1].max() >= npts):
+        raise ValueError(f"{path}: edge index out of range")
+    return nc, npts, e[:, 0].astype(np.int32), e[:, 1].astype(np.int32)
+
+
+def save_pairs(path: str, n_cameras: int, n_points: int, cam_idx, pt_idx) -> None:
+    with open(path, "w") as f:
+        f.write(f"{n_cameras} {n_points} {len(cam_idx)}\n")
+        for c, p in zip(cam_idx, pt_idx):
+            f.write(f"{int(c)} {int(p)}\n")
+
+
+def problem_from_pairs(n_cameras: int, n_points: int, cam_idx, pt_idx, bc: int = 9, seed: int = 1234,
+                       noise: float = 1.0) -> BAProblem:
+    """Seeded synthetic BA problem on a given visibility list: cameras on a
+    circle looking at the origin, points in a cube around it (every point is in
+    front of every camera), N(0, noise) pixel noise, perturbed initial values."""
+    rng = np.random.default_rng(seed)
+    th = 2.0 * np.pi * np.arange(n_cameras) / max(n_cameras, 1)
+    C = np.stack([10.0 * np.cos(th), 10.0 * np.sin(th), np.ones(n_cameras)], axis=1)
+    Rt = _look_at(C, np.zeros_like(C), np.array([0.0, 0.0, 1.0]))
+    tt = -np.einsum("cij,cj->ci", Rt, C)
+    intr = np.stack([rng.uniform(400.0, 600.0, n_cameras), rng.normal(0, 0.01, n_cameras),
+                     rng.normal(0, 0.01, n_cameras)], axis=1) if bc == 9 else None
+    pts = rng.uniform(-2.0, 2.0, size=(n_points, 3))
+    return _finish(rng, "pairs", bc, Rt, tt, intr, pts, np.asarray(cam_idx, np.int32),
+                   np.asarray(pt_idx, np.int32), noise=noise,
+                   meta=dict(nc=n_cameras, np=n_points, source="visibility list"))
+
+
+def load_bal(path: str) -> BAProblem:
+    """A BAL-style file as a 9-parameter BA problem (cx = cy = 0, observations
+    negated, see above); the file's parameters are the initial values."""
+    with open(path) as f:
+        tok = f.read().split()
+    nc, npts, ne = int(tok[0]), int(tok[1]), int(tok[2])
+    need = 3 + 4 * ne + 9 * nc + 3 * npts
+    if len(tok) < need:
+        raise ValueError(f"{path}: {len(tok)} numbers, {need} expected")
+    o = np.array(tok[3:3 + 4 * ne], dtype=np.float64).reshape(ne, 4)
+    q = 3 + 4 * ne
+    cams = np.array(tok[q:q + 9 * nc], dtype=np.float64).reshape(nc, 9)
+    q += 9 * nc
+    pts = np.array(tok[q:q + 3 * npts], dtype=np.float64).reshape(npts, 3)
+    cam_idx = o[:, 0].astype(np.int32)
+    pt_idx = o[:, 1].astype(np.int32)
+    if ne and (cam_idx.min() < 0 or cam_idx.max() >= nc or pt_idx.min() < 0 or pt_idx.max() >= npts):
+        raise ValueError(f"{path}: observation index out of range")
+    return BAProblem(bc=9, cams=cams, pts=pts, nc_var=nc, np_var=npts, cam_idx=cam_idx, pt_idx=pt_idx,
+                     obs=np.ascontiguousarray(-o[:, 2:4]), cx=0.0, cy=0.0, name=os.path.basename(path),
+                     meta=dict(source="BAL"))
+
+
+def save_bal(path: str, p: BAProblem) -> None:
+    """Writes a 9-parameter problem with cx = cy = 0 in the BAL layout (the
+    inverse of load_bal)."""
+    if p.bc != 9 or p.cx != 0.0 or p.cy != 0.0 or p.nc_fix or p.np_fix or p.weight is not None:
+        raise ValueError("BAL files hold unweighted 9-parameter problems about the image centre")
+    with open(path, "w") as f:
+        f.write(f"{p.nc_var} {p.np_var} {p.ne}\n")
+        for c, q, z in zip(p.cam_idx, p.pt_idx, p.obs):
+            f.write(f"{int(c)} {int(q)} {-z[0]:.17g} {-z[1]:.17g}\n")
+        for v in p.cams.reshape(-1):
+            f.write(f"{v:.17g}\n")
+        for v in p.pts.reshape(-1):
+            f.write(f"{v:.17g}\n")

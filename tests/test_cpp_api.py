@@ -44,3 +44,18 @@ def test_cpp_api_runs(tmp_path):
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "ALL OK" in r.stdout
+
+
+def test_cpp_problem_file_readers(tmp_path):
+    """The header's Problem / BALData readers (host code only, runs on CPU)."""
+    gxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no C++ compiler")
+    exe = str(tmp_path / "test_loader")
+    src = os.path.join(ROOT, "tests", "cpp", "test_loader.cpp")
+    r = subprocess.run([gxx, "-O1", "-std=c++17", "-Wall", "-Wextra", "-I" + os.path.join(ROOT, "include"), src,
+                        "-o", exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([exe, str(tmp_path)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "ALL OK" in r.stdout

@@ -13,6 +13,8 @@
 //   pt_pass_kernel   one thread per point: V_p, bV_p.
 #pragma once
 
+#include <type_traits>
+
 #include "nl_common.cuh"
 
 namespace nl {
@@ -195,9 +197,15 @@ static __global__ void __launch_bounds__(NT) cam_pass_kernel(BaDev d, T* __restr
       }
     }
     if (wuid >= 0) {
-      T* dst = W + (size_t)wuid * LW;
+      // 16-byte vector stores of the padded block
+      using V16 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+      constexpr int EPV = 16 / (int)sizeof(T);
+      __align__(16) T blk[LW];
 #pragma unroll
-      for (int i = 0; i < BC * 3; i++) dst[i] = wacc[i];
+      for (int i = 0; i < LW; i++) blk[i] = i < BC * 3 ? wacc[i] : (T)0;
+#pragma unroll
+      for (int i = 0; i < LW / EPV; i++)
+        reinterpret_cast<V16*>(W + (size_t)wuid * LW)[i] = reinterpret_cast<const V16*>(blk)[i];
     }
   }
   // deterministic CTA reduction: warp shuffles, then warps in index order

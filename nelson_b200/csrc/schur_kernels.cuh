@@ -103,13 +103,17 @@ static __global__ void __launch_bounds__(NT) wvinv_bs_kernel(SchurDev d, const T
   for (int i = 0; i < BC; i++) acc[i] = 0.0;
   for (int q = d.w_row_ptr[c] + threadIdx.x; q < d.w_row_ptr[c + 1]; q += NT) {
     const int p = d.w_col[q];
-    const T* w = W + (size_t)q * LW;
-    const T* vi = Vinv + (size_t)p * LV;
-    T v[9];
+    // blocks are padded to 16 bytes: move them as 16-byte vectors
+    using V16 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+    constexpr int EPV = 16 / (int)sizeof(T);
+    __align__(16) T w[LW], v[LV], y[LW];
 #pragma unroll
-    for (int i = 0; i < 9; i++) v[i] = vi[i];
+    for (int i = 0; i < LW / EPV; i++)
+      reinterpret_cast<V16*>(w)[i] = __ldg(reinterpret_cast<const V16*>(W + (size_t)q * LW) + i);
+#pragma unroll
+    for (int i = 0; i < LV / EPV; i++)
+      reinterpret_cast<V16*>(v)[i] = __ldg(reinterpret_cast<const V16*>(Vinv + (size_t)p * LV) + i);
     const T bv0 = bV[3 * (size_t)p], bv1 = bV[3 * (size_t)p + 1], bv2 = bV[3 * (size_t)p + 2];
-    T* y = Y + (size_t)q * LW;
 #pragma unroll
     for (int i = 0; i < BC; i++) {
       const T w0 = w[i * 3], w1 = w[i * 3 + 1], w2 = w[i * 3 + 2];
@@ -121,6 +125,11 @@ static __global__ void __launch_bounds__(NT) wvinv_bs_kernel(SchurDev d, const T
       y[i * 3 + 2] = y2;
       acc[i] += (double)y0 * (double)bv0 + (double)y1 * (double)bv1 + (double)y2 * (double)bv2;
     }
+#pragma unroll
+    for (int i = BC * 3; i < LW; i++) y[i] = (T)0;
+#pragma unroll
+    for (int i = 0; i < LW / EPV; i++)
+      reinterpret_cast<V16*>(Y + (size_t)q * LW)[i] = reinterpret_cast<const V16*>(y)[i];
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -327,7 +336,12 @@ static __global__ void backsub_kernel(SchurDev d, const T* __restrict__ W, const
   for (int s = d.w_col_ptr[p]; s < d.w_col_ptr[p + 1]; s++) {
     const int q = d.w_col_uid[s];
     const int c = d.w_row[q];
-    const T* w = W + (size_t)q * LW;
+    using V16 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+    constexpr int EPV = 16 / (int)sizeof(T);
+    __align__(16) T w[LW];
+#pragma unroll
+    for (int i = 0; i < LW / EPV; i++)
+      reinterpret_cast<V16*>(w)[i] = __ldg(reinterpret_cast<const V16*>(W + (size_t)q * LW) + i);
     const double* x = xU + (size_t)c * BC;
 #pragma unroll
     for (int i = 0; i < BC; i++) {

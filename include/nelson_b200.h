@@ -176,6 +176,15 @@ nl_status nl_rho(nl_problem* h, double mu, double old_chi2, double* out);
  * with the whole iteration on the device; trace may be NULL. */
 nl_status nl_lm_solve(nl_problem* h, const nl_lm_settings* s, nl_solve_report* rep,
                       double* trace, int trace_cap);
+/* LevenbergMarquardt<Solver>::solve on n independent problems at once (the
+ * reference solves one problem per call).  All handles must be ready and on
+ * the same device; each problem's LM sub-iteration is captured once as a CUDA
+ * graph on its handle's streams and replayed, the problems interleaved with at
+ * most two sub-iterations in flight each.  reps (may be NULL) get each
+ * problem's report; latency_ms (may be NULL) each problem's device time from
+ * the common start to its completion.  No trace is recorded. */
+nl_status nl_lm_solve_batch(nl_problem** hs, int n, const nl_lm_settings* s, nl_solve_report* reps,
+                            double* latency_ms);
 /* GaussNewton<Solver>::solve (nelson/GaussNewton.hpp:32-127). */
 nl_status nl_gn_solve(nl_problem* h, const nl_gn_settings* s, nl_solve_report* rep,
                       double* trace, int trace_cap);

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <memory>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include "ba_kernels.cuh"
@@ -62,11 +63,13 @@ struct nl_problem {
   DevBuf d_lam;
   long long launches = 0;
   DevBuf adj_vec, adj_slot2int, adj_out;  // adjoint work (allocated on first nl_adjoint)
+  cudaGraphExec_t sub_exec = nullptr;       // captured LM sub-iteration (batched solves)
   cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
   float eval_ms = 0;
   int have_jac = 0;
 
   ~nl_problem() {
+    if (sub_exec) cudaGraphExecDestroy(sub_exec);
     if (cublas) cublasDestroy(cublas);
     if (host_pin) cudaFreeHost(host_pin);
     if (ev_a) cudaEventDestroy(ev_a);
@@ -853,6 +856,167 @@ nl_status nl_lm_solve(nl_problem* h, const nl_lm_settings* st, nl_solve_report* 
   s.minScale = st->minScaleFactor;
   const long long lim = (long long)std::max(st->maxNumIt, 0) * std::max(st->maxNumSubIt, 1) + 2;
   return run_solver(h, s, rep, trace, trace_cap, (int)std::min<long long>(lim, 1 << 30));
+}
+
+nl_status nl_lm_solve_batch(nl_problem** hs, int n, const nl_lm_settings* st, nl_solve_report* reps,
+                             double* latency_ms) {
+  if (!hs || n <= 0 || !st) return NL_ERR_ARG;
+  for (int i = 0; i < n; i++) {
+    NL_CHECK_READY(hs[i]);
+    if (hs[i]->device != hs[0]->device) return NL_ERR_ARG;
+    for (int j = 0; j < i; j++)
+      if (hs[j] == hs[i]) return NL_ERR_ARG;
+  }
+  NL_CUDA(cudaSetDevice(hs[0]->device));
+  LmDev s{};
+  s.gn = 0;
+  s.maxNumIt = st->maxNumIt;
+  s.maxNumSubIt = st->maxNumSubIt;
+  s.minNumIt = st->minNumIt;
+  s.epsBVector = st->epsBVector;
+  s.epsIncSquare = st->epsIncSquare;
+  s.epsChi2 = st->epsChi2;
+  s.tau = st->tau;
+  s.penaltyV = st->penaltyV;
+  s.initV = st->initV;
+  s.maxScale = st->maxScaleFactor;
+  s.minScale = st->minScaleFactor;
+  s.trace_cap = 0;
+  s.trace_n = 1;
+  const int max_launch =
+      (int)std::min<long long>((long long)std::max(st->maxNumIt, 0) * std::max(st->maxNumSubIt, 1) + 2, 1 << 30);
+  // timing events: [0] the common start, then two per problem (launch parity)
+  struct Events {
+    std::vector<cudaEvent_t> e;
+    ~Events() {
+      for (auto x : e)
+        if (x) cudaEventDestroy(x);
+    }
+  } ev;
+  ev.e.assign(1 + 2 * (size_t)n, nullptr);
+  for (auto& x : ev.e) NL_CUDA(cudaEventCreate(&x));
+  cudaEvent_t ev_start = ev.e[0];
+  NL_CUDA(cudaEventRecord(ev_start, hs[0]->st));
+  // (1) update(true) everywhere, then one read per problem
+  for (int i = 0; i < n; i++) {
+    nl_problem* h = hs[i];
+    NL_CUDA(cudaStreamWaitEvent(h->st, ev_start, 0));
+    nl_status r = enqueue_eval(h, true, h->scal, h->scal + 1, nullptr);
+    if (r != NL_OK) return r;
+    NL_CUDA(cudaMemcpyAsync(h->host_pin, h->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  }
+  std::vector<LmDev> init(n, s);
+  std::vector<int> finished(n, 0), launched(n, 0), inflight(n, 0);
+  std::vector<double> lat(n, 0.0);
+  for (int i = 0; i < n; i++) {
+    nl_problem* h = hs[i];
+    NL_CUDA(cudaStreamSynchronize(h->st));
+    init[i].chi2 = init[i].oldChi2 = h->host_pin[0];
+    init[i].maxAbsB = h->host_pin[1];
+    if (h->host_pin[1] <= s.epsBVector) {  // SuccessAtStart
+      init[i].done = 1;
+      init[i].reason = NL_SUCCESS_AT_START;
+      init[i].iter = -1;
+      finished[i] = 1;
+      continue;
+    }
+    nl_status r = enqueue_copy_params(h, true, nullptr);  // backupSolution
+    if (r != NL_OK) return r;
+    if ((r = h->core->enqueue_hdiag(h->scal + 2)) != NL_OK) return r;
+    NL_CUDA(cudaMemcpyAsync(h->host_pin + 2, h->scal + 2, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  }
+  for (int i = 0; i < n; i++) {
+    if (finished[i]) continue;
+    nl_problem* h = hs[i];
+    NL_CUDA(cudaStreamSynchronize(h->st));
+    LmDev& q = init[i];
+    q.maxAbsHDiag = h->host_pin[2];
+    q.mu = q.tau * q.maxAbsHDiag;  // LevenbergMarquardt.hpp:58
+    q.curV = q.initV;
+    q.iter = q.subiter = q.nsub = 0;
+    q.done = q.maxNumIt <= 0 ? 1 : 0;
+    q.reason = NL_MAX_ITERATION_REACHED;
+    NL_CUDA(cudaMemcpyAsync(h->lm, &q, sizeof(LmDev), cudaMemcpyHostToDevice, h->st));
+    if (q.done) finished[i] = 1;
+    // one LM sub-iteration as a CUDA graph, captured once per handle
+    if (!h->sub_exec) {
+      NL_CUDA(cudaStreamSynchronize(h->st));
+      NL_CUDA(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeRelaxed));
+      nl_status r = enqueue_subiteration(h, nullptr);
+      cudaGraph_t g = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(h->st, &g);
+      if (r != NL_OK) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+      }
+      NL_CUDA(ce);
+      const cudaError_t ie = cudaGraphInstantiate(&h->sub_exec, g, 0);
+      cudaGraphDestroy(g);
+      NL_CUDA(ie);
+    }
+  }
+  for (int i = 0; i < n; i++)
+    if (finished[i]) lat[i] = 0.0;
+  // (2) interleave the problems: at most two sub-iterations in flight each,
+  //     `done` read back behind each launch, completion seen by event query
+  int remaining = 0;
+  for (int i = 0; i < n; i++) remaining += !finished[i];
+  while (remaining > 0) {
+    bool progress = false;
+    for (int i = 0; i < n; i++) {
+      if (finished[i]) continue;
+      nl_problem* h = hs[i];
+      int* done_pin = reinterpret_cast<int*>(h->host_pin + 8);
+      if (inflight[i] > 0) {
+        const int old = launched[i] - inflight[i];
+        cudaEvent_t e = ev.e[1 + 2 * (size_t)i + (old & 1)];
+        const cudaError_t q = cudaEventQuery(e);
+        if (q == cudaSuccess) {
+          inflight[i]--;
+          progress = true;
+          if (done_pin[old & 1] || (launched[i] >= max_launch && inflight[i] == 0)) {
+            float ms = 0;
+            NL_CUDA(cudaEventElapsedTime(&ms, ev_start, e));
+            lat[i] = ms;
+            finished[i] = 1;
+            remaining--;
+            continue;
+          }
+        } else if (q != cudaErrorNotReady) {
+          NL_CUDA(q);
+        }
+      }
+      if (inflight[i] < 2 && launched[i] < max_launch) {
+        NL_CUDA(cudaGraphLaunch(h->sub_exec, h->st));
+        NL_CUDA(cudaMemcpyAsync(done_pin + (launched[i] & 1), &h->lm->done, sizeof(int), cudaMemcpyDeviceToHost,
+                                h->st));
+        NL_CUDA(cudaEventRecord(ev.e[1 + 2 * (size_t)i + (launched[i] & 1)], h->st));
+        launched[i]++;
+        inflight[i]++;
+        progress = true;
+      }
+    }
+    if (!progress) std::this_thread::yield();
+  }
+  // (3) reports
+  for (int i = 0; i < n; i++) {
+    nl_problem* h = hs[i];
+    NL_CUDA(cudaStreamSynchronize(h->st));
+    LmDev fin;
+    NL_CUDA(cudaMemcpy(&fin, h->lm, sizeof(LmDev), cudaMemcpyDeviceToHost));
+    if (init[i].reason == NL_SUCCESS_AT_START && init[i].done) fin = init[i];
+    if (reps) {
+      reps[i].reason = fin.done ? fin.reason : NL_MAX_ITERATION_REACHED;
+      reps[i].iterations = fin.iter;
+      reps[i].subiterations = fin.nsub;
+      reps[i].n_trace = 0;
+      reps[i].chi2 = fin.chi2;
+      reps[i].mu = fin.mu;
+      reps[i].device_ms = lat[i];
+    }
+    if (latency_ms) latency_ms[i] = lat[i];
+  }
+  return NL_OK;
 }
 
 nl_status nl_gn_solve(nl_problem* h, const nl_gn_settings* st, nl_solve_report* rep, double* trace, int trace_cap) {

@@ -134,6 +134,7 @@ class SchurCoreT final : public SchurCore {
     need_s0_ = refine_sweeps > 0 || keep_schur;
     if (need_s0_) NL_TRY(S0_.alloc(sizeof(T) * (size_t)ld_ * ld_));
     if (sizeof(T) == 4 && use_tc) {
+      NL_CUDA(tc_prepare());
       tcs_half_ = (tc_syrk_scratch_bytes(ld_) + 255) / 256 * 256;
       NL_TRY(tcs_.alloc(kPackSlots * tcs_half_));
     }

@@ -344,6 +344,10 @@ cudaError_t tc_pack_f32(const float* S, int ld, int k, int r_first, int nrows, v
   return cudaGetLastError();
 }
 
+cudaError_t tc_prepare() {
+  return cudaFuncSetAttribute(tc_syrk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+}
+
 cudaError_t tc_update_f32(float* S, int ld, int k, int t0, int nt, int ncols, int rb, const void* pack,
                           const void* pack2,
                           const int* active, int* status, cudaStream_t st) {

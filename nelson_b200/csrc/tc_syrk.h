@@ -4,6 +4,10 @@
 
 namespace nl {
 
+// Sets the kernel attributes the tensor-core update needs on the current
+// device (call before capturing launches into a CUDA graph).
+cudaError_t tc_prepare();
+
 // Scratch the tensor-core update needs for a trailing matrix of n_pad rows:
 // the current panel split into BF16 hi/lo halves in UMMA canonical layout.
 size_t tc_syrk_scratch_bytes(int n_pad);

@@ -87,7 +87,7 @@ EXPORTS = [
     "nl_rollback", "nl_max_abs_b", "nl_chi2", "nl_rho", "nl_lm_solve", "nl_gn_solve", "nl_phase_timings",
     "nl_kernel_launches", "nl_solver_create", "nl_solver_destroy", "nl_solver_set_hessian",
     "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_selftest_tc_update", "nl_ba_cost_noalloc",
-    "nl_adjoint",
+    "nl_adjoint", "nl_lm_solve_batch",
     "nl_status_string",
     "nl_version",
 ]
@@ -121,6 +121,7 @@ def load(build_if_missing: bool = True):
     L.nl_solver_create.argtypes = [C.POINTER(SolverDesc), vp, vp, vp, C.POINTER(vp)]
     L.nl_solver_compute_increment.argtypes = [vp, d, d, vp, vp, C.POINTER(i)]
     L.nl_selftest_tc_update.argtypes = [i, C.c_ulonglong, i, C.POINTER(d)]
+    L.nl_lm_solve_batch.argtypes = [C.POINTER(vp), i, C.POINTER(LMSettings), vp, vp]
     L.nl_adjoint.argtypes = [vp, vp, vp, i, vp, vp, vp, vp, C.POINTER(AdjointReport)]
     L.nl_ba_cost_noalloc.argtypes = [i, i, vp, vp, vp, vp, vp, vp, d, d, d, vp, vp]
     for name in EXPORTS:  # fails loudly if the library lacks an entry point
@@ -332,6 +333,20 @@ class BAProblemGPU:
         v = C.c_longlong()
         self._c(self.L.nl_kernel_launches(self.h, C.byref(v)), "nl_kernel_launches")
         return v.value
+
+
+def lm_solve_batch(problems, settings=None):
+    """LM on many BAProblemGPU handles at once (nl_lm_solve_batch): returns
+    (reasons, final chi2 array, iterations array, per-problem latency in ms)."""
+    L = load()
+    n = len(problems)
+    hs = (C.c_void_p * n)(*[p.h for p in problems])
+    reps = (SolveReport * n)()
+    lat = np.zeros(n)
+    s = settings or LMSettings()
+    _chk(L, L.nl_lm_solve_batch(hs, n, C.byref(s), C.cast(reps, C.c_void_p), _p(lat)), "nl_lm_solve_batch")
+    return ([REASONS[r.reason] for r in reps], np.array([r.chi2 for r in reps]),
+            np.array([r.iterations for r in reps]), lat)
 
 
 def selftest_tc_update(ntiles=8, seed=1, device=0) -> float:

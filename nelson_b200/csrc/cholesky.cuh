@@ -15,6 +15,7 @@
 #pragma once
 
 #include "nl_common.cuh"
+#include "tc_pack_layout.cuh"
 
 namespace nl {
 
@@ -221,6 +222,7 @@ constexpr size_t trsm_smem() {
 template <typename T>
 static __global__ void __launch_bounds__(256) trsm_kernel(T* __restrict__ S, int ld, int k, int row_begin, int nrows,
                                                           const double* __restrict__ Linv,
+                                                          uint8_t* __restrict__ pack,
                                                           const int* __restrict__ active) {
   extern __shared__ unsigned char smraw[];
   T* sL = reinterpret_cast<T*>(smraw);      // sL[l][j] = Linv[j][l], (NB + 1) stride
@@ -282,6 +284,29 @@ static __global__ void __launch_bounds__(256) trsm_kernel(T* __restrict__ S, int
     if (rr < nr) {
 #pragma unroll
       for (int v = 0; v < 8; v++) S[(size_t)(r0 + rr) * ld + (size_t)k * NB + tx + 16 * v] = acc[u][v];
+    }
+  }
+  if (sizeof(T) == 4 && pack) {
+    // BF16 hi/lo pack of this slab for the tensor-core update: stage it
+    // row-major over the operand buffer (64 x 130 floats fit in sA), then
+    // each item is 8 consecutive columns of one row
+    constexpr int kSt = NB + 2;
+    static_assert(TRSM_ROWS * kSt <= NB * (TRSM_ROWS + 1), "staging fits the operand buffer");
+    float* st = reinterpret_cast<float*>(sA);
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int v = 0; v < 8; v++) st[(ty * 4 + u) * kSt + tx + 16 * v] = (float)acc[u][v];
+    __syncthreads();
+    const int rel0 = r0 - (k + 1) * NB;  // pack rows start below the diagonal tile
+    for (int i = tid; i < TRSM_ROWS * 16; i += 256) {
+      const int rr = i >> 4, h = i & 15;
+      if (rr >= nr) continue;
+      float x[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) x[q] = st[rr * kSt + 8 * h + q];
+      tc_pack_store8(pack, tc_pack_offset(rel0 + rr, h), x);
     }
   }
 }

@@ -63,7 +63,7 @@ struct nl_problem {
   DevBuf d_lam;
   long long launches = 0;
   DevBuf adj_vec, adj_slot2int, adj_out;  // adjoint work (allocated on first nl_adjoint)
-  cudaGraphExec_t sub_exec = nullptr;       // captured LM sub-iteration (batched solves)
+  cudaGraphExec_t sub_exec = nullptr;       // captured LM sub-iteration without trace (batched solves)
   cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
   float eval_ms = 0;
   int have_jac = 0;
@@ -391,6 +391,26 @@ nl_status upload_params(nl_problem* h) {
   return NL_OK;
 }
 
+// One LM / GN sub-iteration captured as a CUDA graph on the handle's streams
+// (the kernels are predicated on device flags, so the same graph serves every
+// sub-iteration); `trace` is baked into the graph.
+nl_status capture_subiteration(nl_problem* h, double* trace, cudaGraphExec_t* out) {
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  NL_CUDA(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeRelaxed));
+  nl_status r = enqueue_subiteration(h, trace);
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(h->st, &g);
+  if (r != NL_OK) {
+    if (g) cudaGraphDestroy(g);
+    return r;
+  }
+  NL_CUDA(ce);
+  const cudaError_t ie = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  NL_CUDA(ie);
+  return NL_OK;
+}
+
 // Solve driver shared by LM and GN (the host only relaunches the fixed
 // sub-iteration sequence and watches the `done` flag one launch behind).
 nl_status run_solver(nl_problem* h, LmDev& init, nl_solve_report* rep, double* trace, int trace_cap, int max_launch) {
@@ -444,6 +464,8 @@ nl_status run_solver(nl_problem* h, LmDev& init, nl_solve_report* rep, double* t
   int* done_pin = reinterpret_cast<int*>(h->host_pin + 8);
   done_pin[0] = done_pin[1] = init.done;
   int launched = 0;
+  // stream launches, not a captured graph: graph nodes do not keep the
+  // streams' priorities, and the factorisation's critical path relies on them
   while (!init.done && launched < max_launch) {
     if ((r = enqueue_subiteration(h, dtrace)) != NL_OK) return r;
     NL_CUDA(cudaMemcpyAsync(done_pin + (launched & 1), &h->lm->done, sizeof(int), cudaMemcpyDeviceToHost, h->st));
@@ -940,19 +962,8 @@ nl_status nl_lm_solve_batch(nl_problem** hs, int n, const nl_lm_settings* st, nl
     if (q.done) finished[i] = 1;
     // one LM sub-iteration as a CUDA graph, captured once per handle
     if (!h->sub_exec) {
-      NL_CUDA(cudaStreamSynchronize(h->st));
-      NL_CUDA(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeRelaxed));
-      nl_status r = enqueue_subiteration(h, nullptr);
-      cudaGraph_t g = nullptr;
-      const cudaError_t ce = cudaStreamEndCapture(h->st, &g);
-      if (r != NL_OK) {
-        if (g) cudaGraphDestroy(g);
-        return r;
-      }
-      NL_CUDA(ce);
-      const cudaError_t ie = cudaGraphInstantiate(&h->sub_exec, g, 0);
-      cudaGraphDestroy(g);
-      NL_CUDA(ie);
+      nl_status r = capture_subiteration(h, nullptr, &h->sub_exec);
+      if (r != NL_OK) return r;
     }
   }
   for (int i = 0; i < n; i++)

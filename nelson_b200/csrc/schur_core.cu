@@ -278,7 +278,7 @@ class SchurCoreT final : public SchurCore {
     const int below = ld_ - (k + 1) * NB;
     if (below > 0) {
       trsm_kernel<T><<<cdiv(below, TRSM_ROWS), 256, trsm_smem<T>(), st_>>>(S_.as<T>(), ld_, k, (k + 1) * NB, below,
-                                                                            Linv_.as<double>(), active);
+                                                                            Linv_.as<double>(), nullptr, active);
       launches++;
       if (sizeof(T) == 4 && use_tc) {
         NL_CUDA(tc_pack_f32(reinterpret_cast<const float*>(S_.p), ld_, k, 0, below, pack_slot(k), active, st_));
@@ -343,11 +343,10 @@ class SchurCoreT final : public SchurCore {
     // TRSM + pack of panel j's rows [r0, r0 + nrows) (absolute rows, tile aligned)
     auto trsm_pack = [&](int j, int r0, int nrows, cudaStream_t st) -> nl_status {
       if (nrows <= 0) return NL_OK;
+      // the TRSM writes the BF16 pack of its rows in its epilogue
       trsm_kernel<T><<<cdiv(nrows, TRSM_ROWS), 256, trsm_smem<T>(), st>>>(S_.as<T>(), ld_, j, r0, nrows,
-                                                                           Linv_.as<double>(), active);
-      NL_CUDA(tc_pack_f32(reinterpret_cast<const float*>(S_.p), ld_, j, r0 - (j + 1) * NB, nrows, pack_slot(j),
-                          active, st));
-      launches += 2;
+                                                                           Linv_.as<double>(), pack_slot(j), active);
+      launches++;
       return NL_OK;
     };
     int npev = 0;

@@ -30,6 +30,7 @@
 #include <stdint.h>
 
 #include "nl_common.cuh"
+#include "tc_pack_layout.cuh"
 #include "tc_syrk.h"
 
 namespace nl {
@@ -41,6 +42,7 @@ constexpr int kTileBytes = TB * TB * 2;  // one BF16 operand tile (32 KB)
 constexpr int kPackTile = 2 * kTileBytes;  // hi + lo
 constexpr int kChunkK = 32;                // K columns per pipeline chunk
 constexpr int kChunkBytes = TB * kChunkK * 2;  // one operand chunk: 8 KB
+static_assert(kChunkBytes == kPackChunkBytes && kTileBytes == kPackHalfBytes, "pack layout");
 constexpr int kChunksPerPanel = TB / kChunkK;  // 4
 constexpr long long kWaitLimit = 1LL << 22;
 
@@ -147,17 +149,7 @@ __global__ void tc_pack_kernel(const float* __restrict__ S, int ld, int k, int r
   const float4 a = *reinterpret_cast<const float4*>(src);
   const float4 b = *reinterpret_cast<const float4*>(src + 4);
   const float x[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-  __align__(16) __nv_bfloat16 hi[8], lo[8];
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-    hi[i] = __float2bfloat16_rn(x[i]);
-    lo[i] = __float2bfloat16_rn(x[i] - __bfloat162float(hi[i]));
-  }
-  const int tile = r / TB, rr = r % TB, g = rr >> 3, ri = rr & 7;
-  const int c = h >> 2, hh = h & 3;  // K-chunk of 32 columns, core column inside it
-  const size_t off = (size_t)tile * kPackTile + (size_t)c * kChunkBytes + (size_t)((4 * g + hh) * 128 + ri * 16);
-  *reinterpret_cast<uint4*>(pack + off) = *reinterpret_cast<const uint4*>(hi);
-  *reinterpret_cast<uint4*>(pack + off + kTileBytes) = *reinterpret_cast<const uint4*>(lo);
+  tc_pack_store8(pack, tc_pack_offset(r, h), x);
 }
 
 // ---------------------------------------------------------------------------

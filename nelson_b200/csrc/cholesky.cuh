@@ -5,7 +5,7 @@
 // used at nelson/SolverCholeskySchur.hpp:136-140).  S is stored dense,
 // row-major, lower triangle, n padded to a multiple of NB = 128 (identity on
 // the padding).  Per 128-wide panel k:
-//   potrf_diag_kernel  FP64 factor of the diagonal tile and its inverse (one CTA)
+//   potrf_diag_kernel  factor of the diagonal tile and its inverse (one CTA)
 //   trsm_kernel        L_ik = A_ik L_kk^-T as a product with the inverse
 //   syrk update        A_ij -= L_ik L_jk' on the trailing lower triangle
 //                      (tensor-core kernel in tc_syrk.cu for the mixed path,
@@ -23,8 +23,11 @@ constexpr int NB = 128;
 constexpr long long kSpinLimit = 1LL << 24;  // bounded waits (~1 s worst case)
 
 // ---------------------------------------------------------------------------
-// One CTA (544 threads): factor the NB x NB diagonal tile of panel k in FP64
-// and build its inverse, in registers.
+// One CTA (544 threads): factor the NB x NB diagonal tile of panel k in the
+// storage precision T (FP64 for the FP64 path; FP32 for the mixed path, whose
+// trailing updates and off-diagonal solves are FP32-accurate as well and whose
+// factor only preconditions the FP64 refinement) and build its inverse, in
+// registers.
 // Thread t owns 4x4 block (R, C), C <= R, of the lower triangle (528 blocks)
 // and one register block `t` for it: A until block column C is factored
 // (then L_R,C is written to S), afterwards B -> X = inv(L) (right-looking
@@ -37,8 +40,13 @@ constexpr long long kSpinLimit = 1LL << 24;  // bounded waits (~1 s worst case)
 //       t -= L_R,jb Q_jb,C  with Q = L_C,jb' while jb < C (A part) and
 //       Q = X_jb,C once jb >= C (X part): the same instructions for both, so
 //       a warp never splits between the two.
-// L_kk is written to S and inv(L_kk) (FP64, zeros above the diagonal) to Linv.
+// L_kk is written to S and inv(L_kk) (as FP64, zeros above the diagonal) to Linv.
 constexpr int PT = 544;
+
+// 1 / sqrt of a pivot, clamped away from zero (a non-positive pivot is
+// flagged separately)
+__device__ inline float pivot_rsqrt(float d) { return rsqrtf(fmaxf(d, 1e-30f)); }
+__device__ inline double pivot_rsqrt(double d) { return rsqrt(fmax(d, 1e-300)); }
 constexpr int kTiles4 = (NB / 4) * (NB / 4 + 1) / 2;  // 528
 constexpr size_t kPotrfSmem = 0;
 
@@ -50,9 +58,9 @@ static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int 
   // block row jb (row w, column 4 b + u at Xr[.][w][u][b]), double-buffered.
   // Block index innermost: a warp's owners read consecutive block indices, so
   // the loads of the rank-4 update are free of bank conflicts.
-  __shared__ double Lc[2][4][4][NB / 4];
-  __shared__ double Xr[2][4][4][NB / 4];
-  __shared__ double Di[2][4][4];  // inv(L_jb,jb)
+  __shared__ T Lc[2][4][4][NB / 4];
+  __shared__ T Xr[2][4][4][NB / 4];
+  __shared__ T Di[2][4][4];  // inv(L_jb,jb)
   __shared__ int bad;
   if (active && !*active) return;
   const int tid = threadIdx.x;
@@ -68,12 +76,12 @@ static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int 
     C = tid - R * (R + 1) / 2;
   }
   const int r0 = 4 * R, c0 = 4 * C;
-  double t[4][4];
+  T t[4][4];
 #pragma unroll
   for (int u = 0; u < 4; u++)
 #pragma unroll
     for (int v = 0; v < 4; v++)
-      t[u][v] = (own && c0 + v <= r0 + u) ? (double)S[base + (size_t)(r0 + u) * ld + c0 + v] : 0.0;
+      t[u][v] = (own && c0 + v <= r0 + u) ? S[base + (size_t)(r0 + u) * ld + c0 + v] : (T)0;
   // zero the strictly upper blocks of Linv (never written below)
   for (int i = tid; i < NB * NB; i += PT) {
     const int r = i / NB, c = i - r * NB;
@@ -86,18 +94,18 @@ static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int 
     //     multiplications only: Di[i][i] = 1 / L_ii is that rsqrt)
     if (own && R == jb && C == jb) {
       bool fail = false;
-      double rs[4];
+      T rs[4];
 #pragma unroll
       for (int j = 0; j < 4; j++) {
-        double d = t[j][j];
+        T d = t[j][j];
 #pragma unroll
         for (int l = 0; l < j; l++) d -= t[j][l] * t[j][l];
-        fail |= !(d > 0.0) || !isfinite(d);
-        rs[j] = rsqrt(fmax(d, 1e-300));
+        fail |= !(d > (T)0) || !isfinite(d);
+        rs[j] = pivot_rsqrt(d);
         t[j][j] = d * rs[j];
 #pragma unroll
         for (int i = j + 1; i < 4; i++) {
-          double v = t[i][j];
+          T v = t[i][j];
 #pragma unroll
           for (int l = 0; l < j; l++) v -= t[i][l] * t[j][l];
           t[i][j] = v * rs[j];
@@ -109,22 +117,22 @@ static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int 
       for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int c = 0; c < 4; c++) {
-          const double l = c <= i ? t[i][c] : 0.0;
+          const T l = c <= i ? t[i][c] : (T)0;
           Lc[buf][c][i][jb] = l;
-          if (c <= i) S[base + (size_t)(r0 + i) * ld + c0 + c] = (T)l;
+          if (c <= i) S[base + (size_t)(r0 + i) * ld + c0 + c] = l;
         }
       // Di = inv(L_jb,jb) one column at a time; X_jb,jb = Di to Linv and the shared row
 #pragma unroll
       for (int c = 0; c < 4; c++) {
-        double dc[4];
+        T dc[4];
 #pragma unroll
         for (int i = 0; i < 4; i++) {
           if (i < c) {
-            dc[i] = 0.0;
+            dc[i] = (T)0;
           } else if (i == c) {
             dc[i] = rs[i];
           } else {
-            double v = 0.0;
+            T v = (T)0;
 #pragma unroll
             for (int l = c; l < i; l++) v -= t[i][l] * dc[l];
             dc[i] = v * rs[i];
@@ -134,7 +142,7 @@ static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int 
         for (int i = 0; i < 4; i++) {
           Di[buf][i][c] = dc[i];
           Xr[buf][i][c][jb] = dc[i];
-          Lout[(size_t)(r0 + i) * NB + c0 + c] = dc[i];
+          Lout[(size_t)(r0 + i) * NB + c0 + c] = (double)dc[i];
         }
       }
 #pragma unroll
@@ -148,10 +156,10 @@ static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int 
       // one row of L_R,jb = A_R,jb Di' at a time
 #pragma unroll
       for (int u = 0; u < 4; u++) {
-        double l[4];
+        T l[4];
 #pragma unroll
         for (int v = 0; v < 4; v++) {
-          double s = 0.0;
+          T s = (T)0;
 #pragma unroll
           for (int w = 0; w <= v; w++) s += t[u][w] * Di[buf][v][w];
           l[v] = s;
@@ -159,7 +167,7 @@ static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int 
 #pragma unroll
         for (int v = 0; v < 4; v++) {
           Lc[buf][v][u][R] = l[v];
-          S[base + (size_t)(r0 + u) * ld + c0 + v] = (T)l[v];
+          S[base + (size_t)(r0 + u) * ld + c0 + v] = l[v];
           t[u][v] = 0.0;  // the X block starts from zero below the diagonal
         }
       }
@@ -167,10 +175,10 @@ static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int 
       // one column of X_jb,C = Di B_jb,C at a time
 #pragma unroll
       for (int v = 0; v < 4; v++) {
-        double xx[4];
+        T xx[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-          double s = 0.0;
+          T s = (T)0;
 #pragma unroll
           for (int w = 0; w <= u; w++) s += Di[buf][u][w] * t[w][v];
           xx[u] = s;
@@ -178,7 +186,7 @@ static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int 
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           Xr[buf][u][v][C] = xx[u];
-          Lout[(size_t)(r0 + u) * NB + c0 + v] = xx[u];
+          Lout[(size_t)(r0 + u) * NB + c0 + v] = (double)xx[u];
         }
       }
     }
@@ -186,10 +194,10 @@ static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int 
     // (3) one rank-4 update per block below row jb; the next step writes the
     //     other buffers, so no barrier here
     if (own && jb < R) {
-      const double* q = (jb < C) ? &Lc[buf][0][0][0] : &Xr[buf][0][0][0];  // [w][v][b] either way
+      const T* q = (jb < C) ? &Lc[buf][0][0][0] : &Xr[buf][0][0][0];  // [w][v][b] either way
 #pragma unroll
       for (int w = 0; w < 4; w++) {
-        double pr[4], qc[4];
+        T pr[4], qc[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           pr[u] = Lc[buf][w][u][R];

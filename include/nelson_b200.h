@@ -99,6 +99,11 @@ typedef struct {
                           on the critical path (from their enqueue on the main
                           stream, so including any wait for an SM) */
   int panels;          /* number of those factorisations */
+  float wait_ms;       /* main-stream time between a diagonal-tile factor's end
+                          and the start of the next row-tile TRSM (waiting for
+                          the auxiliary stream's column updates) */
+  float first_ms;      /* main-stream time of the row-tile TRSMs and the
+                          diagonal-tile updates (8-CTA kernels), incl. launch gaps */
 } nl_phase_times;
 
 /* ---- problem: device-resident BA section -------------------------------- */

@@ -40,7 +40,7 @@ constexpr long long kSpinLimit = 1LL << 24;  // bounded waits (~1 s worst case)
 //       t -= L_R,jb Q_jb,C  with Q = L_C,jb' while jb < C (A part) and
 //       Q = X_jb,C once jb >= C (X part): the same instructions for both, so
 //       a warp never splits between the two.
-// L_kk is written to S and inv(L_kk) (as FP64, zeros above the diagonal) to Linv.
+// L_kk is written to S and inv(L_kk) (zeros above the diagonal) to Linv.
 constexpr int PT = 544;
 
 // 1 / sqrt of a pivot, clamped away from zero (a non-positive pivot is
@@ -52,7 +52,7 @@ constexpr size_t kPotrfSmem = 0;
 
 template <typename T>
 static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int ld, int k,
-                                                                double* __restrict__ Linv, int* __restrict__ status,
+                                                                T* __restrict__ Linv, int* __restrict__ status,
                                                                 const int* __restrict__ active) {
   // L of block column jb (row 4 b + u, column w at Lc[.][w][u][b]) and X of
   // block row jb (row w, column 4 b + u at Xr[.][w][u][b]), double-buffered.
@@ -65,7 +65,7 @@ static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int 
   if (active && !*active) return;
   const int tid = threadIdx.x;
   const size_t base = (size_t)k * NB * ld + (size_t)k * NB;
-  double* Lout = Linv + (size_t)k * NB * NB;
+  T* Lout = Linv + (size_t)k * NB * NB;
   if (tid == 0) bad = 0;
   int R = 0, C = 0;
   const bool own = tid < kTiles4;
@@ -85,7 +85,7 @@ static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int 
   // zero the strictly upper blocks of Linv (never written below)
   for (int i = tid; i < NB * NB; i += PT) {
     const int r = i / NB, c = i - r * NB;
-    if ((c >> 2) > (r >> 2)) Lout[i] = 0.0;
+    if ((c >> 2) > (r >> 2)) Lout[i] = (T)0;
   }
   __syncthreads();
   for (int jb = 0; jb < NB / 4; jb++) {
@@ -142,7 +142,7 @@ static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int 
         for (int i = 0; i < 4; i++) {
           Di[buf][i][c] = dc[i];
           Xr[buf][i][c][jb] = dc[i];
-          Lout[(size_t)(r0 + i) * NB + c0 + c] = (double)dc[i];
+          Lout[(size_t)(r0 + i) * NB + c0 + c] = dc[i];
         }
       }
 #pragma unroll
@@ -186,7 +186,7 @@ static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int 
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           Xr[buf][u][v][C] = xx[u];
-          Lout[(size_t)(r0 + u) * NB + c0 + v] = (double)xx[u];
+          Lout[(size_t)(r0 + u) * NB + c0 + v] = xx[u];
         }
       }
     }
@@ -229,7 +229,7 @@ constexpr size_t trsm_smem() {
 
 template <typename T>
 static __global__ void __launch_bounds__(256) trsm_kernel(T* __restrict__ S, int ld, int k, int row_begin, int nrows,
-                                                          const double* __restrict__ Linv,
+                                                          const T* __restrict__ Linv,
                                                           uint8_t* __restrict__ pack,
                                                           const int* __restrict__ active) {
   extern __shared__ unsigned char smraw[];
@@ -241,16 +241,16 @@ static __global__ void __launch_bounds__(256) trsm_kernel(T* __restrict__ S, int
   const int nr = min(TRSM_ROWS, row_begin + nrows - r0);
   if (nr <= 0) return;
   // staging: 16 independent loads in flight per thread before the stores
-  const double* Li = Linv + (size_t)k * NB * NB;
+  const T* Li = Linv + (size_t)k * NB * NB;
 #pragma unroll 1
   for (int i0 = tid; i0 < NB * NB; i0 += 256 * 16) {
-    double v[16];
+    T v[16];
 #pragma unroll
     for (int u = 0; u < 16; u++) v[u] = __ldg(Li + i0 + 256 * u);
 #pragma unroll
     for (int u = 0; u < 16; u++) {
       const int i = i0 + 256 * u, j = i / NB, l = i - j * NB;
-      sL[l * (NB + 1) + j] = (T)v[u];
+      sL[l * (NB + 1) + j] = v[u];
     }
   }
 #pragma unroll 1
@@ -315,6 +315,151 @@ static __global__ void __launch_bounds__(256) trsm_kernel(T* __restrict__ S, int
 #pragma unroll
       for (int q = 0; q < 8; q++) x[q] = st[rr * kSt + 8 * h + q];
       tc_pack_store8(pack, tc_pack_offset(rel0 + rr, h), x);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Critical-path kernels of the tensor-core schedule (FP32).  Each runs as 8
+// CTAs of 256 threads, CTA c owning a 16-row slice of one 128 x 128 tile:
+//   trsm_tile_kernel    L_(j+1),j = A_(j+1),j inv(L_jj)' for row tile j+1 of
+//                       panel j, and its BF16 pack
+//   diag_update_kernel  A_tt -= sum_p L_t,p L_t,p' on diagonal tile t over
+//                       panels p in [p0, p0 + np)
+// Thread (w, lane) of a 16 x 128 slice computes slice rows (lane >> 2) + 8 h
+// (h < 2) and columns 16 w + (lane & 3) + 4 m (m < 4).  Both operands stay
+// row-major in shared memory (row stride 132 floats) and are read as float4
+// along K: the 8 row addresses of an A load and the 4 of a B load fall in
+// distinct banks, so every warp load is one wavefront, and the 32 FMAs per
+// 6 loads keep the FP32 pipe, not shared memory, the limit.
+constexpr int kSliceRows = 16;
+constexpr int kSliceCtas = NB / kSliceRows;  // 8
+constexpr int kSlLd = NB + 4;                // 132
+constexpr size_t kTrsmTileSmem = sizeof(float) * (size_t)(NB + kSliceRows) * kSlLd;  // 76,032 B
+constexpr size_t kDiagUpdSmem = sizeof(float) * (size_t)NB * kSlLd;                 // 67,584 B per panel
+
+// acc[h][m] += sum_l a_h[l] b[16 w + (lane & 3) + 4 m][l], l < NB
+__device__ inline void slice_mma(const float* __restrict__ a0, const float* __restrict__ a1,
+                                 const float* __restrict__ sb, int lane, int w, float acc[2][4]) {
+  const float* pb = sb + (16 * w + (lane & 3)) * kSlLd;
+#pragma unroll 4
+  for (int l = 0; l < NB; l += 4) {
+    float4 a[2], b[4];
+    a[0] = *reinterpret_cast<const float4*>(a0 + l);
+    a[1] = *reinterpret_cast<const float4*>(a1 + l);
+#pragma unroll
+    for (int m = 0; m < 4; m++) b[m] = *reinterpret_cast<const float4*>(pb + 4 * m * kSlLd + l);
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+        acc[h][m] = fmaf(a[h].x, b[m].x, acc[h][m]);
+        acc[h][m] = fmaf(a[h].y, b[m].y, acc[h][m]);
+        acc[h][m] = fmaf(a[h].z, b[m].z, acc[h][m]);
+        acc[h][m] = fmaf(a[h].w, b[m].w, acc[h][m]);
+      }
+  }
+}
+
+// 16-byte global -> shared copies that complete asynchronously: a kernel
+// issues all of its staging before one wait, so the staging costs one L2 /
+// HBM round trip however loaded the memory system is
+__device__ inline void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ inline void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// rows x 128 FP32 columns (row stride ld) into shared memory (stride kSlLd)
+__device__ inline void stage_rows_f32(const float* __restrict__ src, size_t ld, int rows, float* __restrict__ dst,
+                                      int tid) {
+  for (int e = tid; e < rows * NB / 4; e += 256) {
+    const int r = e >> 5, c4 = e & 31;
+    cp_async16(dst + r * kSlLd + 4 * c4, src + (size_t)r * ld + 4 * c4);
+  }
+}
+
+static __global__ void __launch_bounds__(256) trsm_tile_kernel(float* __restrict__ S, int ld, int j,
+                                                               const float* __restrict__ Linv,
+                                                               uint8_t* __restrict__ pack,
+                                                               const int* __restrict__ active) {
+  extern __shared__ float4 smf4[];
+  float* sb = reinterpret_cast<float*>(smf4);  // inv(L_jj), row i = output column i
+  float* sa = sb + NB * kSlLd;                 // the slice's 16 rows of A_(j+1),j
+  if (active && !*active) return;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int rel0 = blockIdx.x * kSliceRows;  // first slice row within the tile
+  float* A = S + (size_t)((j + 1) * NB + rel0) * ld + (size_t)j * NB;
+  stage_rows_f32(Linv + (size_t)j * NB * NB, NB, NB, sb, tid);  // zeros above the diagonal included
+  stage_rows_f32(A, ld, kSliceRows, sa, tid);
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  float acc[2][4] = {};
+  const float* a0 = sa + (lane >> 2) * kSlLd;
+  slice_mma(a0, a0 + 8 * kSlLd, sb, lane, w, acc);
+  // stage the slice of L row-major over the A rows, then store rows to S
+  // (float4) and the pack (8 consecutive columns per item)
+  __syncthreads();
+#pragma unroll
+  for (int h = 0; h < 2; h++)
+#pragma unroll
+    for (int m = 0; m < 4; m++) sa[((lane >> 2) + 8 * h) * kSlLd + 16 * w + (lane & 3) + 4 * m] = acc[h][m];
+  __syncthreads();
+  for (int e = tid; e < kSliceRows * NB / 4; e += 256) {
+    const int r = e >> 5, c4 = e & 31;
+    *reinterpret_cast<float4*>(A + (size_t)r * ld + 4 * c4) = *reinterpret_cast<const float4*>(sa + r * kSlLd + 4 * c4);
+  }
+  if (pack) {
+    for (int e = tid; e < kSliceRows * 16; e += 256) {
+      const int r = e >> 4, h = e & 15;
+      float x[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) x[q] = sa[r * kSlLd + 8 * h + q];
+      tc_pack_store8(pack, tc_pack_offset(rel0 + r, h), x);
+    }
+  }
+}
+
+// Slice c owns tile rows 8c .. 8c+7 and 127-8c-7 .. 127-8c: equal shares of
+// the lower triangle.  A_tt's lower triangle only is written.  np <= 2 panels,
+// each staged in its own buffer (np x kDiagUpdSmem bytes of shared memory).
+__device__ inline int diag_slice_row(int c, int p) { return p < 8 ? 8 * c + p : NB - 1 - 8 * c - (p - 8); }
+
+static __global__ void __launch_bounds__(256) diag_update_kernel(float* __restrict__ S, int ld, int t, int p0, int np,
+                                                                 const int* __restrict__ active) {
+  extern __shared__ float4 smf4[];
+  float* sm = reinterpret_cast<float*>(smf4);  // L_t,p (all 128 rows) per panel
+  if (active && !*active) return;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, c = blockIdx.x;
+  const int ra = diag_slice_row(c, lane >> 2), rb = diag_slice_row(c, 8 + (lane >> 2));
+  const float* T0 = S + (size_t)t * NB * ld + (size_t)p0 * NB;
+  stage_rows_f32(T0, ld, NB, sm, tid);
+  cp_async_commit();
+  if (np > 1) stage_rows_f32(T0 + NB, ld, NB, sm + NB * kSlLd, tid);
+  cp_async_commit();
+  float acc[2][4] = {};
+  cp_async_wait<1>();
+  __syncthreads();
+  slice_mma(sm + ra * kSlLd, sm + rb * kSlLd, sm, lane, w, acc);
+  if (np > 1) {
+    cp_async_wait<0>();
+    __syncthreads();
+    const float* sb = sm + NB * kSlLd;
+    slice_mma(sb + ra * kSlLd, sb + rb * kSlLd, sb, lane, w, acc);
+  }
+  float* D = S + (size_t)t * NB * ld + (size_t)t * NB;
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const int r = h ? rb : ra;
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      const int i = 16 * w + (lane & 3) + 4 * m;
+      if (i <= r) D[(size_t)r * ld + i] -= acc[h][m];
     }
   }
 }
@@ -430,16 +575,20 @@ __device__ inline void load4_cg(const double* p, double* v) {
 }
 
 constexpr int SV = 512;
-constexpr size_t kTrsvSmem = sizeof(double) * NB * NB;
+template <typename T>
+constexpr size_t trsv_smem() {
+  return sizeof(T) * NB * NB;
+}
 
 template <typename T>
 static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict__ L, int ld, int ntiles,
-                                                             const double* __restrict__ Linv,
+                                                             const T* __restrict__ Linv,
                                                              const double* __restrict__ b, double* __restrict__ y,
                                                              int* __restrict__ ticket, int* __restrict__ flags,
                                                              int epoch, int* __restrict__ status,
                                                              const int* __restrict__ active) {
-  extern __shared__ double sLi[];  // Linv_I, NB x NB
+  extern __shared__ float4 sLi4[];
+  T* sLi = reinterpret_cast<T*>(sLi4);  // Linv_I, NB x NB
   __shared__ double acc[NB];
   __shared__ int I_s, ok_s;
   if (active && !*active) return;
@@ -448,9 +597,9 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
   __syncthreads();
   const int I = I_s;
   {
-    const double2* src = reinterpret_cast<const double2*>(Linv + (size_t)I * NB * NB);
-    double2* dst = reinterpret_cast<double2*>(sLi);
-    for (int i = tid; i < NB * NB / 2; i += SV) dst[i] = src[i];
+    const float4* src = reinterpret_cast<const float4*>(Linv + (size_t)I * NB * NB);
+    float4* dst = sLi4;
+    for (int i = tid; i < (int)(NB * NB * sizeof(T) / 16); i += SV) dst[i] = src[i];
   }
   double part[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   const T* Lrow = L + (size_t)(I * NB + warp * 8) * ld + 4 * lane;
@@ -474,7 +623,7 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
   }
   __syncthreads();
   // y_I = Linv_I acc
-  const double* Li = sLi + (size_t)(warp * 8) * NB + 4 * lane;
+  const T* Li = sLi + (size_t)(warp * 8) * NB + 4 * lane;
   double av[4] = {acc[4 * lane], acc[4 * lane + 1], acc[4 * lane + 2], acc[4 * lane + 3]};
 #pragma unroll
   for (int rr = 0; rr < 8; rr++) {
@@ -490,12 +639,13 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
 
 template <typename T>
 static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict__ L, int ld, int ntiles,
-                                                             const double* __restrict__ Linv,
+                                                             const T* __restrict__ Linv,
                                                              const double* __restrict__ yv, double* __restrict__ x,
                                                              int* __restrict__ ticket, int* __restrict__ flags,
                                                              int epoch, int* __restrict__ status,
                                                              const int* __restrict__ active) {
-  extern __shared__ double sLi[];  // Linv_I, NB x NB
+  extern __shared__ float4 sLi4[];
+  T* sLi = reinterpret_cast<T*>(sLi4);  // Linv_I, NB x NB
   __shared__ double red[SV / 32][NB];
   __shared__ double acc[NB];
   __shared__ int I_s, ok_s;
@@ -505,9 +655,9 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
   __syncthreads();
   const int I = I_s;
   {
-    const double2* src = reinterpret_cast<const double2*>(Linv + (size_t)I * NB * NB);
-    double2* dst = reinterpret_cast<double2*>(sLi);
-    for (int i = tid; i < NB * NB / 2; i += SV) dst[i] = src[i];
+    const float4* src = reinterpret_cast<const float4*>(Linv + (size_t)I * NB * NB);
+    float4* dst = sLi4;
+    for (int i = tid; i < (int)(NB * NB * sizeof(T) / 16); i += SV) dst[i] = src[i];
   }
   double part[4] = {0, 0, 0, 0};
   for (int J = ntiles - 1; J > I; J--) {
@@ -538,7 +688,7 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
   }
   __syncthreads();
   // x_I = Linv_I' acc : x[c] = sum_r Linv[r][c] acc[r]
-  const double* Li = sLi + (size_t)(warp * 8) * NB + 4 * lane;
+  const T* Li = sLi + (size_t)(warp * 8) * NB + 4 * lane;
   double p2[4] = {0, 0, 0, 0};
 #pragma unroll
   for (int rr = 0; rr < 8; rr++) {

@@ -128,7 +128,7 @@ class SchurCoreT final : public SchurCore {
     NL_TRY(r_.alloc(sizeof(double) * (size_t)ld_));
     NL_TRY(dx_.alloc(sizeof(double) * (size_t)ld_));
     NL_TRY(part_.alloc(sizeof(double) * (size_t)std::max(kSymvChunks * ld_, 4 * kRedCTAs)));
-    NL_TRY(Linv_.alloc(sizeof(double) * (size_t)ntiles_ * NB * NB));
+    NL_TRY(Linv_.alloc(sizeof(T) * (size_t)ntiles_ * NB * NB));
     NL_TRY(flags_.alloc(sizeof(int) * (size_t)(ntiles_ + 1)));
     NL_TRY(S_.alloc(sizeof(T) * (size_t)ld_ * ld_));
     need_s0_ = refine_sweeps > 0 || keep_schur;
@@ -186,8 +186,10 @@ class SchurCoreT final : public SchurCore {
     d_.pair_a = pa_.as<int>();
     d_.pair_b = pb_.as<int>();
     NL_CUDA(cudaFuncSetAttribute(trsm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem<T>()));
-    NL_CUDA(cudaFuncSetAttribute(trsv_fwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsvSmem));
-    NL_CUDA(cudaFuncSetAttribute(trsv_bwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsvSmem));
+    NL_CUDA(cudaFuncSetAttribute(trsv_fwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsv_smem<T>()));
+    NL_CUDA(cudaFuncSetAttribute(trsv_bwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsv_smem<T>()));
+    NL_CUDA(cudaFuncSetAttribute(trsm_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmTileSmem));
+    NL_CUDA(cudaFuncSetAttribute(diag_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * (int)kDiagUpdSmem));
     if (!ev_[0]) {
       for (auto& e : ev_) NL_CUDA(cudaEventCreate(&e));
       NL_CUDA(cudaEventCreateWithFlags(&ev_panel_, cudaEventDisableTiming));
@@ -215,10 +217,10 @@ class SchurCoreT final : public SchurCore {
   // ---- solves with the factor: x = S^-1 b (trsv fwd + bwd) ----
   nl_status enqueue_solve(const double* b, double* x, int* status, const int* active) {
     NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
-    trsv_fwd_kernel<T><<<ntiles_, SV, kTrsvSmem, st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<double>(), b, y_.as<double>(),
+    trsv_fwd_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), b, y_.as<double>(),
                                                  flags_.as<int>(), flags_.as<int>() + 1, 1, status, active);
     NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
-    trsv_bwd_kernel<T><<<ntiles_, SV, kTrsvSmem, st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<double>(), y_.as<double>(), x,
+    trsv_bwd_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), y_.as<double>(), x,
                                                  flags_.as<int>(), flags_.as<int>() + 1, 1, status, active);
     launches += 2;
     return NL_OK;
@@ -273,12 +275,12 @@ class SchurCoreT final : public SchurCore {
   }
 
   nl_status factor_panel(int k, int* status, const int* active) {
-    potrf_diag_kernel<T><<<1, PT, kPotrfSmem, st_>>>(S_.as<T>(), ld_, k, Linv_.as<double>(), status, active);
+    potrf_diag_kernel<T><<<1, PT, kPotrfSmem, st_>>>(S_.as<T>(), ld_, k, Linv_.as<T>(), status, active);
     launches++;
     const int below = ld_ - (k + 1) * NB;
     if (below > 0) {
       trsm_kernel<T><<<cdiv(below, TRSM_ROWS), 256, trsm_smem<T>(), st_>>>(S_.as<T>(), ld_, k, (k + 1) * NB, below,
-                                                                            Linv_.as<double>(), nullptr, active);
+                                                                            Linv_.as<T>(), nullptr, active);
       launches++;
       if (sizeof(T) == 4 && use_tc) {
         NL_CUDA(tc_pack_f32(reinterpret_cast<const float*>(S_.p), ld_, k, 0, below, pack_slot(k), active, st_));
@@ -301,6 +303,8 @@ class SchurCoreT final : public SchurCore {
   //         [wait A1r] TRSM + pack of row tile k+2 of panel k+1;
   //         [wait B of the previous pair] A2d  tile (k+2, k+2) with panels
   //         k, k+1 (K = 256); potrf(k+2); [wait A2r] TRSM + pack of row tile k+3
+  //         (A1d / A2d are diag_update_kernel, the row-tile TRSMs
+  //         trsm_tile_kernel: 8 CTAs each, FP32 on CUDA cores)
   //   aux   A1r  block column k+1 below tile k+2 with panel k; TRSM + pack of
   //         the rows below tile k+2 of panel k+1; [wait B] A2r  block columns
   //         k+2 (below its diagonal) and k+3 with panels k, k+1; TRSM + pack of
@@ -312,8 +316,11 @@ class SchurCoreT final : public SchurCore {
   nl_status enqueue_factor_pairs(int* status, const int* active) {
     const bool tm = timing && !active;
     const int nT = ntiles_;
-    if (tm && (int)upd_ev_.size() < 10 * nT + 10) {  // [0, 8 nT): updates, [8 nT, 10 nT): potrf
-      for (size_t i = upd_ev_.size(); i < (size_t)10 * nT + 10; i++) {
+    // timing events: [0, 8 nT) updates, [8 nT, 10 nT) potrf, [10 nT, 14 nT)
+    // per row tile: start (after its waits) and end of the TRSM and of the
+    // diagonal-tile update
+    if (tm && (int)upd_ev_.size() < 14 * nT + 10) {
+      for (size_t i = upd_ev_.size(); i < (size_t)14 * nT + 10; i++) {
         cudaEvent_t e;
         NL_CUDA(cudaEventCreate(&e));
         upd_ev_.push_back(e);
@@ -345,15 +352,30 @@ class SchurCoreT final : public SchurCore {
       if (nrows <= 0) return NL_OK;
       // the TRSM writes the BF16 pack of its rows in its epilogue
       trsm_kernel<T><<<cdiv(nrows, TRSM_ROWS), 256, trsm_smem<T>(), st>>>(S_.as<T>(), ld_, j, r0, nrows,
-                                                                           Linv_.as<double>(), pack_slot(j), active);
+                                                                           Linv_.as<T>(), pack_slot(j), active);
       launches++;
       return NL_OK;
+    };
+    // row tile j+1 of panel j (the critical one) and the diagonal-tile
+    // updates: 8-CTA FP32 kernels on the main stream
+    auto trsm_first = [&](int j) {
+      if (tm) cudaEventRecord(upd_ev_[10 * nT + 4 * j], st_);
+      trsm_tile_kernel<<<kSliceCtas, 256, kTrsmTileSmem, st_>>>(S, ld_, j, reinterpret_cast<const float*>(Linv_.p),
+                                                                pack_slot(j), active);
+      if (tm) cudaEventRecord(upd_ev_[10 * nT + 4 * j + 1], st_);
+      launches++;
+    };
+    auto diag_upd = [&](int t, int p0, int np) {
+      if (tm) cudaEventRecord(upd_ev_[10 * nT + 4 * (t - 1) + 2], st_);
+      diag_update_kernel<<<kSliceCtas, 256, np * kDiagUpdSmem, st_>>>(S, ld_, t, p0, np, active);
+      if (tm) cudaEventRecord(upd_ev_[10 * nT + 4 * (t - 1) + 3], st_);
+      launches++;
     };
     int npev = 0;
     auto potrf = [&](int j) {
       const int e = 8 * nT + 2 * j;  // timing events after the update events
       if (tm) cudaEventRecord(upd_ev_[e], st_);
-      potrf_diag_kernel<T><<<1, PT, kPotrfSmem, st_>>>(S_.as<T>(), ld_, j, Linv_.as<double>(), status, active);
+      potrf_diag_kernel<T><<<1, PT, kPotrfSmem, st_>>>(S_.as<T>(), ld_, j, Linv_.as<T>(), status, active);
       if (tm) cudaEventRecord(upd_ev_[e + 1], st_);
       npev = j + 1;
       launches++;
@@ -367,7 +389,7 @@ class SchurCoreT final : public SchurCore {
     nl_status r;
     // panel 0
     potrf(0);
-    if ((r = trsm_pack(0, NB, std::min(NB, ld_ - NB), st_)) != NL_OK) return r;
+    if (nT > 1) trsm_first(0);
     NL_CUDA(rec(EV_POTRF, st_));
     NL_CUDA(wait(st3_, EV_POTRF));
     if ((r = trsm_pack(0, 2 * NB, ld_ - 2 * NB, st3_)) != NL_OK) return r;
@@ -376,7 +398,7 @@ class SchurCoreT final : public SchurCore {
       // panel k is factored; row tile k+1 of it is packed (main), the rest
       // is being packed on the aux stream
       NL_CUDA(rec(EV_PACKF, st_));
-      if ((r = upd(k, false, k + 1, 1, 1, 0, st_)) != NL_OK) return r;  // A1d
+      diag_upd(k + 1, k, 1);  // A1d
       NL_CUDA(wait(st3_, EV_PACKF));
       if ((r = upd(k, false, k + 1, nT - k - 1, 1, 1, st3_)) != NL_OK) return r;  // A1r
       NL_CUDA(rec(EV_A1R, st3_));
@@ -386,12 +408,12 @@ class SchurCoreT final : public SchurCore {
       if ((r = trsm_pack(k + 1, (k + 3) * NB, ld_ - (k + 3) * NB, st3_)) != NL_OK) return r;
       NL_CUDA(rec(EV_PACKR, st3_));
       NL_CUDA(wait(st_, EV_A1R));
-      if ((r = trsm_pack(k + 1, (k + 2) * NB, std::min(NB, ld_ - (k + 2) * NB), st_)) != NL_OK) return r;
       if (k + 2 >= nT) break;
+      trsm_first(k + 1);
       // pair update: A2d on main, A2r on aux, B on the side stream
       NL_CUDA(rec(EV_PACKF, st_));
       if (pending_b) NL_CUDA(wait(st_, EV_B));
-      if ((r = upd(k, true, k + 2, 1, 1, 0, st_)) != NL_OK) return r;  // A2d
+      diag_upd(k + 2, k, 2);  // A2d
       NL_CUDA(wait(st3_, EV_PACKF));
       if (pending_b) NL_CUDA(wait(st3_, EV_B));
       if ((r = upd(k, true, k + 2, nT - k - 2, 2, 1, st3_)) != NL_OK) return r;  // A2r
@@ -410,7 +432,7 @@ class SchurCoreT final : public SchurCore {
       NL_CUDA(wait(st3_, EV_POTRF));
       if ((r = trsm_pack(k + 2, (k + 4) * NB, ld_ - (k + 4) * NB, st3_)) != NL_OK) return r;
       NL_CUDA(wait(st_, EV_A2R));
-      if ((r = trsm_pack(k + 2, (k + 3) * NB, std::min(NB, ld_ - (k + 3) * NB), st_)) != NL_OK) return r;
+      if (k + 3 < nT) trsm_first(k + 2);
     }
     // join: the solves that follow read every tile and Linv
     NL_CUDA(rec(EV_AUX, st3_));
@@ -436,6 +458,21 @@ class SchurCoreT final : public SchurCore {
       }
       times.panel_ms = pt;
       times.panels = npev;
+      // per row tile j+1: the waits for the other streams (potrf(j) end ->
+      // TRSM start, TRSM end -> update start) and the two 8-CTA kernels
+      float wt = 0, ft = 0;
+      for (int j = 0; j + 1 < npev; j++) {
+        const cudaEvent_t* e = &upd_ev_[10 * nT + 4 * j];
+        float a = 0, b = 0, c = 0, d = 0;
+        cudaEventElapsedTime(&a, upd_ev_[8 * nT + 2 * j + 1], e[0]);
+        cudaEventElapsedTime(&b, e[0], e[1]);
+        cudaEventElapsedTime(&c, e[1], e[2]);
+        cudaEventElapsedTime(&d, e[2], e[3]);
+        wt += a + c;
+        ft += b + d;
+      }
+      times.wait_ms = wt;
+      times.first_ms = ft;
     }
     return NL_OK;
   }

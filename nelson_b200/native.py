@@ -66,7 +66,7 @@ class PhaseTimes(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("vinv_ms", "wvinv_bs_ms", "schur_ms", "factor_ms", "solve_ms",
                                           "backsub_ms", "total_ms", "eval_ms", "update_ms")] + \
         [("update_launches", C.c_int), ("update_flop", C.c_double), ("update_bytes", C.c_double),
-         ("panel_ms", C.c_float), ("panels", C.c_int)]
+         ("panel_ms", C.c_float), ("panels", C.c_int), ("wait_ms", C.c_float), ("first_ms", C.c_float)]
 
 
 class AdjointReport(C.Structure):

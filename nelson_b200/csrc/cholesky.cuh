@@ -23,57 +23,151 @@ constexpr int NB = 128;
 constexpr long long kSpinLimit = 1LL << 24;  // bounded waits (~1 s worst case)
 
 // ---------------------------------------------------------------------------
-// One CTA (544 threads): factor the NB x NB diagonal tile of panel k in the
-// storage precision T (FP64 for the FP64 path; FP32 for the mixed path, whose
+// One CTA: factor the NB x NB diagonal tile of panel k in the storage
+// precision T (FP64 for the FP64 path; FP32 for the mixed path, whose
 // trailing updates and off-diagonal solves are FP32-accurate as well and whose
 // factor only preconditions the FP64 refinement) and build its inverse, in
-// registers.
-// Thread t owns 4x4 block (R, C), C <= R, of the lower triangle (528 blocks)
-// and one register block `t` for it: A until block column C is factored
-// (then L_R,C is written to S), afterwards B -> X = inv(L) (right-looking
-// forward substitution of L X = I).  For each block column jb (32 super-steps,
-// two barriers each):
-//   (1) the owner of (jb, jb) factors its 4x4 block and inverts it (Di);
-//   (2) owners of block column jb form L_R,jb = A_R,jb Di' and publish it;
-//       owners of block row jb finish X_jb,C = Di B_jb,C and publish it;
-//   (3) every block with jb < R applies one rank-4 update
-//       t -= L_R,jb Q_jb,C  with Q = L_C,jb' while jb < C (A part) and
-//       Q = X_jb,C once jb >= C (X part): the same instructions for both, so
-//       a warp never splits between the two.
-// L_kk is written to S and inv(L_kk) (zeros above the diagonal) to Linv.
-constexpr int PT = 544;
+// registers, as 32 super-steps of 4 columns.
+//
+// Owner threads (528): thread t owns 4x4 block (R, C), C <= R, of the lower
+// triangle and one register block for it: A until block column C is factored,
+// afterwards B -> X = inv(L) (right-looking forward substitution of L X = I).
+// Pivot warp (warp 14): does all per-super-step work that is not a bulk update,
+// so that no owner warp runs it for one or two active lanes.  Super-step jb:
+//   (2) pivot warp, lane l < 31: for the row-jb block (jb, C = l) if l < jb,
+//       else for the column-jb block (R = l + 1, jb): out = M Di' with M the
+//       staged B' (row block: X_jb,C = out') or A (column block: L_R,jb =
+//       out); publishes L / X in shared memory and writes them to S / Linv.
+//   (3) owners with jb < R (except the next diagonal block) apply one rank-4
+//       update  t -= L_R,jb Q_jb,C  with Q = L_C,jb' while jb < C (A part) and
+//       Q = X_jb,C once jb >= C (X part) -- the same instructions for both --
+//       then stage their block in shared memory if it just became final:
+//       column-(jb+1) blocks (A), row-(jb+1) blocks (B'), diagonal block jb+2.
+//       Concurrently the pivot warp's lane jb, which holds L_jb+1,jb, factors
+//       the next diagonal block A_jb+1,jb+1 - L_jb+1,jb L_jb+1,jb' and inverts
+//       it (Di of super-step jb+1): the serial 4x4 factor overlaps the updates.
+// Warps are spread over the SM's four schedulers by index mod 4; the pivot
+// warp's scheduler carries three owner warps, the others four or five.
+// Shared 4x4 blocks are 20-word rows (16 used): lanes reading or writing
+// consecutive blocks with 16-byte vectors stay within the minimum wavefronts.
+// Two barriers per super-step.  L_kk is written to S and the blocks of
+// inv(L_kk) on and below the diagonal to Linv (its strictly upper blocks are
+// never written: the caller keeps them zero).
+constexpr int kPivotWarp = 14;
+constexpr int PT = 32 * 18;  // 17 owner warps (528 owners) + the pivot warp
+constexpr int kTiles4 = (NB / 4) * (NB / 4 + 1) / 2;  // 528
+constexpr int kBlk = 20;     // words per shared 4x4 block
+constexpr size_t kPotrfSmem = 0;
+
+// four consecutive elements (16-byte aligned for float, 32 for double; any
+// address space)
+__device__ inline void store_row4(float* p, float a, float b, float c, float d) {
+  *reinterpret_cast<float4*>(p) = make_float4(a, b, c, d);
+}
+__device__ inline void store_row4(double* p, double a, double b, double c, double d) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(a, b);
+  reinterpret_cast<double2*>(p)[1] = make_double2(c, d);
+}
+__device__ inline void load_row4(const float* p, float v[4]) {
+  const float4 x = *reinterpret_cast<const float4*>(p);
+  v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+}
+__device__ inline void load_row4(const double* p, double v[4]) {
+  const double2 x = reinterpret_cast<const double2*>(p)[0], y = reinterpret_cast<const double2*>(p)[1];
+  v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
+}
 
 // 1 / sqrt of a pivot, clamped away from zero (a non-positive pivot is
 // flagged separately)
 __device__ inline float pivot_rsqrt(float d) { return rsqrtf(fmaxf(d, 1e-30f)); }
 __device__ inline double pivot_rsqrt(double d) { return rsqrt(fmax(d, 1e-300)); }
-constexpr int kTiles4 = (NB / 4) * (NB / 4 + 1) / 2;  // 528
-constexpr size_t kPotrfSmem = 0;
+
+// Factor the 4x4 SPD block a (lower part used) of diagonal block jb and invert
+// the factor: L to S (zeros above its diagonal), Di = inv(L) to the shared Di
+// (row-major 4x4) and X block (row i, column c at i * 4 + c) and to Linv.
+// Returns false on a non-positive pivot.
+template <typename T>
+__device__ inline bool factor_pivot_block(T a[4][4], int jb, T* __restrict__ S, size_t base, int ld,
+                                          T* __restrict__ Lout, T* Di, T* Xblk) {
+  bool fail = false;
+  T rs[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    T d = a[j][j];
+#pragma unroll
+    for (int l = 0; l < j; l++) d -= a[j][l] * a[j][l];
+    fail |= !(d > (T)0) || !isfinite(d);
+    rs[j] = pivot_rsqrt(d);
+    a[j][j] = d * rs[j];
+#pragma unroll
+    for (int i = j + 1; i < 4; i++) {
+      T v = a[i][j];
+#pragma unroll
+      for (int l = 0; l < j; l++) v -= a[i][l] * a[j][l];
+      a[i][j] = v * rs[j];
+    }
+  }
+  const int r0 = 4 * jb;
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+    store_row4(S + base + (size_t)(r0 + i) * ld + r0, a[i][0], i >= 1 ? a[i][1] : (T)0, i >= 2 ? a[i][2] : (T)0,
+               i >= 3 ? a[i][3] : (T)0);
+  // inv(L) one column at a time: multiplications only (the rsqrt is 1 / L_ii)
+  T di[4][4];
+#pragma unroll
+  for (int c = 0; c < 4; c++)
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      if (i < c) {
+        di[i][c] = (T)0;
+      } else if (i == c) {
+        di[i][c] = rs[i];
+      } else {
+        T v = (T)0;
+#pragma unroll
+        for (int l = c; l < i; l++) v -= a[i][l] * di[l][c];
+        di[i][c] = v * rs[i];
+      }
+    }
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    store_row4(Di + 4 * i, di[i][0], di[i][1], di[i][2], di[i][3]);
+    store_row4(Xblk + 4 * i, di[i][0], di[i][1], di[i][2], di[i][3]);
+    store_row4(Lout + (size_t)(r0 + i) * NB + r0, di[i][0], di[i][1], di[i][2], di[i][3]);
+  }
+  return !fail;
+}
 
 template <typename T>
-static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int ld, int k,
-                                                                T* __restrict__ Linv, int* __restrict__ status,
-                                                                const int* __restrict__ active) {
-  // L of block column jb (row 4 b + u, column w at Lc[.][w][u][b]) and X of
-  // block row jb (row w, column 4 b + u at Xr[.][w][u][b]), double-buffered.
-  // Block index innermost: a warp's owners read consecutive block indices, so
-  // the loads of the rank-4 update are free of bank conflicts.
-  __shared__ T Lc[2][4][4][NB / 4];
-  __shared__ T Xr[2][4][4][NB / 4];
-  __shared__ T Di[2][4][4];  // inv(L_jb,jb)
+static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S, int ld, int k,
+                                                               T* __restrict__ Linv, int* __restrict__ status,
+                                                               const int* __restrict__ active) {
+  // Published blocks of super-step jb (double-buffered): L_R,jb at Lc[.][R]
+  // (row u, column w at w * 4 + u) and X_jb,C at Xr[.][C] (row w, column v at
+  // w * 4 + v), so that rank-4 step w reads 4 consecutive words of each.
+  // Staged blocks M at Mst[slot] (row u, column w at u * 4 + w; row block C:
+  // slot C, holding B'; column block R: slot R - 1, holding A); staged
+  // diagonal blocks by parity.
+  __shared__ __align__(16) T Lc[2][NB / 4][kBlk];
+  __shared__ __align__(16) T Xr[2][NB / 4][kBlk];
+  __shared__ __align__(16) T Mst[NB / 4][kBlk];
+  __shared__ __align__(16) T Di[2][16];  // inv(L_jb,jb), row-major
+  __shared__ T Dst[2][4][4];
   __shared__ int bad;
   if (active && !*active) return;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, wi = tid >> 5;
+  const bool pivot = wi == kPivotWarp;
+  const int oid = wi < kPivotWarp ? tid : tid - 32;  // owner index
   const size_t base = (size_t)k * NB * ld + (size_t)k * NB;
   T* Lout = Linv + (size_t)k * NB * NB;
   if (tid == 0) bad = 0;
   int R = 0, C = 0;
-  const bool own = tid < kTiles4;
+  const bool own = !pivot && oid < kTiles4;
   if (own) {
-    R = (int)((sqrtf(8.0f * tid + 1.0f) - 1.0f) * 0.5f);
-    while ((R + 1) * (R + 2) / 2 <= tid) R++;
-    while (R * (R + 1) / 2 > tid) R--;
-    C = tid - R * (R + 1) / 2;
+    R = (int)((sqrtf(8.0f * oid + 1.0f) - 1.0f) * 0.5f);
+    while ((R + 1) * (R + 2) / 2 <= oid) R++;
+    while (R * (R + 1) / 2 > oid) R--;
+    C = oid - R * (R + 1) / 2;
   }
   const int r0 = 4 * R, c0 = 4 * C;
   T t[4][4];
@@ -82,135 +176,117 @@ static __global__ void __maxnreg__(72) potrf_diag_kernel(T* __restrict__ S, int 
 #pragma unroll
     for (int v = 0; v < 4; v++)
       t[u][v] = (own && c0 + v <= r0 + u) ? S[base + (size_t)(r0 + u) * ld + c0 + v] : (T)0;
-  // zero the strictly upper blocks of Linv (never written below)
-  for (int i = tid; i < NB * NB; i += PT) {
-    const int r = i / NB, c = i - r * NB;
-    if ((c >> 2) > (r >> 2)) Lout[i] = (T)0;
+  // stage column 0 and the first two diagonal blocks
+  if (own && C == 0 && R > 0) {
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      store_row4(&Mst[R - 1][4 * u], t[u][0], t[u][1], t[u][2], t[u][3]);
+#pragma unroll
+      for (int w = 0; w < 4; w++) t[u][w] = (T)0;
+    }
+  } else if (own && R == C && R <= 1) {
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int v = 0; v < 4; v++) Dst[R][u][v] = t[u][v];
   }
   __syncthreads();
+  if (pivot && lane == 0) {
+    T a[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int v = 0; v < 4; v++) a[u][v] = Dst[0][u][v];
+    if (!factor_pivot_block(a, 0, S, base, ld, Lout, Di[0], Xr[0][0])) bad = 1;
+  }
+  __syncthreads();
+  T out[4][4];  // pivot warp: this super-step's L (or X') block
   for (int jb = 0; jb < NB / 4; jb++) {
     const int buf = jb & 1;
-    // (1) factor + invert the diagonal 4x4 block (one rsqrt per column,
-    //     multiplications only: Di[i][i] = 1 / L_ii is that rsqrt)
-    if (own && R == jb && C == jb) {
-      bool fail = false;
-      T rs[4];
+    // (2) the row-jb and column-jb blocks, one per pivot-warp lane
+    if (pivot && lane < NB / 4 - 1) {
+      T m[4][4], d[4][4];
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        T d = t[j][j];
-#pragma unroll
-        for (int l = 0; l < j; l++) d -= t[j][l] * t[j][l];
-        fail |= !(d > (T)0) || !isfinite(d);
-        rs[j] = pivot_rsqrt(d);
-        t[j][j] = d * rs[j];
-#pragma unroll
-        for (int i = j + 1; i < 4; i++) {
-          T v = t[i][j];
-#pragma unroll
-          for (int l = 0; l < j; l++) v -= t[i][l] * t[j][l];
-          t[i][j] = v * rs[j];
-        }
-      }
-      if (fail) bad = 1;
-      // L_jb,jb to S and the shared column
-#pragma unroll
-      for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-          const T l = c <= i ? t[i][c] : (T)0;
-          Lc[buf][c][i][jb] = l;
-          if (c <= i) S[base + (size_t)(r0 + i) * ld + c0 + c] = l;
-        }
-      // Di = inv(L_jb,jb) one column at a time; X_jb,jb = Di to Linv and the shared row
-#pragma unroll
-      for (int c = 0; c < 4; c++) {
-        T dc[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-          if (i < c) {
-            dc[i] = (T)0;
-          } else if (i == c) {
-            dc[i] = rs[i];
-          } else {
-            T v = (T)0;
-#pragma unroll
-            for (int l = c; l < i; l++) v -= t[i][l] * dc[l];
-            dc[i] = v * rs[i];
-          }
-        }
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-          Di[buf][i][c] = dc[i];
-          Xr[buf][i][c][jb] = dc[i];
-          Lout[(size_t)(r0 + i) * NB + c0 + c] = dc[i];
-        }
+      for (int u = 0; u < 4; u++) {
+        load_row4(&Mst[lane][4 * u], m[u]);
+        load_row4(&Di[buf][4 * u], d[u]);
       }
 #pragma unroll
       for (int u = 0; u < 4; u++)
 #pragma unroll
-        for (int v = 0; v < 4; v++) t[u][v] = 0.0;  // finished
-    }
-    __syncthreads();
-    // (2) block column jb of L (A part ends), block row jb of X (X part ends)
-    if (own && C == jb && R > jb) {
-      // one row of L_R,jb = A_R,jb Di' at a time
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        T l[4];
-#pragma unroll
         for (int v = 0; v < 4; v++) {
           T s = (T)0;
 #pragma unroll
-          for (int w = 0; w <= v; w++) s += t[u][w] * Di[buf][v][w];
-          l[v] = s;
+          for (int w = 0; w <= v; w++) s += m[u][w] * d[v][w];
+          out[u][v] = s;
         }
+      const bool rowb = lane < jb;
+      const int idx = rowb ? lane : lane + 1;  // C of a row block, R of a column block
+      // L_R,jb[u][v] at v * 4 + u; X_jb,C[v][u] = out[u][v] at v * 4 + u
+      T* pub = rowb ? Xr[buf][idx] : Lc[buf][idx];
 #pragma unroll
-        for (int v = 0; v < 4; v++) {
-          Lc[buf][v][u][R] = l[v];
-          S[base + (size_t)(r0 + u) * ld + c0 + v] = l[v];
-          t[u][v] = 0.0;  // the X block starts from zero below the diagonal
-        }
-      }
-    } else if (own && R == jb && C < jb) {
-      // one column of X_jb,C = Di B_jb,C at a time
+      for (int v = 0; v < 4; v++) store_row4(pub + 4 * v, out[0][v], out[1][v], out[2][v], out[3][v]);
+      if (rowb) {
+        // X_jb,C = out': row v of X is column v of out
 #pragma unroll
-      for (int v = 0; v < 4; v++) {
-        T xx[4];
+        for (int v = 0; v < 4; v++)
+          store_row4(Lout + (size_t)(4 * jb + v) * NB + 4 * idx, out[0][v], out[1][v], out[2][v], out[3][v]);
+      } else {
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-          T s = (T)0;
-#pragma unroll
-          for (int w = 0; w <= u; w++) s += Di[buf][u][w] * t[w][v];
-          xx[u] = s;
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          Xr[buf][u][v][C] = xx[u];
-          Lout[(size_t)(r0 + u) * NB + c0 + v] = xx[u];
-        }
+        for (int u = 0; u < 4; u++)
+          store_row4(S + base + (size_t)(4 * idx + u) * ld + 4 * jb, out[u][0], out[u][1], out[u][2], out[u][3]);
       }
     }
     __syncthreads();
-    // (3) one rank-4 update per block below row jb; the next step writes the
-    //     other buffers, so no barrier here
-    if (own && jb < R) {
-      const T* q = (jb < C) ? &Lc[buf][0][0][0] : &Xr[buf][0][0][0];  // [w][v][b] either way
+    // (3) one rank-4 update per block below row jb, then staging; the next
+    //     step writes the other buffers, so no barrier here
+    if (own && jb < R && !(R == C && R == jb + 1)) {
+      const T* q = (jb < C) ? Lc[buf][C] : Xr[buf][C];  // Q_jb,C row w at 4 w either way
 #pragma unroll
       for (int w = 0; w < 4; w++) {
         T pr[4], qc[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          pr[u] = Lc[buf][w][u][R];
-          qc[u] = q[(w * 4 + u) * (NB / 4) + C];
-        }
+        load_row4(&Lc[buf][R][4 * w], pr);
+        load_row4(q + 4 * w, qc);
 #pragma unroll
         for (int u = 0; u < 4; u++)
 #pragma unroll
           for (int v = 0; v < 4; v++) t[u][v] -= pr[u] * qc[v];
       }
+      if (C == jb + 1 && R > jb + 1) {  // A_R,jb+1 is final
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          store_row4(&Mst[R - 1][4 * u], t[u][0], t[u][1], t[u][2], t[u][3]);
+#pragma unroll
+          for (int w = 0; w < 4; w++) t[u][w] = (T)0;  // the X block starts from zero below the diagonal
+        }
+      } else if (R == jb + 1) {  // B_jb+1,C is final (C <= jb): stage B'
+#pragma unroll
+        for (int u = 0; u < 4; u++) store_row4(&Mst[C][4 * u], t[0][u], t[1][u], t[2][u], t[3][u]);
+      } else if (R == C && R == jb + 2) {  // all but the last update of A_jb+2,jb+2
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+          for (int v = 0; v < 4; v++) Dst[R & 1][u][v] = t[u][v];
+      }
     }
+    // look-ahead: the next diagonal block, from its staged value and the
+    // L_jb+1,jb held by lane jb
+    if (pivot && lane == jb && jb + 1 < NB / 4) {
+      const int nb = jb + 1;
+      T a[4][4];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int c = 0; c <= i; c++) {
+          T v = Dst[nb & 1][i][c];
+#pragma unroll
+          for (int w = 0; w < 4; w++) v -= out[i][w] * out[c][w];
+          a[i][c] = v;
+        }
+      if (!factor_pivot_block(a, nb, S, base, ld, Lout, Di[nb & 1], Xr[nb & 1][nb])) bad = 1;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   if (tid == 0 && bad) atomicOr(status, ST_CHOL_FAIL);
 }
 

@@ -129,6 +129,9 @@ class SchurCoreT final : public SchurCore {
     NL_TRY(dx_.alloc(sizeof(double) * (size_t)ld_));
     NL_TRY(part_.alloc(sizeof(double) * (size_t)std::max(kSymvChunks * ld_, 4 * kRedCTAs)));
     NL_TRY(Linv_.alloc(sizeof(T) * (size_t)ntiles_ * NB * NB));
+    // the diagonal-tile factor writes only the blocks on and below the
+    // diagonal: the strictly upper blocks of every inverse stay zero
+    NL_CUDA(cudaMemsetAsync(Linv_.p, 0, Linv_.bytes, st_));
     NL_TRY(flags_.alloc(sizeof(int) * (size_t)(ntiles_ + 1)));
     NL_TRY(S_.alloc(sizeof(T) * (size_t)ld_ * ld_));
     need_s0_ = refine_sweeps > 0 || keep_schur;

@@ -22,6 +22,14 @@ namespace nl {
 constexpr int NB = 128;
 constexpr long long kSpinLimit = 1LL << 24;  // bounded waits (~1 s worst case)
 
+// Programmatic dependent launch of the critical-path chain (potrf -> row-tile
+// TRSM -> diagonal-tile update -> potrf ...): each kernel lets the next one in
+// its stream launch at its start, and waits for its predecessor's completion
+// (and memory flush) before touching what that predecessor wrote.  Both are
+// no-ops for a kernel launched without the attribute.
+__device__ inline void chain_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ inline void chain_release() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
 // ---------------------------------------------------------------------------
 // One CTA: factor the NB x NB diagonal tile of panel k in the storage
 // precision T (FP64 for the FP64 path; FP32 for the mixed path, whose
@@ -154,6 +162,8 @@ static __global__ void __launch_bounds__(PT) potrf_diag_kernel(T* __restrict__ S
   __shared__ __align__(16) T Di[2][16];  // inv(L_jb,jb), row-major
   __shared__ T Dst[2][4][4];
   __shared__ int bad;
+  chain_release();
+  chain_wait();
   if (active && !*active) return;
   const int tid = threadIdx.x, lane = tid & 31, wi = tid >> 5;
   const bool pivot = wi == kPivotWarp;
@@ -466,6 +476,8 @@ static __global__ void __launch_bounds__(256) trsm_tile_kernel(float* __restrict
   extern __shared__ float4 smf4[];
   float* sb = reinterpret_cast<float*>(smf4);  // inv(L_jj), row i = output column i
   float* sa = sb + NB * kSlLd;                 // the slice's 16 rows of A_(j+1),j
+  chain_release();
+  chain_wait();
   if (active && !*active) return;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int rel0 = blockIdx.x * kSliceRows;  // first slice row within the tile
@@ -510,16 +522,27 @@ static __global__ void __launch_bounds__(256) diag_update_kernel(float* __restri
                                                                  const int* __restrict__ active) {
   extern __shared__ float4 smf4[];
   float* sm = reinterpret_cast<float*>(smf4);  // L_t,p (all 128 rows) per panel
-  if (active && !*active) return;
+  chain_release();
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, c = blockIdx.x;
   const int ra = diag_slice_row(c, lane >> 2), rb = diag_slice_row(c, 8 + (lane >> 2));
   const float* T0 = S + (size_t)t * NB * ld + (size_t)p0 * NB;
-  stage_rows_f32(T0, ld, NB, sm, tid);
+  // with two panels the first was finished before the stream's preceding
+  // kernel (the row-tile TRSM of the second) started: fetch it while that
+  // kernel runs
+  if (np > 1) stage_rows_f32(T0, ld, NB, sm, tid);
   cp_async_commit();
-  if (np > 1) stage_rows_f32(T0 + NB, ld, NB, sm + NB * kSlLd, tid);
+  chain_wait();
+  if (active && !*active) {
+    cp_async_wait<0>();
+    return;
+  }
+  stage_rows_f32(T0 + (np > 1 ? NB : 0), ld, NB, sm + (np > 1 ? NB * kSlLd : 0), tid);
   cp_async_commit();
   float acc[2][4] = {};
-  cp_async_wait<1>();
+  if (np > 1)
+    cp_async_wait<1>();
+  else
+    cp_async_wait<0>();
   __syncthreads();
   slice_mma(sm + ra * kSlLd, sm + rb * kSlLd, sm, lane, w, acc);
   if (np > 1) {

@@ -293,6 +293,24 @@ class SchurCoreT final : public SchurCore {
     return NL_OK;
   }
 
+  // A kernel on the main stream; with pdl, as a programmatic dependent of the
+  // stream's preceding kernel (it may start before that one ends and waits
+  // for it with griddepcontrol.wait).
+  template <typename... KArgs, typename... Args>
+  cudaError_t launch_chain(void (*kern)(KArgs...), int grid, int block, size_t smem, bool pdl, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st_;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+  }
+
   uint8_t* pack_slot(int k) const { return static_cast<uint8_t*>(tcs_.p) + (size_t)(k % kPackSlots) * tcs_half_; }
 
   // Tensor-core schedule: panels in pairs, so the bulk of the trailing update
@@ -368,20 +386,27 @@ class SchurCoreT final : public SchurCore {
       if (tm) cudaEventRecord(upd_ev_[10 * nT + 4 * j + 1], st_);
       launches++;
     };
-    auto diag_upd = [&](int t, int p0, int np) {
+    // pdl: launched early against the preceding kernel of the main stream
+    // (only where no event wait sits between the two)
+    auto diag_upd = [&](int t, int p0, int np, bool pdl) -> nl_status {
       if (tm) cudaEventRecord(upd_ev_[10 * nT + 4 * (t - 1) + 2], st_);
-      diag_update_kernel<<<kSliceCtas, 256, np * kDiagUpdSmem, st_>>>(S, ld_, t, p0, np, active);
+      NL_CUDA(launch_chain(diag_update_kernel, kSliceCtas, 256, np * kDiagUpdSmem, pdl && !tm, S, ld_, t, p0, np,
+                           active));
       if (tm) cudaEventRecord(upd_ev_[10 * nT + 4 * (t - 1) + 3], st_);
       launches++;
+      return NL_OK;
     };
     int npev = 0;
-    auto potrf = [&](int j) {
+    auto potrf = [&](int j) -> nl_status {
       const int e = 8 * nT + 2 * j;  // timing events after the update events
       if (tm) cudaEventRecord(upd_ev_[e], st_);
-      potrf_diag_kernel<T><<<1, PT, kPotrfSmem, st_>>>(S_.as<T>(), ld_, j, Linv_.as<T>(), status, active);
+      // a programmatic dependent of the diagonal update before it
+      NL_CUDA(launch_chain(potrf_diag_kernel<T>, 1, PT, kPotrfSmem, j > 0 && !tm, S_.as<T>(), ld_, j, Linv_.as<T>(),
+                           status, active));
       if (tm) cudaEventRecord(upd_ev_[e + 1], st_);
       npev = j + 1;
       launches++;
+      return NL_OK;
     };
     auto rec = [&](int e, cudaStream_t st) { return cudaEventRecord(dev_[e], st); };
     auto wait = [&](cudaStream_t st, int e) { return cudaStreamWaitEvent(st, dev_[e], 0); };
@@ -391,7 +416,7 @@ class SchurCoreT final : public SchurCore {
     }
     nl_status r;
     // panel 0
-    potrf(0);
+    if ((r = potrf(0)) != NL_OK) return r;
     if (nT > 1) trsm_first(0);
     NL_CUDA(rec(EV_POTRF, st_));
     NL_CUDA(wait(st3_, EV_POTRF));
@@ -401,11 +426,11 @@ class SchurCoreT final : public SchurCore {
       // panel k is factored; row tile k+1 of it is packed (main), the rest
       // is being packed on the aux stream
       NL_CUDA(rec(EV_PACKF, st_));
-      diag_upd(k + 1, k, 1);  // A1d
+      if ((r = diag_upd(k + 1, k, 1, true)) != NL_OK) return r;  // A1d
       NL_CUDA(wait(st3_, EV_PACKF));
       if ((r = upd(k, false, k + 1, nT - k - 1, 1, 1, st3_)) != NL_OK) return r;  // A1r
       NL_CUDA(rec(EV_A1R, st3_));
-      potrf(k + 1);
+      if ((r = potrf(k + 1)) != NL_OK) return r;
       NL_CUDA(rec(EV_POTRF, st_));
       NL_CUDA(wait(st3_, EV_POTRF));
       if ((r = trsm_pack(k + 1, (k + 3) * NB, ld_ - (k + 3) * NB, st3_)) != NL_OK) return r;
@@ -416,7 +441,7 @@ class SchurCoreT final : public SchurCore {
       // pair update: A2d on main, A2r on aux, B on the side stream
       NL_CUDA(rec(EV_PACKF, st_));
       if (pending_b) NL_CUDA(wait(st_, EV_B));
-      diag_upd(k + 2, k, 2);  // A2d
+      if ((r = diag_upd(k + 2, k, 2, !pending_b)) != NL_OK) return r;  // A2d
       NL_CUDA(wait(st3_, EV_PACKF));
       if (pending_b) NL_CUDA(wait(st3_, EV_B));
       if ((r = upd(k, true, k + 2, nT - k - 2, 2, 1, st3_)) != NL_OK) return r;  // A2r
@@ -430,7 +455,7 @@ class SchurCoreT final : public SchurCore {
       } else {
         pending_b = false;
       }
-      potrf(k + 2);
+      if ((r = potrf(k + 2)) != NL_OK) return r;
       NL_CUDA(rec(EV_POTRF, st_));
       NL_CUDA(wait(st3_, EV_POTRF));
       if ((r = trsm_pack(k + 2, (k + 4) * NB, ld_ - (k + 4) * NB, st3_)) != NL_OK) return r;

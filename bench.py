@@ -340,6 +340,15 @@ def main():
     mu = 1e-3 * gm.max_abs_hdiag()
     gm.compute_increment(0.0, mu)
     pt = gm.phase_times()
+    # the factorisation's critical path, step by step (a separate call: timing
+    # every step slows the factorisation itself)
+    gm.set_timing_detail(True)
+    gm.compute_increment(0.0, mu)
+    ptd = gm.phase_times()
+    gm.set_timing_detail(False)
+    chain = {"factor_ms_timed_per_step": round(ptd["factor_ms"], 4), "panels": ptd["panels"],
+             "diag_factor_ms": round(ptd["panel_ms"], 4), "row_tile_trsm_and_diag_update_ms": round(ptd["first_ms"], 4),
+             "waits_ms": round(ptd["wait_ms"], 4)}
     # The trailing update is a rank-K update (K = 256 for the paired panels of
     # the tensor-core schedule, 128 for the look-ahead column): every updated
     # 128x128 FP32 tile is read and written once per launch (128 KB) while the
@@ -363,7 +372,9 @@ def main():
                 "tensor": {"achieved_tflops": tfl, "peak_tflops": bf16,
                            "frac": (tfl / bf16) if tfl else None,
                            "note": "algorithmic FP32 flops; split-BF16x3 issues 3x as many MMA flops"},
-                "phases_ms": {k: round(v, 4) for k, v in pt.items() if k.endswith("_ms")}}
+                "phases_ms": {k: round(v, 4) for k, v in pt.items()
+                              if k.endswith("_ms") and k not in ("panel_ms", "wait_ms", "first_ms")},
+                "critical_path": chain}
 
     # ---- CPU baseline: the FP64 oracle on a bounded sample ----
     cpu = None

@@ -95,6 +95,8 @@ typedef struct {
   double update_flop;  /* algorithmic flops of those updates (2 * multiply-adds) */
   double update_bytes; /* algorithmic bytes of those updates: each updated
                           128 x 128 tile read and written once per launch */
+  /* The three critical-path fields below are filled only after
+   * nl_set_timing_detail(h, 1) (mixed precision); otherwise they are 0. */
   float panel_ms;      /* summed device time of the diagonal-tile factorisations
                           on the critical path (from their enqueue on the main
                           stream, so including any wait for an SM) */
@@ -224,6 +226,12 @@ nl_status nl_adjoint(nl_problem* h, const double* dL_dcams, const double* dL_dpt
                      double* g_weight, double* mu_cams, double* mu_pts, nl_adjoint_report* rep);
 
 nl_status nl_phase_timings(nl_problem* h, nl_phase_times* out);
+/* detail = 1: nl_compute_increment also times every step of the
+ * factorisation's critical path (panel_ms, wait_ms, first_ms).  That costs one
+ * event record per kernel boundary on the host and disables the early launch
+ * of the chain's kernels, so the factorisation itself runs slower; 0 (the
+ * default) times the phases and the trailing updates only. */
+nl_status nl_set_timing_detail(nl_problem* h, int detail);
 /* Number of kernels of this library launched on the handle since creation. */
 nl_status nl_kernel_launches(nl_problem* h, long long* out);
 

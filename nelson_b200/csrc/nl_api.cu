@@ -31,6 +31,7 @@ inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 struct nl_problem {
   nl_problem_desc desc{};
   int device = 0;
+  int timing_detail = 0;
   cudaStream_t st = nullptr;
   cublasHandle_t cublas = nullptr;
   DevBuf cublas_ws;
@@ -766,6 +767,7 @@ nl_status nl_compute_increment(nl_problem* h, double rel, double abs_, int* ok) 
   NL_CUDA(cudaMemcpyAsync(h->d_lam.p, h->host_pin + 16, sizeof(lam), cudaMemcpyHostToDevice, h->st));
   NL_CUDA(cudaMemsetAsync(h->status, 0, sizeof(int), h->st));
   h->core->timing = 1;
+  h->core->timing_detail = h->timing_detail;
   nl_status s = h->core->enqueue_increment(h->d_lam.as<double>(), h->status, nullptr);
   h->core->timing = 0;
   if (s != NL_OK) return s;
@@ -1180,6 +1182,12 @@ nl_status nl_phase_timings(nl_problem* h, nl_phase_times* out) {
   NL_CHECK_READY(h);
   *out = h->core->times;
   out->eval_ms = h->eval_ms;
+  return NL_OK;
+}
+
+nl_status nl_set_timing_detail(nl_problem* h, int detail) {
+  NL_CHECK_H(h);
+  h->timing_detail = detail ? 1 : 0;
   return NL_OK;
 }
 

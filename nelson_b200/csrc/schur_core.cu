@@ -336,6 +336,7 @@ class SchurCoreT final : public SchurCore {
   enum { EV_PACKF = 0, EV_POTRF, EV_A1R, EV_PACKR, EV_A2R, EV_B, EV_AUX };
   nl_status enqueue_factor_pairs(int* status, const int* active) {
     const bool tm = timing && !active;
+    const bool tmc = tm && timing_detail;  // per-panel chain events
     const int nT = ntiles_;
     // timing events: [0, 8 nT) updates, [8 nT, 10 nT) potrf, [10 nT, 14 nT)
     // per row tile: start (after its waits) and end of the TRSM and of the
@@ -380,30 +381,30 @@ class SchurCoreT final : public SchurCore {
     // row tile j+1 of panel j (the critical one) and the diagonal-tile
     // updates: 8-CTA FP32 kernels on the main stream
     auto trsm_first = [&](int j) {
-      if (tm) cudaEventRecord(upd_ev_[10 * nT + 4 * j], st_);
+      if (tmc) cudaEventRecord(upd_ev_[10 * nT + 4 * j], st_);
       trsm_tile_kernel<<<kSliceCtas, 256, kTrsmTileSmem, st_>>>(S, ld_, j, reinterpret_cast<const float*>(Linv_.p),
                                                                 pack_slot(j), active);
-      if (tm) cudaEventRecord(upd_ev_[10 * nT + 4 * j + 1], st_);
+      if (tmc) cudaEventRecord(upd_ev_[10 * nT + 4 * j + 1], st_);
       launches++;
     };
     // pdl: launched early against the preceding kernel of the main stream
     // (only where no event wait sits between the two)
     auto diag_upd = [&](int t, int p0, int np, bool pdl) -> nl_status {
-      if (tm) cudaEventRecord(upd_ev_[10 * nT + 4 * (t - 1) + 2], st_);
-      NL_CUDA(launch_chain(diag_update_kernel, kSliceCtas, 256, np * kDiagUpdSmem, pdl && !tm, S, ld_, t, p0, np,
+      if (tmc) cudaEventRecord(upd_ev_[10 * nT + 4 * (t - 1) + 2], st_);
+      NL_CUDA(launch_chain(diag_update_kernel, kSliceCtas, 256, np * kDiagUpdSmem, pdl && !tmc, S, ld_, t, p0, np,
                            active));
-      if (tm) cudaEventRecord(upd_ev_[10 * nT + 4 * (t - 1) + 3], st_);
+      if (tmc) cudaEventRecord(upd_ev_[10 * nT + 4 * (t - 1) + 3], st_);
       launches++;
       return NL_OK;
     };
     int npev = 0;
     auto potrf = [&](int j) -> nl_status {
       const int e = 8 * nT + 2 * j;  // timing events after the update events
-      if (tm) cudaEventRecord(upd_ev_[e], st_);
+      if (tmc) cudaEventRecord(upd_ev_[e], st_);
       // a programmatic dependent of the diagonal update before it
-      NL_CUDA(launch_chain(potrf_diag_kernel<T>, 1, PT, kPotrfSmem, j > 0 && !tm, S_.as<T>(), ld_, j, Linv_.as<T>(),
-                           status, active));
-      if (tm) cudaEventRecord(upd_ev_[e + 1], st_);
+      NL_CUDA(launch_chain(potrf_diag_kernel<T>, 1, PT, kPotrfSmem, j > 0 && !tmc, S_.as<T>(), ld_, j,
+                           Linv_.as<T>(), status, active));
+      if (tmc) cudaEventRecord(upd_ev_[e + 1], st_);
       npev = j + 1;
       launches++;
       return NL_OK;
@@ -479,17 +480,17 @@ class SchurCoreT final : public SchurCore {
       times.update_flop = upd_flop;
       times.update_bytes = upd_bytes;
       float pt = 0;
-      for (int j = 0; j < npev; j++) {
+      for (int j = 0; j < npev && tmc; j++) {
         float ms = 0;
         cudaEventElapsedTime(&ms, upd_ev_[8 * nT + 2 * j], upd_ev_[8 * nT + 2 * j + 1]);
         pt += ms;
       }
       times.panel_ms = pt;
-      times.panels = npev;
+      times.panels = tmc ? npev : 0;
       // per row tile j+1: the waits for the other streams (potrf(j) end ->
       // TRSM start, TRSM end -> update start) and the two 8-CTA kernels
       float wt = 0, ft = 0;
-      for (int j = 0; j + 1 < npev; j++) {
+      for (int j = 0; j + 1 < npev && tmc; j++) {
         const cudaEvent_t* e = &upd_ev_[10 * nT + 4 * j];
         float a = 0, b = 0, c = 0, d = 0;
         cudaEventElapsedTime(&a, upd_ev_[8 * nT + 2 * j + 1], e[0]);

@@ -87,7 +87,7 @@ EXPORTS = [
     "nl_rollback", "nl_max_abs_b", "nl_chi2", "nl_rho", "nl_lm_solve", "nl_gn_solve", "nl_phase_timings",
     "nl_kernel_launches", "nl_solver_create", "nl_solver_destroy", "nl_solver_set_hessian",
     "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_selftest_tc_update", "nl_ba_cost_noalloc",
-    "nl_adjoint", "nl_lm_solve_batch",
+    "nl_adjoint", "nl_lm_solve_batch", "nl_set_timing_detail",
     "nl_status_string",
     "nl_version",
 ]
@@ -328,6 +328,11 @@ class BAProblemGPU:
         t = PhaseTimes()
         self._c(self.L.nl_phase_timings(self.h, C.byref(t)), "nl_phase_timings")
         return {n: getattr(t, n) for n, _ in PhaseTimes._fields_}
+
+    def set_timing_detail(self, detail: bool):
+        """Time every critical-path step of the factorisation in the next
+        compute_increment calls (slower: see nl_set_timing_detail)."""
+        self._c(self.L.nl_set_timing_detail(self.h, C.c_int(1 if detail else 0)), "nl_set_timing_detail")
 
     def kernel_launches(self):
         v = C.c_longlong()

@@ -211,7 +211,7 @@ def run_batch(args, rank, world):
         line = {"metric": "problems/s (batched uneven problems, LM)", "value": len(probs) / (span_ms / 1e3),
                 "unit": "problems/s", "n_gpus": world, "steps": its, "warmup": args.warmup,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32 (FP64 panels/refinement/cost)", "data": "synthetic (seeded, config-3 generator)",
+                "dtype": "f32 (FP64 refinement residual, solve accumulators, cost)", "data": "synthetic (seeded, config-3 generator)",
                 "config": {"workload": "config 3: 256 problems, cams U{8..64} (6-param), pts U{200..4000}, "
                                        f"k~U{{3..8}}, {its} LM iterations each"},
                 "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
@@ -393,7 +393,7 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_m / its_m, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32 (FP64 panels/refinement/cost)",
+                "vs_baseline": None, "dtype": "f32 (FP64 refinement residual, solve accumulators, cost)",
                 "data": "synthetic (seeded, config-2 shapes; no public dataset)",
                 "config": {"workload": f"config {args.config}: 1500 cams (9-param) / 500k pts / "
                                        f"{prob.ne} obs, LevenbergMarquardt",

@@ -655,6 +655,17 @@ static __device__ inline bool wait_flag(const int* flag, int epoch, int* status)
   return true;
 }
 
+// Publish a solved tile: the barrier orders every thread's writes of the
+// tile before thread 0's GPU-scope fence, which by cumulativity orders them
+// before the flag for every observer (one fence per CTA, not one per thread).
+__device__ inline void publish_tile(int* flag, int epoch, int tid) {
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    atomicExch(flag, epoch);
+  }
+}
+
 template <typename T>
 __device__ inline void load4(const T* p, double* v) {
   if (sizeof(T) == 4) {
@@ -731,9 +742,7 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
     const double s = warp_sum(lv[0] * av[0] + lv[1] * av[1] + lv[2] * av[2] + lv[3] * av[3]);
     if (lane == 0) y[(size_t)I * NB + warp * 8 + rr] = s;
   }
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) atomicExch(flags + I, epoch);
+  publish_tile(flags + I, epoch, tid);
 }
 
 template <typename T>
@@ -809,9 +818,7 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
     for (int w = 0; w < SV / 32; w++) s += red[w][tid];
     x[(size_t)I * NB + tid] = s;
   }
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) atomicExch(flags + I, epoch);
+  publish_tile(flags + I, epoch, tid);
 }
 
 // ---------------------------------------------------------------------------

@@ -642,28 +642,32 @@ __device__ inline void syrk_cc_tile(T* __restrict__ S, int ld, int k, int gI, in
 // 512 threads: warp w owns rows 8w..8w+7 of a 128-row tile, lane l owns
 // columns 4l..4l+3; partial dot products stay in registers across tiles and
 // are reduced once.
+// Flags are read with GPU-scope acquire loads and written with release
+// stores: the acquire that sees a tile's flag orders the waiting CTA's later
+// reads of that tile (after its barrier) behind the tile's writes.
+__device__ inline int load_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 static __device__ inline bool wait_flag(const int* flag, int epoch, int* status) {
   long long it = 0;
-  while (*(volatile const int*)flag != epoch) {
+  while (load_acquire(flag) != epoch) {
     if (++it > kSpinLimit) {
       atomicOr(status, ST_SPIN_TIMEOUT);
       return false;
     }
     if (it > 4096) __nanosleep(100);
   }
-  __threadfence();
   return true;
 }
 
 // Publish a solved tile: the barrier orders every thread's writes of the
-// tile before thread 0's GPU-scope fence, which by cumulativity orders them
-// before the flag for every observer (one fence per CTA, not one per thread).
+// tile before thread 0's release store of the flag, which by cumulativity
+// orders them before the flag for every observer (one release per CTA).
 __device__ inline void publish_tile(int* flag, int epoch, int tid) {
   __syncthreads();
-  if (tid == 0) {
-    __threadfence();
-    atomicExch(flag, epoch);
-  }
+  if (tid == 0) asm volatile("st.release.gpu.global.b32 [%0], %1;\n" ::"l"(flag), "r"(epoch) : "memory");
 }
 
 template <typename T>

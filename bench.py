@@ -333,6 +333,24 @@ def main():
     h2d = (cams_h.numel() + pts_h.numel() + obs_h.numel()) * 8
     d2h = (cams_o.numel() + pts_o.numel()) * 8
 
+    # ---- the envelope solver (nl_set_solver_kind) on the same problem: the
+    #      same increments, the tiles of S outside its Cholesky envelope skipped
+    #      (a side measurement; the metric above is the dense solver's) ----
+    envelope = {"note": "NL_SOLVER_ENVELOPE: tile-level profile Cholesky of the same S, camera order unchanged"}
+    for name, g in (("mixed", gm), ("fp64", gd)):
+        g.set_solver_kind(N.SOLVER_ENVELOPE)
+        g.set_params(prob.cams, prob.pts)
+        g.lm_solve(N.LMSettings(maxNumIt=1), trace_cap=0)
+        g.set_params(prob.cams, prob.pts)
+        barrier()
+        _, _, it_e, _, rep_e = g.lm_solve(N.LMSettings(maxNumIt=args.steps), trace_cap=4096, report=True)
+        barrier()
+        envelope[name] = {"value": world * max(it_e, 1) / (max_over_ranks(rep_e["device_ms"]) / 1000.0),
+                          "unit": UNIT, "final_chi2": rep_e["chi2"]}
+        g.set_solver_kind(N.SOLVER_DENSE)
+    envelope["speedup_vs_fp64_gpu"] = envelope["mixed"]["value"] / envelope["fp64"]["value"]
+    envelope["final_chi2_equal_to_dense"] = envelope["mixed"]["final_chi2"] == chi2_m
+
     # ---- roofline of the dominant kernel: the trailing update of the factorisation ----
     hbm, bf16, peak_src = measured_peaks()
     gm.set_params(prob.cams, prob.pts)
@@ -405,7 +423,8 @@ def main():
                 "final_chi2": chi2_m, "reason": r_m, "subiterations": sub_m,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "step": f"upload + nl_lm_solve({args.steps} its) + download"},
-                "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": ck}
+                "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": ck,
+                "envelope_solver": envelope}
         print(json.dumps(line), flush=True)
     gm.close()
     gd.close()

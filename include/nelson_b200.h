@@ -43,7 +43,16 @@ typedef enum {
 /* ---- precision modes ---------------------------------------------------- */
 #define NL_PREC_FP64 0  /* Jacobians, Hessian, Schur and Cholesky in FP64      */
 #define NL_PREC_MIXED 1 /* FP32 Jacobians/Hessian/Schur, tensor-core trailing
-                           updates, FP64 diagonal panels + refinement + cost   */
+                           updates, FP32 diagonal tiles, FP64 refinement residual,
+                           solve accumulators and cost                          */
+
+/* Factorisation of the reduced camera system S (nl_set_solver_kind). */
+#define NL_SOLVER_DENSE 0    /* every 128-tile of S, as SolverCholeskySchur's dense
+                                LDLT (nelson/SolverCholeskySchur.hpp:136-140)     */
+#define NL_SOLVER_ENVELOPE 1 /* only the tiles inside the Cholesky envelope of S:
+                                the same factor (there is no fill before a row's
+                                first nonzero), far less work when the camera
+                                order keeps camera pairs near the diagonal        */
 
 /* ---- settings (same fields and defaults as the reference) --------------- */
 /* LevenbergMarquardtSettings, nelson/LevenbergMarquardt.h:18-34;
@@ -232,6 +241,16 @@ nl_status nl_phase_timings(nl_problem* h, nl_phase_times* out);
  * of the chain's kernels, so the factorisation itself runs slower; 0 (the
  * default) times the phases and the trailing updates only. */
 nl_status nl_set_timing_detail(nl_problem* h, int detail);
+/* NL_SOLVER_DENSE (default) or NL_SOLVER_ENVELOPE for the computeIncrements
+ * that follow.  The envelope solver is the tile-level profile Cholesky of the
+ * same S in the same (internal) camera order: its increments are
+ * bit-identical to the dense solver's, the trailing updates, panel TRSMs and
+ * triangular solves skip the tiles that are zero in the factor.  It is the
+ * dense-kernel step toward the block-sparse
+ * SolverDiagonalBlocksInverseWWtMultSchur
+ * (nelson/SolverDiagonalBlocksInverseWWtMultSchur.hpp:36-140), without that
+ * solver's AMD reordering (nelson/DoubleSection.hpp:30-63). */
+nl_status nl_set_solver_kind(nl_problem* h, int kind);
 /* Number of kernels of this library launched on the handle since creation. */
 nl_status nl_kernel_launches(nl_problem* h, long long* out);
 
@@ -257,6 +276,8 @@ nl_status nl_solver_set_hessian(nl_solver* s, const double* U, const double* V,
 nl_status nl_solver_max_abs_hdiag(nl_solver* s, double* out);
 nl_status nl_solver_compute_increment(nl_solver* s, double rel_lambda, double abs_lambda,
                                       double* incU, double* incV, int* ok);
+/* nl_set_solver_kind for the solver-only handle. */
+nl_status nl_solver_set_kind(nl_solver* s, int kind);
 
 /* Device self-test of the mixed path's tensor-core trailing update: builds a
  * random FP32 matrix of ntiles x 128 rows on `device`, applies the panel-0

@@ -700,6 +700,7 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
                                                              const double* __restrict__ b, double* __restrict__ y,
                                                              int* __restrict__ ticket, int* __restrict__ flags,
                                                              int epoch, int* __restrict__ status,
+                                                             const int* __restrict__ env,
                                                              const int* __restrict__ active) {
   extern __shared__ float4 sLi4[];
   T* sLi = reinterpret_cast<T*>(sLi4);  // Linv_I, NB x NB
@@ -717,7 +718,8 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
   }
   double part[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   const T* Lrow = L + (size_t)(I * NB + warp * 8) * ld + 4 * lane;
-  for (int J = 0; J < I; J++) {
+  // with an envelope, the tiles of row I before its first nonzero are zero
+  for (int J = env ? env[I] : 0; J < I; J++) {
     double lv[8][4];  // the L tile does not depend on y_J: load it before waiting
 #pragma unroll
     for (int rr = 0; rr < 8; rr++) load4(Lrow + (size_t)rr * ld + (size_t)J * NB, lv[rr]);
@@ -755,6 +757,7 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
                                                              const double* __restrict__ yv, double* __restrict__ x,
                                                              int* __restrict__ ticket, int* __restrict__ flags,
                                                              int epoch, int* __restrict__ status,
+                                                             const int* __restrict__ env,
                                                              const int* __restrict__ active) {
   extern __shared__ float4 sLi4[];
   T* sLi = reinterpret_cast<T*>(sLi4);  // Linv_I, NB x NB
@@ -772,7 +775,8 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
     for (int i = tid; i < (int)(NB * NB * sizeof(T) / 16); i += SV) dst[i] = src[i];
   }
   double part[4] = {0, 0, 0, 0};
-  for (int J = ntiles - 1; J > I; J--) {
+  // with an envelope, the tiles of column I past its last nonzero are zero
+  for (int J = env ? env[ntiles + I] : ntiles - 1; J > I; J--) {
     const T* Lb = L + (size_t)(J * NB + warp * 8) * ld + (size_t)I * NB + 4 * lane;
     double lv[8][4];  // loaded before waiting for x_J
 #pragma unroll

@@ -1185,6 +1185,14 @@ nl_status nl_phase_timings(nl_problem* h, nl_phase_times* out) {
   return NL_OK;
 }
 
+nl_status nl_set_solver_kind(nl_problem* h, int kind) {
+  NL_CHECK_H(h);
+  if (kind != NL_SOLVER_DENSE && kind != NL_SOLVER_ENVELOPE) return NL_ERR_ARG;
+  if (!h->core) return NL_ERR_STATE;
+  h->core->envelope = kind == NL_SOLVER_ENVELOPE ? 1 : 0;
+  return NL_OK;
+}
+
 nl_status nl_set_timing_detail(nl_problem* h, int detail) {
   NL_CHECK_H(h);
   h->timing_detail = detail ? 1 : 0;
@@ -1300,6 +1308,13 @@ nl_status nl_solver_max_abs_hdiag(nl_solver* s, double* out) {
   NL_CUDA(cudaMemcpyAsync(s->pin, dv, sizeof(double), cudaMemcpyDeviceToHost, s->st));
   NL_CUDA(cudaStreamSynchronize(s->st));
   *out = s->pin[0];
+  return NL_OK;
+}
+
+nl_status nl_solver_set_kind(nl_solver* s, int kind) {
+  if (!s || !s->core) return NL_ERR_ARG;
+  if (kind != NL_SOLVER_DENSE && kind != NL_SOLVER_ENVELOPE) return NL_ERR_ARG;
+  s->core->envelope = kind == NL_SOLVER_ENVELOPE ? 1 : 0;
   return NL_OK;
 }
 

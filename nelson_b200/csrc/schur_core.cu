@@ -89,6 +89,24 @@ class SchurCoreT final : public SchurCore {
         }
     for (int q = 0; q < nU_; q++) s_uuid[bid[(size_t)st.u_r[q] * nci_ + st.u_c[q]]] = q;
     nS_ = (int)s_i.size();
+    // Cholesky envelope of S by 128-tiles: env_first_[T] = first tile column
+    // with a nonzero in tile row T (block (i, j), i <= j, sits at rows j BC..,
+    // columns i BC.. of the lower storage).  The factor has no fill before a
+    // row's first nonzero, so L_TJ = 0 for J < env_first_[T].
+    // env_last_[k] = last tile row T with env_first_[T] <= k (the last
+    // nonzero tile of L's column k); env_run_[k] = max over k' <= k of it.
+    env_first_.assign(ntiles_, 0);
+    for (int t = 0; t < ntiles_; t++) env_first_[t] = t;
+    for (int b = 0; b < nS_; b++) {
+      const int tc = (s_i[b] * BC) / NB;
+      for (int t = (s_j[b] * BC) / NB; t <= (s_j[b] * BC + BC - 1) / NB; t++) env_first_[t] = std::min(env_first_[t], tc);
+    }
+    env_last_.assign(ntiles_, 0);
+    for (int k = 0; k < ntiles_; k++) env_last_[k] = k;
+    for (int t = 0; t < ntiles_; t++)
+      for (int k = env_first_[t]; k < t; k++) env_last_[k] = std::max(env_last_[k], t);
+    env_run_.assign(ntiles_, 0);
+    for (int k = 0; k < ntiles_; k++) env_run_[k] = std::max(env_last_[k], k > 0 ? env_run_[k - 1] : 0);
     // Schur work order: output blocks by pair count, heaviest first
     std::vector<int> s_order(std::max(nS_, 1), 0);
     for (int b = 0; b < nS_; b++) s_order[b] = b;
@@ -132,6 +150,10 @@ class SchurCoreT final : public SchurCore {
     // the diagonal-tile factor writes only the blocks on and below the
     // diagonal: the strictly upper blocks of every inverse stay zero
     NL_CUDA(cudaMemsetAsync(Linv_.p, 0, Linv_.bytes, st_));
+    NL_TRY(env_dev_.alloc(sizeof(int) * 2 * (size_t)ntiles_));
+    NL_CUDA(cudaMemcpyAsync(env_dev_.p, env_first_.data(), sizeof(int) * ntiles_, cudaMemcpyHostToDevice, st_));
+    NL_CUDA(cudaMemcpyAsync(env_dev_.as<int>() + ntiles_, env_last_.data(), sizeof(int) * ntiles_,
+                            cudaMemcpyHostToDevice, st_));
     NL_TRY(flags_.alloc(sizeof(int) * (size_t)(ntiles_ + 1)));
     NL_TRY(S_.alloc(sizeof(T) * (size_t)ld_ * ld_));
     need_s0_ = refine_sweeps > 0 || keep_schur;
@@ -220,11 +242,12 @@ class SchurCoreT final : public SchurCore {
   // ---- solves with the factor: x = S^-1 b (trsv fwd + bwd) ----
   nl_status enqueue_solve(const double* b, double* x, int* status, const int* active) {
     NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
+    const int* env = envelope ? env_dev_.as<int>() : nullptr;
     trsv_fwd_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), b, y_.as<double>(),
-                                                 flags_.as<int>(), flags_.as<int>() + 1, 1, status, active);
+                                                 flags_.as<int>(), flags_.as<int>() + 1, 1, status, env, active);
     NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
     trsv_bwd_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), y_.as<double>(), x,
-                                                 flags_.as<int>(), flags_.as<int>() + 1, 1, status, active);
+                                                 flags_.as<int>(), flags_.as<int>() + 1, 1, status, env, active);
     launches += 2;
     return NL_OK;
   }
@@ -238,6 +261,7 @@ class SchurCoreT final : public SchurCore {
   // on the side stream and waits for panel k.  The BF16 pack of panel k is
   // double-buffered.
   nl_status launch_update(int k, int t0, int nt, bool col_only, cudaStream_t st, int* status, const int* active) {
+    nt = std::min(nt, env_end(k) - t0 + 1);  // tile rows past the envelope get zero updates
     if (nt <= 0) return NL_OK;
     if (sizeof(T) == 8 && precision_ == NL_PREC_FP64 && cublas_) {
       // Row-major lower storage = column-major upper.  X = rows >= r0 of
@@ -245,7 +269,7 @@ class SchurCoreT final : public SchurCore {
       double* Sd = reinterpret_cast<double*>(S_.p);
       const double alpha = -1.0, beta = 1.0;
       const size_t r0 = (size_t)t0 * NB, kc = (size_t)k * NB;
-      const int n_rem = ld_ - (int)r0;
+      const int n_rem = nt * NB;  // ld_ - r0 without the envelope
       // each stream has its own handle (and workspace)
       cublasHandle_t hb = (st == st_) ? cublas_ : cublas2_;
       if (cublasSetStream(hb, st) != CUBLAS_STATUS_SUCCESS) return NL_ERR_CUDA;
@@ -280,7 +304,7 @@ class SchurCoreT final : public SchurCore {
   nl_status factor_panel(int k, int* status, const int* active) {
     potrf_diag_kernel<T><<<1, PT, kPotrfSmem, st_>>>(S_.as<T>(), ld_, k, Linv_.as<T>(), status, active);
     launches++;
-    const int below = ld_ - (k + 1) * NB;
+    const int below = std::min(ld_, (env_end(k) + 1) * NB) - (k + 1) * NB;  // rows past the envelope are zero
     if (below > 0) {
       trsm_kernel<T><<<cdiv(below, TRSM_ROWS), 256, trsm_smem<T>(), st_>>>(S_.as<T>(), ld_, k, (k + 1) * NB, below,
                                                                             Linv_.as<T>(), nullptr, active);
@@ -358,6 +382,7 @@ class SchurCoreT final : public SchurCore {
       return t;
     };
     auto upd = [&](int k, bool pair, int t0, int nt, int ncols, int rb, cudaStream_t st) -> nl_status {
+      nt = std::min(nt, env_end(k + 1) - t0 + 1);  // tile rows past the envelope get zero updates
       if (nt <= 0 || tiles_of(nt, ncols, rb) <= 0) return NL_OK;
       if (tm) NL_CUDA(cudaEventRecord(upd_ev_[nev], st));
       NL_CUDA(tc_update_f32(S, ld_, k, t0, nt, ncols, rb, pack_slot(k), pair ? pack_slot(k + 1) : nullptr, active,
@@ -371,6 +396,9 @@ class SchurCoreT final : public SchurCore {
     };
     // TRSM + pack of panel j's rows [r0, r0 + nrows) (absolute rows, tile aligned)
     auto trsm_pack = [&](int j, int r0, int nrows, cudaStream_t st) -> nl_status {
+      // rows past the envelope are zero in L; the pack covers every row the
+      // pair updates of panels j - 1 .. j + 1 read
+      nrows = std::min(nrows, (env_end(j + 1) + 1) * NB - r0);
       if (nrows <= 0) return NL_OK;
       // the TRSM writes the BF16 pack of its rows in its epilogue
       trsm_kernel<T><<<cdiv(nrows, TRSM_ROWS), 256, trsm_smem<T>(), st>>>(S_.as<T>(), ld_, j, r0, nrows,
@@ -746,6 +774,11 @@ class SchurCoreT final : public SchurCore {
   bool need_s0_ = false;
   SchurDev d_{};
   DevBuf U_, V_, W_, Y_, Vinv_, bU_, bV_, bS_, incU_, incV_, y_, r_, dx_, part_, Linv_, flags_, S_, S0_, tcs_;
+  // envelope of S (host) and its first / last arrays on the device (solves)
+  std::vector<int> env_first_, env_last_, env_run_;
+  DevBuf env_dev_;
+  // last tile row that panel k's TRSM and updates must cover
+  int env_end(int k) const { return envelope ? env_run_[std::min(k, ntiles_ - 1)] : ntiles_ - 1; }
   DevBuf v_uid_, w_row_ptr_, w_col_, w_row_, w_col_ptr_, w_col_uid_, u_diag_, s_i_, s_j_, s_uuid_, s_ptr_, pa_, pb_, s_order_,
       sched_;
   cudaEvent_t ev_[7] = {};

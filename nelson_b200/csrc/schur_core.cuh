@@ -106,6 +106,7 @@ class SchurCore {
   nl_phase_times times{};
   long long launches = 0;
   int timing = 0;          // record per-phase CUDA events
+  int envelope = 0;        // envelope solver: skip the tiles of S outside the Cholesky envelope
   int timing_detail = 0;   // with timing: also per-panel events on the factorisation's critical path
                            // (costly on the host: one record per kernel boundary, and no early launch)
 };

@@ -14,6 +14,7 @@ import numpy as np
 from . import build as _build
 
 PREC_FP64, PREC_MIXED = 0, 1
+SOLVER_DENSE, SOLVER_ENVELOPE = 0, 1
 TRACE_STRIDE = 8
 REASONS = ["SuccessAtStart", "SuccessSmallIncrement", "SuccessEpsB", "SuccessSmallResiduals",
            "SolverFailure", "MaxIterationReached", "MaxSubIterationReached"]
@@ -87,7 +88,7 @@ EXPORTS = [
     "nl_rollback", "nl_max_abs_b", "nl_chi2", "nl_rho", "nl_lm_solve", "nl_gn_solve", "nl_phase_timings",
     "nl_kernel_launches", "nl_solver_create", "nl_solver_destroy", "nl_solver_set_hessian",
     "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_selftest_tc_update", "nl_ba_cost_noalloc",
-    "nl_adjoint", "nl_lm_solve_batch", "nl_set_timing_detail",
+    "nl_adjoint", "nl_lm_solve_batch", "nl_set_timing_detail", "nl_set_solver_kind", "nl_solver_set_kind",
     "nl_status_string",
     "nl_version",
 ]
@@ -329,6 +330,12 @@ class BAProblemGPU:
         self._c(self.L.nl_phase_timings(self.h, C.byref(t)), "nl_phase_timings")
         return {n: getattr(t, n) for n, _ in PhaseTimes._fields_}
 
+    def set_solver_kind(self, kind: int):
+        """SOLVER_DENSE (default) or SOLVER_ENVELOPE (nl_set_solver_kind): the
+        envelope solver skips the tiles of S outside its Cholesky envelope,
+        with bit-identical increments."""
+        self._c(self.L.nl_set_solver_kind(self.h, C.c_int(kind)), "nl_set_solver_kind")
+
     def set_timing_detail(self, detail: bool):
         """Time every critical-path step of the factorisation in the next
         compute_increment calls (slower: see nl_set_timing_detail)."""
@@ -379,6 +386,10 @@ class SchurSolverGPU:
         _chk(self.L, self.L.nl_solver_create(C.byref(d), _p(u_rc), _p(v_rc), _p(w_rc), C.byref(h)),
              "nl_solver_create")
         self.h = h
+
+    def set_solver_kind(self, kind: int):
+        """SOLVER_DENSE (default) or SOLVER_ENVELOPE (nl_solver_set_kind)."""
+        _chk(self.L, self.L.nl_solver_set_kind(self.h, C.c_int(kind)), "nl_solver_set_kind")
 
     def close(self):
         if getattr(self, "h", None):

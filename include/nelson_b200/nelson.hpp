@@ -250,7 +250,10 @@ class SolverCholeskySchurCuda {
   void init(BASection& p) {
     p_ = &p;
     check(nl_solver_init(p.handle()), "nl_solver_init");
+    select(p);
   }
+  // the factorisation this solver stands for, on p's handle
+  void select(BASection& p) { check(nl_set_solver_kind(p.handle(), NL_SOLVER_DENSE), "nl_set_solver_kind"); }
   double maxAbsHDiag() const {
     double m;
     check(nl_max_abs_hdiag(p_->handle(), &m), "nl_max_abs_hdiag");
@@ -282,6 +285,19 @@ class SolverCholeskySchurCuda {
 
  private:
   BASection* p_ = nullptr;
+};
+
+// The solver that takes SolverDiagonalBlocksInverseWWtMultSchur's place in
+// the solver choice (nelson/SolverDiagonalBlocksInverseWWtMultSchur.hpp:36-140):
+// the same Schur complement, factored over its Cholesky envelope only
+// (NL_SOLVER_ENVELOPE); its increments are SolverCholeskySchurCuda's.
+class SolverEnvelopeSchurCuda : public SolverCholeskySchurCuda {
+ public:
+  void init(BASection& p) {
+    SolverCholeskySchurCuda::init(p);
+    select(p);
+  }
+  void select(BASection& p) { check(nl_set_solver_kind(p.handle(), NL_SOLVER_ENVELOPE), "nl_set_solver_kind"); }
 };
 
 // ---------------------------------------------------------------------------
@@ -354,6 +370,7 @@ class LevenbergMarquardt {
 
   // The same loop with every step on the device (nl_lm_solve).
   TerminationReason solveOnDevice(BASection& P, nl_solve_report* report = nullptr) {
+    solver_.select(P);
     const nl_lm_settings c = settings_.c();
     nl_solve_report rep{};
     std::vector<double> tr(size_t(settings_.maxNumIt + 1) * (settings_.maxNumSubIt + 1) *
@@ -422,6 +439,7 @@ class GaussNewton {
   }
 
   TerminationReason solveOnDevice(BASection& P, nl_solve_report* report = nullptr) {
+    solver_.select(P);
     const nl_gn_settings c = settings_.c();
     nl_solve_report rep{};
     std::vector<double> tr(size_t(settings_.maxNumIt + 2) * NL_TRACE_STRIDE);

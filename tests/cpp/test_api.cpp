@@ -161,6 +161,18 @@ int main() {
       const double dg = trace_diff(gnA.stats(), gnB.stats(), &n);
       expect(gA == gB, "GN termination reason host == device", double(gA), double(gB));
       expect(dg <= tol, "GN per-iteration cost host vs device (rel)", dg, tol);
+
+      // 4. the envelope solver (SolverEnvelopeSchurCuda) gives the dense solver's trace
+      BASection e1 = make_section(s, prec, 11), e2 = make_section(s, prec, 11);
+      nelson_b200::LevenbergMarquardt<> lmD;
+      nelson_b200::LevenbergMarquardt<nelson_b200::SolverEnvelopeSchurCuda> lmE;
+      lmD.settings().maxNumIt = 10;
+      lmE.settings().maxNumIt = 10;
+      const auto rD = lmD.solveOnDevice(e1);
+      const auto rE = lmE.solveOnDevice(e2);
+      const double de = trace_diff(lmD.stats(), lmE.stats(), &n);
+      expect(rD == rE, "envelope solver termination reason == dense", double(rD), double(rE));
+      expect(de <= 1e-12, "envelope solver per-iteration cost vs dense (rel)", de, 1e-12);
     }
   } catch (const nelson_b200::Error& e) {
     std::printf("FAIL exception: %s\n", e.what());

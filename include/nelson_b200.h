@@ -154,6 +154,17 @@ nl_status nl_set_user2internal_u(nl_problem* h, const int* perm);
  * U/V/W patterns and block UIDs exactly as the reference and uploads the
  * edge -> block maps. */
 nl_status nl_structure_ready(nl_problem* h);
+/* In place of DoubleSection::permuteAMD_SchurU (nelson/DoubleSection.hpp:30-63):
+ * an internal camera order from the same camera graph (variable cameras that
+ * observe a common variable point, the pattern of U + W W'), computed by
+ * reverse Cuthill-McKee instead of AMD -- it narrows the envelope of S that
+ * NL_SOLVER_ENVELOPE factors (AMD aims at the fill of a sparse factor, which
+ * this library does not build).  Sets the user -> internal permutation; call
+ * after the edges are added and before nl_structure_ready. */
+nl_status nl_permute_rcm_u(nl_problem* h);
+/* The user -> internal camera permutation in effect (nc_var entries; the
+ * identity unless set): increments come in internal order. */
+nl_status nl_get_user2internal_u(nl_problem* h, int* perm);
 /* Replace observations / weights of an existing structure (same edge order). */
 nl_status nl_set_observations(nl_problem* h, const double* obs, const double* weight);
 

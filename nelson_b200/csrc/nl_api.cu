@@ -669,6 +669,83 @@ nl_status nl_set_user2internal_u(nl_problem* h, const int* perm) {
   return NL_OK;
 }
 
+nl_status nl_get_user2internal_u(nl_problem* h, int* perm) {
+  NL_CHECK_H(h);
+  if (!perm) return NL_ERR_ARG;
+  memcpy(perm, h->perm.data(), sizeof(int) * h->desc.nc_var);
+  return NL_OK;
+}
+
+nl_status nl_permute_rcm_u(nl_problem* h) {
+  NL_CHECK_H(h);
+  if (h->ready) return NL_ERR_STATE;
+  const int nc = h->desc.nc_var, ne = (int)h->e_cam.size();
+  if (nc == 0) return NL_OK;
+  // camera graph: variable cameras that observe a common variable point
+  std::vector<std::vector<int>> by_pt(h->desc.np_var);
+  for (int e = 0; e < ne; e++)
+    if (!h->e_camfix[e] && !h->e_ptfix[e]) by_pt[h->e_pt[e]].push_back(h->e_cam[e]);
+  std::vector<std::vector<int>> adj(nc);
+  for (auto& cams : by_pt)
+    for (size_t a = 0; a < cams.size(); a++)
+      for (size_t b = 0; b < cams.size(); b++)
+        if (cams[a] != cams[b]) adj[cams[a]].push_back(cams[b]);
+  std::vector<int> deg(nc);
+  for (int c = 0; c < nc; c++) {
+    std::sort(adj[c].begin(), adj[c].end());
+    adj[c].erase(std::unique(adj[c].begin(), adj[c].end()), adj[c].end());
+    deg[c] = (int)adj[c].size();
+  }
+  for (int c = 0; c < nc; c++)
+    std::sort(adj[c].begin(), adj[c].end(), [&](int x, int y) { return deg[x] != deg[y] ? deg[x] < deg[y] : x < y; });
+  // breadth-first levels from r; returns the visit order, marks `seen`
+  std::vector<int> level(nc, -1), order;
+  order.reserve(nc);
+  auto bfs = [&](int r, std::vector<int>& out) {
+    out.clear();
+    level[r] = 0;
+    out.push_back(r);
+    for (size_t q = 0; q < out.size(); q++)
+      for (int n : adj[out[q]])
+        if (level[n] < 0) {
+          level[n] = level[out[q]] + 1;
+          out.push_back(n);
+        }
+  };
+  std::vector<char> done(nc, 0);
+  std::vector<int> comp;
+  for (int s0 = 0; s0 < nc; s0++) {
+    if (done[s0]) continue;
+    // pseudo-peripheral start: the lowest-degree vertex of the last level,
+    // repeated while the eccentricity grows (George-Liu)
+    int r = s0;
+    bfs(r, comp);
+    for (int it = 0; it < 8; it++) {
+      const int ecc = level[comp.back()];
+      int best = comp.back();
+      for (int v : comp)
+        if (level[v] == ecc && deg[v] < deg[best]) best = v;
+      for (int v : comp) level[v] = -1;
+      std::vector<int> c2;
+      bfs(best, c2);
+      const bool grew = level[c2.back()] > ecc;
+      for (int v : c2) level[v] = -1;
+      if (!grew) break;
+      r = best;
+      bfs(r, comp);
+    }
+    for (int v : comp) level[v] = -1;
+    bfs(r, comp);  // Cuthill-McKee order of this component
+    for (int v : comp) {
+      done[v] = 1;
+      order.push_back(v);
+    }
+  }
+  // reversed: internal position i holds user camera order[nc - 1 - i]
+  for (int i = 0; i < nc; i++) h->perm[order[nc - 1 - i]] = i;
+  return NL_OK;
+}
+
 nl_status nl_structure_ready(nl_problem* h) {
   NL_CHECK_H(h);
   if (h->ready) return NL_ERR_STATE;

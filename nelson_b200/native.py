@@ -88,7 +88,7 @@ EXPORTS = [
     "nl_rollback", "nl_max_abs_b", "nl_chi2", "nl_rho", "nl_lm_solve", "nl_gn_solve", "nl_phase_timings",
     "nl_kernel_launches", "nl_solver_create", "nl_solver_destroy", "nl_solver_set_hessian",
     "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_selftest_tc_update", "nl_ba_cost_noalloc",
-    "nl_adjoint", "nl_lm_solve_batch", "nl_set_timing_detail", "nl_set_solver_kind", "nl_solver_set_kind",
+    "nl_adjoint", "nl_lm_solve_batch", "nl_set_timing_detail", "nl_set_solver_kind", "nl_solver_set_kind", "nl_permute_rcm_u", "nl_get_user2internal_u",
     "nl_status_string",
     "nl_version",
 ]
@@ -182,7 +182,9 @@ class BAProblemGPU:
         g._c(g.L.nl_add_ba_edges(g.h, prob.ne, _p(np.ascontiguousarray(prob.cam_idx, np.int32)), _p(cf),
                                  _p(np.ascontiguousarray(prob.pt_idx, np.int32)), _p(pf),
                                  _p(np.ascontiguousarray(prob.obs, np.float64)), _p(w)), "nl_add_ba_edges")
-        if perm is not None:
+        if isinstance(perm, str) and perm == "rcm":
+            g._c(g.L.nl_permute_rcm_u(g.h), "nl_permute_rcm_u")
+        elif perm is not None:
             g._c(g.L.nl_set_user2internal_u(g.h, _p(np.ascontiguousarray(perm, np.int32))), "set_user2internal")
         g.structure_ready()
         return g
@@ -329,6 +331,12 @@ class BAProblemGPU:
         t = PhaseTimes()
         self._c(self.L.nl_phase_timings(self.h, C.byref(t)), "nl_phase_timings")
         return {n: getattr(t, n) for n, _ in PhaseTimes._fields_}
+
+    def user2internal(self):
+        """The user -> internal camera permutation (nl_get_user2internal_u)."""
+        perm = np.zeros(self.nc_var, np.int32)
+        self._c(self.L.nl_get_user2internal_u(self.h, _p(perm)), "nl_get_user2internal_u")
+        return perm
 
     def set_solver_kind(self, kind: int):
         """SOLVER_DENSE (default) or SOLVER_ENVELOPE (nl_set_solver_kind): the

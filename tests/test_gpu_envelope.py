@@ -11,6 +11,8 @@ smaller trailing matrix, whose internal tiling may differ, so it is held to
 (camera pairs near the diagonal: a narrow envelope) and a ring scene (the
 ring closes, so the envelope spans the last tile rows).
 """
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -86,6 +88,52 @@ def test_envelope_solver_only_handle(oracle_lib, prec):
     tol = 1e-10 if prec == N.PREC_FP64 else 1e-4
     assert _rel(du1, du_o) < tol and _rel(dv1, dv_o) < tol
     s.close()
+
+
+def _shuffle_cameras(p, seed=5):
+    """The same scene with its variable cameras in a random order."""
+    q = np.random.default_rng(seed).permutation(p.nc_var)
+    inv = np.argsort(q).astype(np.int32)
+    return dataclasses.replace(p, cams=p.cams[q].copy(), cam_idx=inv[p.cam_idx],
+                               cams_true=None if p.cams_true is None else p.cams_true[q].copy(),
+                               name=p.name + "+shuffled")
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_rcm_order_narrows_a_shuffled_envelope(prec):
+    """nl_permute_rcm_u (the reverse Cuthill-McKee stand-in for
+    permuteAMD_SchurU) puts co-observing cameras next to each other again:
+    the envelope solver's trailing updates shrink, the LM trace stays the
+    same up to rounding (another elimination order)."""
+    p = _shuffle_cameras(make_config(2, 0.2))
+    runs = {}
+    for order in ("user", "rcm"):
+        g = N.BAProblemGPU.from_ba(p, precision=prec, perm=None if order == "user" else "rcm")
+        g.set_solver_kind(N.SOLVER_ENVELOPE)
+        g.update(True)
+        mu = 1e-3 * g.max_abs_hdiag()
+        assert g.compute_increment(0.0, mu)
+        nbytes = g.phase_times()["update_bytes"]
+        perm = g.user2internal()
+        g.set_params(p.cams, p.pts)
+        _, tr, _, _ = g.lm_solve(N.LMSettings(maxNumIt=4))
+        runs[order] = (nbytes, perm, tr[:, 2].copy())
+        g.close()
+    assert np.array_equal(np.sort(runs["rcm"][1]), np.arange(p.nc_var))
+    assert np.array_equal(runs["user"][1], np.arange(p.nc_var))
+    if prec == N.PREC_MIXED:
+        assert runs["rcm"][0] < 0.5 * runs["user"][0], (runs["rcm"][0], runs["user"][0])
+    c0, c1 = runs["user"][2], runs["rcm"][2]
+    tol = 1e-9 if prec == N.PREC_FP64 else 1e-6
+    assert len(c0) == len(c1) and np.abs(c1 - c0).max() <= tol * np.abs(c0).max()
+
+
+def test_rcm_order_only_before_structure():
+    p = make_config(0)
+    g = N.BAProblemGPU.from_ba(p, precision=N.PREC_MIXED)
+    with pytest.raises(N.NelsonError):
+        g._c(g.L.nl_permute_rcm_u(g.h), "nl_permute_rcm_u")
+    g.close()
 
 
 def test_envelope_rejects_unknown_kind():

@@ -79,7 +79,7 @@ Scene make_scene(unsigned seed) {
   return s;
 }
 
-BASection make_section(const Scene& s, int precision, unsigned seed) {
+BASection make_section(const Scene& s, int precision, unsigned seed, bool rcm = false) {
   BASection ba(9, s.nc, s.np, s.ncFix, s.npFix, precision, 500.0, 320.0, 240.0, 0);
   std::mt19937_64 g(seed);
   std::uniform_real_distribution<double> U(-1, 1);
@@ -97,6 +97,7 @@ BASection make_section(const Scene& s, int precision, unsigned seed) {
     ba.addEdge(NodeId(s.cam[e], s.camFixed[e] ? nelson_b200::NodeType::Fixed : nelson_b200::NodeType::Variable),
                NodeId(s.pt[e], s.ptFixed[e] ? nelson_b200::NodeType::Fixed : nelson_b200::NodeType::Variable),
                s.obs[2 * e], s.obs[2 * e + 1]);
+  if (rcm) ba.permuteRCM_SchurU();
   ba.structureReady();
   return ba;
 }
@@ -173,6 +174,16 @@ int main() {
       const double de = trace_diff(lmD.stats(), lmE.stats(), &n);
       expect(rD == rE, "envelope solver termination reason == dense", double(rD), double(rE));
       expect(de <= 1e-12, "envelope solver per-iteration cost vs dense (rel)", de, 1e-12);
+
+      // 5. the reverse Cuthill-McKee camera order (permuteRCM_SchurU): the same
+      //    trace up to rounding (another elimination order)
+      BASection r1 = make_section(s, prec, 11, true);
+      nelson_b200::LevenbergMarquardt<nelson_b200::SolverEnvelopeSchurCuda> lmR;
+      lmR.settings().maxNumIt = 10;
+      const auto rR = lmR.solveOnDevice(r1);
+      const double dr = trace_diff(lmD.stats(), lmR.stats(), &n);
+      (void)rR;
+      expect(dr <= tol, "RCM order per-iteration cost vs user order (rel)", dr, tol);
     }
   } catch (const nelson_b200::Error& e) {
     std::printf("FAIL exception: %s\n", e.what());

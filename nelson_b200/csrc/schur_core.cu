@@ -590,8 +590,14 @@ class SchurCoreT final : public SchurCore {
       times.update_ms = tot;
       times.update_launches = nupd;
       times.update_flop = upd_flop;
+      // tiles read and written per panel: block column k+1 and the triangle
+      // below it, both cut at the envelope (launch_update's clipping)
       double tiles = 0;
-      for (int m = 1; m < ntiles_; m++) tiles += (double)m * (m + 1) / 2;
+      for (int k = 0; k + 1 < ntiles_; k++) {
+        const int last = env_end(k);
+        const double na = std::max(0, last - k), nb = std::max(0, last - k - 1);
+        tiles += na + nb * (nb + 1) / 2;
+      }
       times.update_bytes = tiles * (double)NB * NB * sizeof(T) * 2;
     }
     return NL_OK;

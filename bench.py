@@ -116,6 +116,47 @@ class Clocks:
                 "samples": len(sm), "window_ms": round(1e3 * (t1 - t0), 1) if self.t0 is not None else None}
 
 
+class Ranks:
+    """The bench's N > 1 plumbing: one process per GPU, each solving its own
+    replica of the problem (the path has no cross-problem exchange).  The only
+    collectives are the barrier around a timed region and the max of the
+    per-rank times; the reported rate is the whole job's: world x the units
+    one rank processed / the slowest rank's time."""
+
+    def __init__(self, world, backend, device, timeout_s=600):
+        import torch
+        self.torch, self.world, self.device, self.pg = torch, world, device, None
+        if world > 1:
+            import torch.distributed as dist
+            from datetime import timedelta
+            kw = {"device_id": device} if backend == "nccl" else {}
+            dist.init_process_group(backend, timeout=timedelta(seconds=timeout_s), **kw)
+            self.pg = dist
+
+    def barrier(self):
+        if self.device.type == "cuda":
+            self.torch.cuda.synchronize()
+        if self.pg is not None:
+            self.pg.barrier()
+
+    def max(self, x):
+        if self.pg is None:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=self.device)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def total_rate(self, units_per_rank, seconds):
+        """Whole-job units/s from one rank's units and this rank's seconds
+        (max over ranks taken here)."""
+        return self.world * units_per_rank / self.max(seconds)
+
+    def close(self):
+        if self.pg is not None:
+            self.pg.destroy_process_group()
+            self.pg = None
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -245,12 +286,7 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
-        pg = dist
+    ranks = Ranks(world, "nccl", torch.device("cuda", local))
 
     from nelson_b200 import native as N
     from nelson_b200.problems import make_config
@@ -259,17 +295,8 @@ def main():
     gm = N.BAProblemGPU.from_ba(prob, precision=N.PREC_MIXED, device=local)
     gd = N.BAProblemGPU.from_ba(prob, precision=N.PREC_FP64, device=local)
 
-    def barrier():
-        torch.cuda.synchronize()
-        if pg is not None:
-            pg.barrier()
-
-    def max_over_ranks(x):
-        if pg is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+    barrier = ranks.barrier
+    max_over_ranks = ranks.max
 
     # ---- warm-up: W LM iterations on both paths ----
     for g in (gm, gd):
@@ -428,8 +455,7 @@ def main():
         print(json.dumps(line), flush=True)
     gm.close()
     gd.close()
-    if pg is not None:
-        pg.destroy_process_group()
+    ranks.close()
 
 
 if __name__ == "__main__":

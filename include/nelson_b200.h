@@ -162,6 +162,10 @@ nl_status nl_structure_ready(nl_problem* h);
  * this library does not build).  Sets the user -> internal permutation; call
  * after the edges are added and before nl_structure_ready. */
 nl_status nl_permute_rcm_u(nl_problem* h);
+/* The same ordering as a host function that needs no device: nc cameras, np
+ * points, ne edges (cam[e], pt[e]); writes perm[camera] = internal position
+ * (reverse Cuthill-McKee of the graph of cameras sharing a point). */
+nl_status nl_rcm_order(int nc, int np, int ne, const int* cam, const int* pt, int* perm);
 /* The user -> internal camera permutation in effect (nc_var entries; the
  * identity unless set): increments come in internal order. */
 nl_status nl_get_user2internal_u(nl_problem* h, int* perm);

@@ -676,15 +676,14 @@ nl_status nl_get_user2internal_u(nl_problem* h, int* perm) {
   return NL_OK;
 }
 
-nl_status nl_permute_rcm_u(nl_problem* h) {
-  NL_CHECK_H(h);
-  if (h->ready) return NL_ERR_STATE;
-  const int nc = h->desc.nc_var, ne = (int)h->e_cam.size();
-  if (nc == 0) return NL_OK;
-  // camera graph: variable cameras that observe a common variable point
-  std::vector<std::vector<int>> by_pt(h->desc.np_var);
+nl_status nl_rcm_order(int nc, int np, int ne, const int* cam, const int* pt, int* perm) {
+  if (nc < 0 || np < 0 || ne < 0 || !perm || (ne > 0 && (!cam || !pt))) return NL_ERR_ARG;
   for (int e = 0; e < ne; e++)
-    if (!h->e_camfix[e] && !h->e_ptfix[e]) by_pt[h->e_pt[e]].push_back(h->e_cam[e]);
+    if (cam[e] < 0 || cam[e] >= nc || pt[e] < 0 || pt[e] >= np) return NL_ERR_ARG;
+  if (nc == 0) return NL_OK;
+  // camera graph: cameras that observe a common point
+  std::vector<std::vector<int>> by_pt(np);
+  for (int e = 0; e < ne; e++) by_pt[pt[e]].push_back(cam[e]);
   std::vector<std::vector<int>> adj(nc);
   for (auto& cams : by_pt)
     for (size_t a = 0; a < cams.size(); a++)
@@ -698,7 +697,7 @@ nl_status nl_permute_rcm_u(nl_problem* h) {
   }
   for (int c = 0; c < nc; c++)
     std::sort(adj[c].begin(), adj[c].end(), [&](int x, int y) { return deg[x] != deg[y] ? deg[x] < deg[y] : x < y; });
-  // breadth-first levels from r; returns the visit order, marks `seen`
+  // breadth-first levels from r, neighbours in increasing degree
   std::vector<int> level(nc, -1), order;
   order.reserve(nc);
   auto bfs = [&](int r, std::vector<int>& out) {
@@ -713,7 +712,7 @@ nl_status nl_permute_rcm_u(nl_problem* h) {
         }
   };
   std::vector<char> done(nc, 0);
-  std::vector<int> comp;
+  std::vector<int> comp, c2;
   for (int s0 = 0; s0 < nc; s0++) {
     if (done[s0]) continue;
     // pseudo-peripheral start: the lowest-degree vertex of the last level,
@@ -726,7 +725,6 @@ nl_status nl_permute_rcm_u(nl_problem* h) {
       for (int v : comp)
         if (level[v] == ecc && deg[v] < deg[best]) best = v;
       for (int v : comp) level[v] = -1;
-      std::vector<int> c2;
       bfs(best, c2);
       const bool grew = level[c2.back()] > ecc;
       for (int v : c2) level[v] = -1;
@@ -741,9 +739,22 @@ nl_status nl_permute_rcm_u(nl_problem* h) {
       order.push_back(v);
     }
   }
-  // reversed: internal position i holds user camera order[nc - 1 - i]
-  for (int i = 0; i < nc; i++) h->perm[order[nc - 1 - i]] = i;
+  // reversed: internal position i holds camera order[nc - 1 - i]
+  for (int i = 0; i < nc; i++) perm[order[nc - 1 - i]] = i;
   return NL_OK;
+}
+
+nl_status nl_permute_rcm_u(nl_problem* h) {
+  NL_CHECK_H(h);
+  if (h->ready) return NL_ERR_STATE;
+  // the edges between variable cameras and variable points
+  std::vector<int> cam, pt;
+  for (size_t e = 0; e < h->e_cam.size(); e++)
+    if (!h->e_camfix[e] && !h->e_ptfix[e]) {
+      cam.push_back(h->e_cam[e]);
+      pt.push_back(h->e_pt[e]);
+    }
+  return nl_rcm_order(h->desc.nc_var, h->desc.np_var, (int)cam.size(), cam.data(), pt.data(), h->perm.data());
 }
 
 nl_status nl_structure_ready(nl_problem* h) {

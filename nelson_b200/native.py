@@ -88,7 +88,7 @@ EXPORTS = [
     "nl_rollback", "nl_max_abs_b", "nl_chi2", "nl_rho", "nl_lm_solve", "nl_gn_solve", "nl_phase_timings",
     "nl_kernel_launches", "nl_solver_create", "nl_solver_destroy", "nl_solver_set_hessian",
     "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_selftest_tc_update", "nl_ba_cost_noalloc",
-    "nl_adjoint", "nl_lm_solve_batch", "nl_set_timing_detail", "nl_set_solver_kind", "nl_solver_set_kind", "nl_permute_rcm_u", "nl_get_user2internal_u",
+    "nl_adjoint", "nl_lm_solve_batch", "nl_set_timing_detail", "nl_set_solver_kind", "nl_solver_set_kind", "nl_permute_rcm_u", "nl_get_user2internal_u", "nl_rcm_order",
     "nl_status_string",
     "nl_version",
 ]
@@ -353,6 +353,18 @@ class BAProblemGPU:
         v = C.c_longlong()
         self._c(self.L.nl_kernel_launches(self.h, C.byref(v)), "nl_kernel_launches")
         return v.value
+
+
+def rcm_order(nc, np_, cam_idx, pt_idx):
+    """nl_rcm_order: the reverse Cuthill-McKee internal camera order of a
+    camera / point edge list (host only, no device); perm[camera] = position."""
+    L = load()
+    cam = np.ascontiguousarray(cam_idx, np.int32)
+    pt = np.ascontiguousarray(pt_idx, np.int32)
+    perm = np.zeros(nc, np.int32)
+    _chk(L, L.nl_rcm_order(C.c_int(nc), C.c_int(np_), C.c_int(cam.size), _p(cam), _p(pt), _p(perm)),
+         "nl_rcm_order")
+    return perm
 
 
 def lm_solve_batch(problems, settings=None):

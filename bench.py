@@ -15,7 +15,13 @@ computeIncrement + oplus + cost + gain ratio, then the Jacobian pass.
               uploads cameras, points and observations from pinned memory,
               runs nl_lm_solve for the K iterations, downloads the parameters.
   roofline    the dominant kernel (the Cholesky trailing update of S).
-  cpu_baseline the FP64 CPU oracle (OpenMP, all host cores) on a bounded sample.
+  cpu_baseline the FP64 CPU oracle (OpenMP, all host cores) on a bounded sample
+              (2 LM iterations at config 2; all K iterations at configs 0 / 1).
+  oracle_parity the per-sub-iteration cost, damping and gain ratio of both GPU
+              traces against that oracle sample's (bounds 1e-9 FP64, 1e-6 mixed).
+
+--config 1 (or 0) runs the same measurement on that workload: config 1 is 200
+9-parameter cameras, 50,000 points, 375 k observations (S 1,800 x 1,800).
 
 --impl reference times the FP64 CPU oracle (the restatement of the reference's
 CPU path) on the same workload; under torchrun only rank 0 runs it.
@@ -158,11 +164,48 @@ class Ranks:
 
 
 def measured_peaks():
+    """HBM copy bandwidth (GB/s) and dense BF16 throughput (TF/s, burst and
+    sustained) of this pool's B200s, or the fallback figures."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
-    return 6650.0, 1590.0, "fallback"
+        return {"hbm": d.get("hbm_gbs", 6650.0), "bf16": d.get("bf16_tflops", 1590.0),
+                "bf16_sustained": d.get("bf16_tflops_sustained", d.get("bf16_tflops", 1400.0)), "src": "measured"}
+    return {"hbm": 6650.0, "bf16": 1590.0, "bf16_sustained": 1400.0, "src": "fallback"}
+
+
+def workload_config(cfg, scale, prob, world):
+    """The `config` object both arms print for the same workload."""
+    s_bytes = (-(-prob.nc_var * prob.bc // 128) * 128) ** 2 * 4
+    w_bytes = prob.ne * 112
+    big = s_bytes + w_bytes > 126 * 2 ** 20
+    return {"workload": f"config {cfg}: {prob.nc_var} cams ({prob.bc}-param) / {prob.np_var} pts / "
+                        f"{prob.ne} obs, LevenbergMarquardt",
+            "scale": scale, "parallelism": f"replicas x{world}",
+            "l2": (f"inputs larger than L2 (S {s_bytes / 2**20:.0f} MiB + W {w_bytes / 2**20:.0f} MiB FP32)" if big
+                   else f"working set {(s_bytes + w_bytes) / 2**20:.0f} MiB (S + W, FP32) is not larger than L2 "
+                        f"and L2 is not flushed between LM iterations")}
+
+
+def trace_parity(tr_gpu, tr_orc):
+    """Largest relative differences of the per-sub-iteration records (chi2,
+    mu, rho) between a GPU trace and the oracle's, over the records both have
+    while the oracle's cost is still falling."""
+    n = min(len(tr_gpu), len(tr_orc))
+    out = {"records": 0, "chi2": 0.0, "mu": 0.0, "rho": 0.0}
+    for k in range(n):
+        a, b = tr_gpu[k], tr_orc[k]
+        if b[2] < 0 or a[2] < 0:
+            continue
+        if k > 0 and abs(tr_orc[k, 2] - tr_orc[k - 1, 2]) < 1e-9 * tr_orc[k, 2]:
+            break
+        out["records"] += 1
+        out["chi2"] = max(out["chi2"], abs(a[2] - b[2]) / abs(b[2]))
+        if b[3] != 0:
+            out["mu"] = max(out["mu"], abs(a[3] - b[3]) / abs(b[3]))
+        if k > 0:
+            out["rho"] = max(out["rho"], abs(a[4] - b[4]) / max(abs(b[4]), 1e-300))
+    return out
 
 
 def profiled_traffic():
@@ -196,14 +239,14 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / its,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded, config-2 shapes)",
-            "config": {"workload": f"config {args.config}: 1500 cams (9-param) / 500k pts / 3.5M obs, LM",
-                       "scale": args.scale},
+            "data": f"synthetic (seeded, config-{args.config} shapes; no public dataset)",
+            "config": workload_config(args.config, args.scale, prob, world),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": f"{its} LM iterations of config {args.config} in one oracle solve "
                                        f"(FP64 C++/OpenMP restatement; the reference itself cannot be built here)"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "final_chi2": float(tr[-1, 2]), "reason": reason}
+            "final_chi2": float(tr[-1, 2]), "reason": reason,
+            "trace": [[float(x) for x in r[:5]] for r in tr]}
     print(json.dumps(line), flush=True)
 
 
@@ -271,7 +314,8 @@ def main():
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--config", type=int, default=2)
     ap.add_argument("--scale", type=float, default=1.0)
-    ap.add_argument("--cpu-iters", type=int, default=1, help="LM iterations of the CPU baseline sample")
+    ap.add_argument("--cpu-iters", type=int, default=0,
+                    help="LM iterations of the CPU baseline sample (0: all K for configs 0 / 1, 2 for config 2)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -379,7 +423,8 @@ def main():
     envelope["final_chi2_equal_to_dense"] = envelope["mixed"]["final_chi2"] == chi2_m
 
     # ---- roofline of the dominant kernel: the trailing update of the factorisation ----
-    hbm, bf16, peak_src = measured_peaks()
+    peaks = measured_peaks()
+    hbm, bf16 = peaks["hbm"], peaks["bf16_sustained"]
     gm.set_params(prob.cams, prob.pts)
     gm.update(True)
     mu = 1e-3 * gm.max_abs_hdiag()
@@ -410,43 +455,51 @@ def main():
     tfl = pt["update_flop"] / upd_s / 1e12 if upd_s > 0 else None
     roofline = {"bound": "hbm", "kernel": "tc_syrk_kernel: Cholesky trailing update of S (tcgen05, split-BF16x3)",
                 "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": (ach / hbm) if ach else None,
-                "peak_source": f"{peak_src} HBM copy bandwidth",
+                "peak_source": f"{peaks['src']} HBM copy bandwidth",
                 "algorithmic_bytes_per_launch": alg_bytes / nlaunch, "launches_per_factorisation": nlaunch,
                 "traffic": traffic_launch,
                 "traffic_source": (traffic or {}).get("source"),
                 "tensor": {"achieved_tflops": tfl, "peak_tflops": bf16,
                            "frac": (tfl / bf16) if tfl else None,
+                           "peak_source": f"{peaks['src']} sustained dense BF16 (the kernel runs inside a long step)",
                            "note": "algorithmic FP32 flops; split-BF16x3 issues 3x as many MMA flops"},
                 "phases_ms": {k: round(v, 4) for k, v in pt.items()
                               if k.endswith("_ms") and k not in ("panel_ms", "wait_ms", "first_ms")},
                 "critical_path": chain}
 
     # ---- CPU baseline: the FP64 oracle on a bounded sample ----
+    # ... and its trace is the parity check of both GPU traces on this workload
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle.oracle import LMSettings as OLM
         from oracle.oracle import Oracle
         cores = len(os.sched_getaffinity(0))
         o = Oracle.from_ba(prob, threads=cores)
+        cpu_iters = args.cpu_iters if args.cpu_iters > 0 else {0: args.steps, 1: args.steps}.get(args.config, 2)
         t0 = time.perf_counter()
-        _, tro, its_o, _ = o.lm_solve(OLM(maxNumIt=args.cpu_iters))
+        _, tro, its_o, _ = o.lm_solve(OLM(maxNumIt=min(cpu_iters, args.steps)))
         dt = time.perf_counter() - t0
         cpu = {"value": max(its_o, 1) / dt, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"{max(its_o, 1)} LM iteration(s) of config {args.config} incl. the initial evaluation, "
                          f"FP64 C++/OpenMP oracle ({dt:.1f} s)"}
+        pm, pd = trace_parity(tr_m, tro), trace_parity(tr_d, tro)
+        parity = {"oracle_iterations": int(its_o), "records_compared": pd["records"],
+                  "fp64_gpu": {k: pd[k] for k in ("chi2", "mu", "rho")},
+                  "mixed": {k: pm[k] for k in ("chi2", "mu", "rho")},
+                  "bounds": {"fp64_chi2": 1e-9, "mixed_chi2": 1e-6},
+                  "ok": bool(pd["chi2"] <= 1e-9 and pm["chi2"] <= 1e-6 and pd["records"] > 0)}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_m / its_m, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32 (FP64 refinement residual, solve accumulators, cost)",
-                "data": "synthetic (seeded, config-2 shapes; no public dataset)",
-                "config": {"workload": f"config {args.config}: 1500 cams (9-param) / 500k pts / "
-                                       f"{prob.ne} obs, LevenbergMarquardt",
-                           "scale": args.scale, "parallelism": f"replicas x{world}",
-                           "l2": "inputs larger than L2 (S alone is 736 MB)"},
+                "data": f"synthetic (seeded, config-{args.config} shapes; no public dataset)",
+                "config": workload_config(args.config, args.scale, prob, world),
                 "fp64_gpu": {"value": fp64_value, "unit": UNIT, "ms_per_step": ms_d / its_d},
                 "speedup_vs_fp64_gpu": value / fp64_value,
                 "final_cost_rel_err_vs_fp64": final_rel, "per_iter_cost_rel_err_vs_fp64": iter_rel,
+                "oracle_parity": parity,
                 "final_chi2": chi2_m, "reason": r_m, "subiterations": sub_m,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "step": f"upload + nl_lm_solve({args.steps} its) + download"},

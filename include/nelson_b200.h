@@ -98,7 +98,7 @@ typedef struct {
  * (the phases of SolverCholeskySchurIterationTimeStat, nelson/SolverCholeskySchur.h:25-38). */
 typedef struct {
   float vinv_ms, wvinv_bs_ms, schur_ms, factor_ms, solve_ms, backsub_ms, total_ms;
-  float eval_ms;     /* last update(true) */
+  float eval_ms;     /* device time of the last nl_update(h, 1, ...) */
   float update_ms;   /* device time of the trailing updates inside factor_ms */
   int update_launches;
   double update_flop;  /* algorithmic flops of those updates (2 * multiply-adds) */
@@ -266,6 +266,21 @@ nl_status nl_set_timing_detail(nl_problem* h, int detail);
  * (nelson/SolverDiagonalBlocksInverseWWtMultSchur.hpp:36-140), without that
  * solver's AMD reordering (nelson/DoubleSection.hpp:30-63). */
 nl_status nl_set_solver_kind(nl_problem* h, int kind);
+/* Bound of the flag waits between the CTAs of the triangular solves: a CTA
+ * that has polled a tile's flag `polls` times without seeing it published
+ * records a timeout, returns, and the call reports NL_ERR_TIMEOUT (the wait
+ * ends instead of hanging the GPU).  polls <= 0 restores the default
+ * (2^24 polls, about a second).  (No counterpart in the reference: its solves
+ * run on the host.) */
+nl_status nl_set_wait_limit(nl_problem* h, long long polls);
+/* Check of that bound: runs the forward triangular solve of the handle's
+ * current factor with the flag of the first tile never published (its CTA is
+ * not launched), so every other CTA's first wait runs out.  Returns
+ * NL_ERR_TIMEOUT when the waits gave up as designed, NL_ERR_STATE when the
+ * reduced system has fewer than two 128-row tiles.  The handle stays usable:
+ * the next nl_compute_increment solves normally.  (No counterpart in the
+ * reference.) */
+nl_status nl_check_wait_timeout(nl_problem* h);
 /* Number of kernels of this library launched on the handle since creation. */
 nl_status nl_kernel_launches(nl_problem* h, long long* out);
 
@@ -323,7 +338,10 @@ nl_status nl_selftest_tc_update(int ntiles, unsigned long long seed, int device,
  * present on every GPU that loads it until the process exits.  At most
  * NL_NOALLOC_MAX_EDGES edges; larger ne is rejected with NL_ERR_ARG.  The
  * first call on a device looks up that array's address (with that device
- * current); make it before any stream capture.  All calls share the array:
+ * current); make it before any stream capture.  That address is kept for the
+ * life of the process: after cudaDeviceReset on a device, do not call this
+ * function on that device again (the kept address would be stale).  All calls
+ * share the array:
  * calls whose work overlaps on the GPU (other streams, other threads) race and
  * must be serialised by the caller. */
 #define NL_NOALLOC_MAX_EDGES 16777216

@@ -20,7 +20,7 @@
 namespace nl {
 
 constexpr int NB = 128;
-constexpr long long kSpinLimit = 1LL << 24;  // bounded waits (~1 s worst case)
+constexpr long long kSpinLimit = 1LL << 24;  // default bound of the flag waits (~1 s worst case)
 
 // Programmatic dependent launch of the critical-path chain (potrf -> row-tile
 // TRSM -> diagonal-tile update -> potrf ...): each kernel lets the next one in
@@ -650,10 +650,10 @@ __device__ inline int load_acquire(const int* p) {
   asm volatile("ld.acquire.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
-static __device__ inline bool wait_flag(const int* flag, int epoch, int* status) {
+static __device__ inline bool wait_flag(const int* flag, int epoch, int* status, long long limit) {
   long long it = 0;
   while (load_acquire(flag) != epoch) {
-    if (++it > kSpinLimit) {
+    if (++it > limit) {
       atomicOr(status, ST_SPIN_TIMEOUT);
       return false;
     }
@@ -669,6 +669,8 @@ __device__ inline void publish_tile(int* flag, int epoch, int tid) {
   __syncthreads();
   if (tid == 0) asm volatile("st.release.gpu.global.b32 [%0], %1;\n" ::"l"(flag), "r"(epoch) : "memory");
 }
+
+static __global__ void set_int_kernel(int* p, int v) { *p = v; }
 
 template <typename T>
 __device__ inline void load4(const T* p, double* v) {
@@ -700,6 +702,7 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
                                                              const double* __restrict__ b, double* __restrict__ y,
                                                              int* __restrict__ ticket, int* __restrict__ flags,
                                                              int epoch, int* __restrict__ status,
+                                                             long long spin_limit,
                                                              const int* __restrict__ env,
                                                              const int* __restrict__ active) {
   extern __shared__ float4 sLi4[];
@@ -723,7 +726,7 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
     double lv[8][4];  // the L tile does not depend on y_J: load it before waiting
 #pragma unroll
     for (int rr = 0; rr < 8; rr++) load4(Lrow + (size_t)rr * ld + (size_t)J * NB, lv[rr]);
-    if (tid == 0) ok_s = wait_flag(flags + J, epoch, status) ? 1 : 0;
+    if (tid == 0) ok_s = wait_flag(flags + J, epoch, status, spin_limit) ? 1 : 0;
     __syncthreads();
     if (!ok_s) return;
     double yv[4];
@@ -757,6 +760,7 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
                                                              const double* __restrict__ yv, double* __restrict__ x,
                                                              int* __restrict__ ticket, int* __restrict__ flags,
                                                              int epoch, int* __restrict__ status,
+                                                             long long spin_limit,
                                                              const int* __restrict__ env,
                                                              const int* __restrict__ active) {
   extern __shared__ float4 sLi4[];
@@ -781,7 +785,7 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
     double lv[8][4];  // loaded before waiting for x_J
 #pragma unroll
     for (int rr = 0; rr < 8; rr++) load4(Lb + (size_t)rr * ld, lv[rr]);
-    if (tid == 0) ok_s = wait_flag(flags + J, epoch, status) ? 1 : 0;
+    if (tid == 0) ok_s = wait_flag(flags + J, epoch, status, spin_limit) ? 1 : 0;
     __syncthreads();
     if (!ok_s) return;
 #pragma unroll

@@ -300,6 +300,7 @@ nl_status enqueue_eval_t(nl_problem* h, bool hessian, double* chi2_out, double* 
 }
 
 nl_status enqueue_eval(nl_problem* h, bool hessian, double* chi2_out, double* maxb_out, const int* active) {
+  NvtxRange rg(hessian ? "nl:update(true)" : "nl:update(false)");
   const bool f64 = h->desc.precision == NL_PREC_FP64;
   if (h->desc.bc == 9)
     return f64 ? enqueue_eval_t<double, 9>(h, hessian, chi2_out, maxb_out, active)
@@ -819,11 +820,13 @@ nl_status nl_get_edge_uids(nl_problem* h, int* h11, int* h12, int* h22) {
 nl_status nl_update(nl_problem* h, int hessian, double* chi2) {
   NL_CHECK_READY(h);
   NL_CUDA(cudaSetDevice(h->device));
-  NL_CUDA(cudaEventRecord(h->ev_a, h->st));
+  NL_CUDA(cudaEventRecord(h->ev_t0, h->st));
   nl_status s = enqueue_eval(h, hessian != 0, h->scal, h->scal + 1, nullptr);
   if (s != NL_OK) return s;
+  NL_CUDA(cudaEventRecord(h->ev_t1, h->st));
   double v;
   if ((s = sync_read(h, h->scal, &v, 1)) != NL_OK) return s;
+  if (hessian) NL_CUDA(cudaEventElapsedTime(&h->eval_ms, h->ev_t0, h->ev_t1));
   if (chi2) *chi2 = v;
   return NL_OK;
 }
@@ -1285,6 +1288,26 @@ nl_status nl_set_timing_detail(nl_problem* h, int detail) {
   NL_CHECK_H(h);
   h->timing_detail = detail ? 1 : 0;
   return NL_OK;
+}
+
+nl_status nl_set_wait_limit(nl_problem* h, long long polls) {
+  NL_CHECK_H(h);
+  if (!h->core) return NL_ERR_STATE;
+  h->core->wait_limit = polls > 0 ? polls : kSpinLimit;
+  return NL_OK;
+}
+
+nl_status nl_check_wait_timeout(nl_problem* h) {
+  NL_CHECK_READY(h);
+  NL_CUDA(cudaSetDevice(h->device));
+  NL_CUDA(cudaMemsetAsync(h->status, 0, sizeof(int), h->st));
+  nl_status s = h->core->enqueue_solve_withheld(h->status);
+  if (s != NL_OK) return s;
+  NL_CUDA(cudaMemcpyAsync(h->host_pin + 20, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  int st = 0;
+  memcpy(&st, h->host_pin + 20, sizeof(int));
+  return (st & ST_SPIN_TIMEOUT) ? NL_ERR_TIMEOUT : NL_OK;
 }
 
 nl_status nl_kernel_launches(nl_problem* h, long long* out) {

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include "../../include/nelson_b200.h"
@@ -20,6 +21,17 @@ struct Layout {
   static constexpr int W = pad16<T>(BC * 3);   // W / Y (= W V^-1) block, BC x 3
   static constexpr int U = pad16<T>(BC * BC);  // U block, BC x BC
   static constexpr int V = pad16<T>(9);        // V / V^-1 block, 3 x 3
+};
+
+// Host-side NVTX range over the enqueue of one phase (named like the phases
+// of SolverCholeskySchurIterationTimeStat, nelson/SolverCholeskySchur.h:25-38),
+// so a profiler timeline groups each phase's kernel launches.  Costs nothing
+// when no tool is attached.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
 };
 
 // Device-side error / status word bits (nl_status in the C ABI).

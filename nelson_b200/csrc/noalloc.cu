@@ -22,7 +22,11 @@
 // Device address of the array: the name `noalloc_partials` in host code is
 // only a host-side handle for the symbol.  The first call on each device looks
 // up the real address with cudaGetSymbolAddress, with that device current, and
-// caches it; that first call should come before any stream capture.
+// caches it; that first call should come before any stream capture.  The
+// cached address belongs to the device's primary context: a program that
+// calls cudaDeviceReset (or otherwise tears that context down) must not call
+// nl_ba_cost_noalloc on that device afterwards, since the cache would still
+// hold the old context's address.
 #include <cuda_runtime.h>
 
 #include <mutex>

@@ -244,11 +244,31 @@ class SchurCoreT final : public SchurCore {
     NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
     const int* env = envelope ? env_dev_.as<int>() : nullptr;
     trsv_fwd_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), b, y_.as<double>(),
-                                                 flags_.as<int>(), flags_.as<int>() + 1, 1, status, env, active);
+                                                 flags_.as<int>(), flags_.as<int>() + 1, 1, status, wait_limit, env,
+                                                 active);
     NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
     trsv_bwd_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), y_.as<double>(), x,
-                                                 flags_.as<int>(), flags_.as<int>() + 1, 1, status, env, active);
+                                                 flags_.as<int>(), flags_.as<int>() + 1, 1, status, wait_limit, env,
+                                                 active);
     launches += 2;
+    return NL_OK;
+  }
+
+  // The forward solve with tile 0 left out: the ticket counter starts at 1,
+  // so the ntiles - 1 CTAs take tiles 1 .. ntiles - 1 and each first waits
+  // for tile 0's flag, which nothing publishes.  Every CTA's wait runs out
+  // after wait_limit polls, records ST_SPIN_TIMEOUT and returns before it
+  // writes anything; no access leaves the buffers (tiles 1 .. ntiles - 1 of
+  // L and Linv).
+  nl_status enqueue_solve_withheld(int* status) override {
+    if (ntiles_ < 2) return NL_ERR_STATE;
+    NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
+    set_int_kernel<<<1, 1, 0, st_>>>(flags_.as<int>(), 1);
+    trsv_fwd_kernel<T><<<ntiles_ - 1, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), bS_.as<double>(),
+                                                     y_.as<double>(), flags_.as<int>(), flags_.as<int>() + 1, 1,
+                                                     status, wait_limit, nullptr, nullptr);
+    launches += 2;
+    NL_CUDA(cudaGetLastError());
     return NL_OK;
   }
 
@@ -605,13 +625,17 @@ class SchurCoreT final : public SchurCore {
 
   nl_status enqueue_increment(const double* lam, int* status, const int* active) override {
     const bool tm = timing && !active;
+    NvtxRange rg("nl:computeIncrement");
     if (tm) NL_CUDA(cudaEventRecord(ev_[0], st_));
+    nvtxRangePushA("nl:vinv+wvinv_bs");
     vinv_kernel<T, BC><<<cdiv(std::max(np_, 1), 128), 128, 0, st_>>>(d_, V_.as<T>(), Vinv_.as<T>(), lam, status, active);
     if (tm) NL_CUDA(cudaEventRecord(ev_[1], st_));
     if (nci_ > 0)
       wvinv_bs_kernel<T, BC, 128><<<nci_, 128, 0, st_>>>(d_, W_.as<T>(), Vinv_.as<T>(), Y_.as<T>(), bU_.as<T>(),
                                                          bV_.as<T>(), bS_.as<double>(), active);
     if (tm) NL_CUDA(cudaEventRecord(ev_[2], st_));
+    nvtxRangePop();
+    nvtxRangePushA("nl:schur");
     NL_CUDA(cudaMemsetAsync(S_.p, 0, S_.bytes, st_));
     if (need_s0_) NL_CUDA(cudaMemsetAsync(S0_.p, 0, S0_.bytes, st_));
     {
@@ -625,10 +649,16 @@ class SchurCoreT final : public SchurCore {
                                                                      ld_, active);
     }
     launches += 4;
+    nvtxRangePop();
     if (tm) NL_CUDA(cudaEventRecord(ev_[3], st_));
-    nl_status s = enqueue_factor(status, active);
+    nl_status s;
+    {
+      NvtxRange r("nl:factorize");
+      s = enqueue_factor(status, active);
+    }
     if (s != NL_OK) return s;
     if (tm) NL_CUDA(cudaEventRecord(ev_[4], st_));
+    NvtxRange rs("nl:solve+backsub");
     if ((s = enqueue_solve(bS_.as<double>(), incU, status, active)) != NL_OK) return s;
     for (int it = 0; it < refine_sweeps && need_s0_; it++) {
       symv_partial_kernel<T, kSymvChunks><<<dim3(ntiles_, kSymvChunks), SV, 0, st_>>>(

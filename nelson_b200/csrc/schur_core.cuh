@@ -83,6 +83,9 @@ class SchurCore {
   // current bU / bV (same V^-1, W V^-1 and factor of S): incU / incV get
   // -(J'WJ + damping)^-1 b.
   virtual nl_status enqueue_resolve(int* status) = 0;
+  // Test of the bounded waits: a forward solve in which one tile's flag is
+  // never published, so every wait runs out after wait_limit polls.
+  virtual nl_status enqueue_solve_withheld(int* status) = 0;
   virtual nl_status enqueue_hdiag(double* out) = 0;
   virtual nl_status enqueue_maxabs_b(double* out, const int* active) = 0;
   virtual nl_status enqueue_inc_dot(const LmDev* s, double* part, int* nparts) = 0;
@@ -107,6 +110,7 @@ class SchurCore {
   long long launches = 0;
   int timing = 0;          // record per-phase CUDA events
   int envelope = 0;        // envelope solver: skip the tiles of S outside the Cholesky envelope
+  long long wait_limit = kSpinLimit;  // polls before a flag wait of the solves gives up
   int timing_detail = 0;   // with timing: also per-panel events on the factorisation's critical path
                            // (costly on the host: one record per kernel boundary, and no early launch)
 };

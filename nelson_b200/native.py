@@ -89,6 +89,7 @@ EXPORTS = [
     "nl_kernel_launches", "nl_solver_create", "nl_solver_destroy", "nl_solver_set_hessian",
     "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_selftest_tc_update", "nl_ba_cost_noalloc",
     "nl_adjoint", "nl_lm_solve_batch", "nl_set_timing_detail", "nl_set_solver_kind", "nl_solver_set_kind", "nl_permute_rcm_u", "nl_get_user2internal_u", "nl_rcm_order",
+    "nl_set_wait_limit", "nl_check_wait_timeout",
     "nl_status_string",
     "nl_version",
 ]
@@ -125,6 +126,8 @@ def load(build_if_missing: bool = True):
     L.nl_lm_solve_batch.argtypes = [C.POINTER(vp), i, C.POINTER(LMSettings), vp, vp]
     L.nl_adjoint.argtypes = [vp, vp, vp, i, vp, vp, vp, vp, C.POINTER(AdjointReport)]
     L.nl_ba_cost_noalloc.argtypes = [i, i, vp, vp, vp, vp, vp, vp, d, d, d, vp, vp]
+    L.nl_set_wait_limit.argtypes = [vp, C.c_longlong]
+    L.nl_check_wait_timeout.argtypes = [vp]
     for name in EXPORTS:  # fails loudly if the library lacks an entry point
         if name not in ("nl_status_string", "nl_version"):
             getattr(L, name).restype = C.c_int
@@ -348,6 +351,17 @@ class BAProblemGPU:
         """Time every critical-path step of the factorisation in the next
         compute_increment calls (slower: see nl_set_timing_detail)."""
         self._c(self.L.nl_set_timing_detail(self.h, C.c_int(1 if detail else 0)), "nl_set_timing_detail")
+
+    def set_wait_limit(self, polls: int):
+        """Bound of the triangular solves' flag waits, in polls (<= 0: the
+        default); nl_set_wait_limit."""
+        self._c(self.L.nl_set_wait_limit(self.h, C.c_longlong(int(polls))), "nl_set_wait_limit")
+
+    def check_wait_timeout(self) -> int:
+        """nl_check_wait_timeout: the forward solve with one tile's flag
+        withheld; returns the status code (7 = NL_ERR_TIMEOUT when every wait
+        gave up as designed)."""
+        return int(self.L.nl_check_wait_timeout(self.h))
 
     def kernel_launches(self):
         v = C.c_longlong()

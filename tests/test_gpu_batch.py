@@ -37,14 +37,23 @@ def test_batch_equals_single(prec):
         g.close()
 
 
-def test_batch_matches_oracle(oracle_lib):
-    probs = make_batch(6)
-    hs = [N.BAProblemGPU.from_ba(p, precision=N.PREC_FP64) for p in probs]
+@pytest.mark.parametrize("prec,tol", [(N.PREC_FP64, 1e-9), (N.PREC_MIXED, 1e-6)])
+def test_batch_matches_oracle(oracle_lib, prec, tol):
+    """Every problem of a 24-problem batch against the oracle's LM on the same
+    problem: final cost (1e-9 FP64, 1e-6 mixed), iteration count and
+    termination reason, and the points."""
+    probs = make_batch(24)
+    hs = [N.BAProblemGPU.from_ba(p, precision=prec) for p in probs]
     reasons, chi2, its, lat = N.lm_solve_batch(hs, N.LMSettings(maxNumIt=6))
     for k, p in enumerate(probs):
         o = oracle_lib.Oracle.from_ba(p)
-        o.lm_solve(oracle_lib.LMSettings(maxNumIt=6))
-        assert chi2[k] == pytest.approx(o.chi2(), rel=1e-9)
+        r_o, _, it_o, _ = o.lm_solve(oracle_lib.LMSettings(maxNumIt=6))
+        assert chi2[k] == pytest.approx(o.chi2(), rel=tol), k
+        assert reasons[k] == r_o and its[k] == it_o, k
+        pts_o = o.get_params()[1]
+        # gauge-free problems: the points agree to the cost's precision
+        assert np.abs(hs[k].get_params()[1] - pts_o).max() <= (1e-6 if prec == N.PREC_FP64 else 1e-3) * \
+            np.abs(pts_o).max(), k
     for g in hs:
         g.close()
 

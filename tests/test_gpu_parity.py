@@ -155,3 +155,35 @@ def test_increment_multi_tile(Orc, cfg, scale, prec):
         itol = 1e-10 if prec == N.PREC_FP64 else (MIXED_INC_TOL if mu_rel >= 1e-3 else 1e-3)
         assert rel(du_g, du_o) < itol and rel(dv_g, dv_o) < itol, (mu_rel, rel(du_g, du_o), rel(dv_g, dv_o))
     g.close()
+
+
+@pytest.mark.parametrize("prec", [N.PREC_FP64, N.PREC_MIXED])
+def test_config1_full_size(Orc, prec):
+    """Config 1 at its stated size (200 9-parameter cameras, 50,000 points,
+    375 k observations, S 1,800 x 1,800): structure and edge UIDs bit-exact,
+    then 20 LM iterations with the per-sub-iteration cost within 1e-9 (FP64)
+    / 1e-6 (mixed) of the oracle's and the same damping sequence."""
+    p = make_config(1, 1.0)
+    assert (p.nc_var, p.bc, p.np_var) == (200, 9, 50000)
+    o = Orc.Oracle.from_ba(p)
+    g = N.BAProblemGPU.from_ba(p, precision=prec)
+    assert (o.nU, o.nV, o.nW, o.ne) == (g.nU, g.nV, g.nW, g.ne)
+    for a, b in zip(o.patterns(), g.patterns()):
+        assert np.array_equal(a, b)
+    for a, b in zip(o.edge_uids(), g.edge_uids()):
+        assert np.array_equal(a, b)
+    r_o, tr_o, it_o, _ = o.lm_solve(Orc.LMSettings(maxNumIt=20))
+    r_g, tr_g, it_g, _ = g.lm_solve(N.LMSettings(maxNumIt=20))
+    n = min(len(tr_o), len(tr_g))
+    compared = 0
+    for k in range(n):
+        if tr_o[k, 2] < 0 or tr_g[k, 2] < 0:
+            continue
+        if k > 0 and abs(tr_o[k, 2] - tr_o[k - 1, 2]) < 1e-9 * tr_o[k, 2]:
+            break
+        assert abs(tr_o[k, 2] - tr_g[k, 2]) <= LM_TOL[prec] * tr_o[k, 2], (k, tr_o[k], tr_g[k])
+        assert tr_g[k, 3] == pytest.approx(tr_o[k, 3], rel=1e-6), k
+        compared += 1
+    assert compared >= 5
+    assert abs(g.chi2() - o.chi2()) <= LM_TOL[prec] * o.chi2()
+    g.close()

@@ -11,11 +11,23 @@
 //   GaussNewton<Solver> (GaussNewton.h/.hpp)        GaussNewton<Solver>
 //   LevenbergMarquardtSettings / GaussNewtonSettings  same names and defaults
 //
-// LevenbergMarquardt::solve / GaussNewton::solve below restate the
-// reference's control flow (nelson/LevenbergMarquardt.hpp:36-146,
-// nelson/GaussNewton.hpp:32-127) over the problem and solver concepts, one
-// C-ABI call per step; solveOnDevice() runs the same loop entirely on the GPU
-// (nl_lm_solve / nl_gn_solve) and is what a production caller uses.
+// The solvers meet the reference's Solver concept (nelson/SolverCholeskySchur.h:
+// 71-115: Type, hasSettings, Settings, init(H, b), maxAbsHDiag(),
+// computeIncrement(H, b, relLambda, absLambda), incrementVector(),
+// incrementVectorSquaredNorm()) and BASection meets the problem concept
+// LevenbergMarquardt / GaussNewton use (update(bool), hessian().H() / b() /
+// chi2() / maxAbsValBVect(), oplus(inc), backupSolution(), rollbackSolution(),
+// computeRhoChi2Change(mu, inc, oldChi2)), so the reference's own
+// LevenbergMarquardt<Solver>::solve(op) instantiates with them unchanged.
+// The H and b a BASection hands out are handles of its device-resident
+// Hessian (DeviceHessianMatrices / DeviceHessianVectors); a Hessian assembled
+// on the host goes through SolverCholeskySchurCudaHost instead.
+//
+// LevenbergMarquardt::solve / GaussNewton::solve below are written against
+// exactly those calls, in the reference's order (nelson/LevenbergMarquardt.hpp:
+// 36-146, nelson/GaussNewton.hpp:32-127); solveOnDevice() runs the same loop
+// entirely on the GPU (nl_lm_solve / nl_gn_solve) and is what a production
+// caller uses.
 //
 // Errors: every failing C-ABI call throws nelson_b200::Error carrying the
 // nl_status.  A Cholesky failure of the reduced system is not an error: it is
@@ -114,6 +126,30 @@ struct IterationRecord {
 };
 
 // ---------------------------------------------------------------------------
+// The Hessian blocks [U W; W' V], the gradient b and the increment of a
+// BASection live on the device.  These handles stand where the reference
+// passes DoubleSectionHessianMatrices and DoubleSectionHessianVectors
+// (nelson/DoubleSectionHessian.h:37-141): a solver or a problem that receives
+// one works on the device data of the handle's section.
+struct DeviceHessianMatrices {
+  nl_problem* h = nullptr;
+};
+struct DeviceHessianVectors {
+  enum class Kind { Gradient, Increment };
+  nl_problem* h = nullptr;
+  Kind kind = Kind::Gradient;
+  // Host copies, bU in internal camera order (the reference's bU() / bV()).
+  void get(std::vector<double>& bU, std::vector<double>& bV, int numU, int numV, int bc) const {
+    bU.resize(size_t(numU) * bc);
+    bV.resize(size_t(numV) * 3);
+    if (kind == Kind::Increment)
+      check(nl_get_increment(h, bU.data(), bV.data()), "nl_get_increment");
+    else
+      check(nl_get_hessian(h, nullptr, nullptr, nullptr, bU.data(), bV.data()), "nl_get_hessian");
+  }
+};
+
+// ---------------------------------------------------------------------------
 // BASection: a DoubleSection of cameras (U, 6 or 9 parameters) and points
 // (V, 3 parameters) joined by the projection EdgeBinaryUV, resident on one
 // GPU.  Call order as in the reference: construct (parametersReady), addEdge
@@ -137,13 +173,14 @@ class BASection {
     d.device = device;
     check(nl_create(&d, &h_), "nl_create");
     desc_ = d;
+    hessian_ = Hessian(h_);
   }
   ~BASection() {
     if (h_) nl_destroy(h_);
   }
   BASection(const BASection&) = delete;
   BASection& operator=(const BASection&) = delete;
-  BASection(BASection&& o) noexcept : h_(std::exchange(o.h_, nullptr)), desc_(o.desc_) {}
+  BASection(BASection&& o) noexcept : h_(std::exchange(o.h_, nullptr)), desc_(o.desc_), hessian_(h_) {}
 
   nl_problem* handle() const { return h_; }
   int cameraBlockSize() const { return desc_.bc; }
@@ -210,32 +247,46 @@ class BASection {
     double c;
     check(nl_update(h_, computeHessian ? 1 : 0, &c), "nl_update");
   }
-  // hessian().chi2() / hessian().maxAbsValBVect() (nelson/HessianBase.h).
-  class HessianView {
+  // DoubleSection::hessian() (nelson/DoubleSection.h:265-272): H(), b(),
+  // chi2(), maxAbsValBVect() of the section's device-resident Hessian.
+  class Hessian {
    public:
-    explicit HessianView(nl_problem* h) : h_(h) {}
+    explicit Hessian(nl_problem* h = nullptr) : H_{h}, b_{h, DeviceHessianVectors::Kind::Gradient} {}
+    DeviceHessianMatrices& H() { return H_; }
+    const DeviceHessianMatrices& H() const { return H_; }
+    const DeviceHessianVectors& b() const { return b_; }
     double chi2() const {
       double c;
-      check(nl_chi2(h_, &c), "nl_chi2");
+      check(nl_chi2(H_.h, &c), "nl_chi2");
       return c;
     }
     double maxAbsValBVect() const {
       double b;
-      check(nl_max_abs_b(h_, &b), "nl_max_abs_b");
+      check(nl_max_abs_b(H_.h, &b), "nl_max_abs_b");
       return b;
     }
 
    private:
-    nl_problem* h_;
+    DeviceHessianMatrices H_;
+    DeviceHessianVectors b_;
   };
-  HessianView hessian() const { return HessianView(h_); }
-  // oplus with the solver's increment vector (the increment stays on the device).
-  void oplus() { check(nl_oplus(h_), "nl_oplus"); }
+  Hessian& hessian() { return hessian_; }
+  const Hessian& hessian() const { return hessian_; }
+
+  // oplus(inc) with the increment a solver computed on this section (the
+  // increment stays on the device).
+  void oplus(const DeviceHessianVectors& inc) {
+    if (inc.h != h_ || inc.kind != DeviceHessianVectors::Kind::Increment)
+      throw Error(NL_ERR_ARG, "oplus: not this section's increment");
+    check(nl_oplus(h_), "nl_oplus");
+  }
   void backupSolution() { check(nl_backup(h_), "nl_backup"); }
   void rollbackSolution() { check(nl_rollback(h_), "nl_rollback"); }
-  // computeRhoChi2Change (nelson/DoubleSection.hpp:469-480), on the current
-  // increment: (oldChi2 - chi2) / (inc' (mu inc - b)).
-  double computeRhoChi2Change(double mu, double oldChi2) const {
+  // DoubleSection::computeRhoChi2Change (nelson/DoubleSection.h:300-311):
+  // (oldChi2 - chi2) / (inc' (mu inc - b)).
+  double computeRhoChi2Change(double mu, const DeviceHessianVectors& inc, double oldChi2) const {
+    if (inc.h != h_ || inc.kind != DeviceHessianVectors::Kind::Increment)
+      throw Error(NL_ERR_ARG, "computeRhoChi2Change: not this section's increment");
     double r;
     check(nl_rho(h_, mu, oldChi2, &r), "nl_rho");
     return r;
@@ -244,54 +295,72 @@ class BASection {
  private:
   nl_problem* h_ = nullptr;
   nl_problem_desc desc_{};
+  Hessian hessian_;
   std::vector<int> cam_, camFixed_, pt_, ptFixed_;
   bool rcm_ = false;
   std::vector<double> obs_, w_;
 };
 
 // ---------------------------------------------------------------------------
-// The Solver concept (nelson/SolverCholeskySchur.h:96-115) on a BASection's
-// device-resident Hessian.
+// SolverCholeskySchur's Solver concept (nelson/SolverCholeskySchur.h:71-115)
+// on a BASection's device-resident Hessian: init(H, b) binds the section the
+// handles name, computeIncrement(H, b, rel, abs) runs the whole Schur
+// increment on the device, incrementVector() is the handle of the device
+// increment that the section's oplus / computeRhoChi2Change accept.
 class SolverCholeskySchurCuda {
  public:
-  void init(BASection& p) {
-    p_ = &p;
-    check(nl_solver_init(p.handle()), "nl_solver_init");
-    select(p);
+  using Type = double;
+  static constexpr bool hasSettings = false;
+  class Settings {};
+
+  // SolverCholeskySchur::init (nelson/SolverCholeskySchur.hpp:44-62).
+  void init(DeviceHessianMatrices& H, const DeviceHessianVectors& b) {
+    if (!H.h || b.h != H.h) throw Error(NL_ERR_ARG, "init: H and b of different sections");
+    h_ = H.h;
+    inc_ = DeviceHessianVectors{h_, DeviceHessianVectors::Kind::Increment};
+    check(nl_solver_init(h_), "nl_solver_init");
+    check(nl_set_solver_kind(h_, kind()), "nl_set_solver_kind");
   }
-  // the factorisation this solver stands for, on p's handle
-  void select(BASection& p) { check(nl_set_solver_kind(p.handle(), NL_SOLVER_DENSE), "nl_set_solver_kind"); }
+  // SolverCholeskySchur::maxAbsHDiag (nelson/SolverCholeskySchur.hpp:75-78).
   double maxAbsHDiag() const {
     double m;
-    check(nl_max_abs_hdiag(p_->handle(), &m), "nl_max_abs_hdiag");
+    check(nl_max_abs_hdiag(h_, &m), "nl_max_abs_hdiag");
     return m;
   }
   // computeIncrement(H, b, relLambda, absLambda) (SolverCholeskySchur.hpp:91-157):
   // false when a damped block or the reduced system is not positive definite
   // (the increment is then zero).
-  bool computeIncrement(double relLambda, double absLambda) {
+  bool computeIncrement(DeviceHessianMatrices& H, const DeviceHessianVectors& b, double relLambda,
+                        double absLambda) {
+    if (H.h != h_ || b.h != h_) throw Error(NL_ERR_STATE, "computeIncrement: solver initialised on another section");
     int ok = 0;
-    check(nl_compute_increment(p_->handle(), relLambda, absLambda, &ok), "nl_compute_increment");
+    check(nl_compute_increment(h_, relLambda, absLambda, &ok), "nl_compute_increment");
     return ok != 0;
   }
+  const DeviceHessianVectors& incrementVector() const { return inc_; }
   double incrementVectorSquaredNorm() const {
     double s;
-    check(nl_inc_sqnorm(p_->handle(), &s), "nl_inc_sqnorm");
+    check(nl_inc_sqnorm(h_, &s), "nl_inc_sqnorm");
     return s;
   }
-  void incrementVector(std::vector<double>& incU, std::vector<double>& incV) const {
-    incU.resize(size_t(p_->numParametersU()) * p_->cameraBlockSize());
-    incV.resize(size_t(p_->numParametersV()) * 3);
-    check(nl_get_increment(p_->handle(), incU.data(), incV.data()), "nl_get_increment");
-  }
-  nl_phase_times timeStats() const {
+  // The phases of SolverCholeskySchurTimeStat (nelson/SolverCholeskySchur.h:25-38).
+  nl_phase_times timingStats() const {
     nl_phase_times t{};
-    check(nl_phase_timings(p_->handle(), &t), "nl_phase_timings");
+    check(nl_phase_timings(h_, &t), "nl_phase_timings");
     return t;
   }
+  // the factorisation this solver stands for, on p's handle (solveOnDevice)
+  void select(BASection& p) const { check(nl_set_solver_kind(p.handle(), kind()), "nl_set_solver_kind"); }
+
+ protected:
+  virtual int kind() const { return NL_SOLVER_DENSE; }
 
  private:
-  BASection* p_ = nullptr;
+  nl_problem* h_ = nullptr;
+  DeviceHessianVectors inc_;
+
+ public:
+  virtual ~SolverCholeskySchurCuda() = default;
 };
 
 // The solver that takes SolverDiagonalBlocksInverseWWtMultSchur's place in
@@ -299,12 +368,161 @@ class SolverCholeskySchurCuda {
 // the same Schur complement, factored over its Cholesky envelope only
 // (NL_SOLVER_ENVELOPE); its increments are SolverCholeskySchurCuda's.
 class SolverEnvelopeSchurCuda : public SolverCholeskySchurCuda {
+ protected:
+  int kind() const override { return NL_SOLVER_ENVELOPE; }
+};
+
+// ---------------------------------------------------------------------------
+// SolverCholeskySchur on a Hessian assembled on the host (any edge types the
+// device does not evaluate): the Solver concept over the caller's own
+// Hessian matrices / vectors types, read and written through an access
+// traits class.  HostHessianAccess<Matrices, Vectors> provides
+//   static int bu(const Matrices&)                      U block size
+//   static int numU(const Matrices&), numV(const Matrices&)   parameter blocks
+//   static void patterns(const Matrices&, std::vector<int>& u_rc,
+//                        std::vector<int>& v_rc, std::vector<int>& w_rc)
+//       (row, col) per block UID in the reference's storage order: U upper
+//       CSC, V diagonal, W CSR (nelson/DoubleSection.hpp:157-191)
+//   static void values(const Matrices&, std::vector<double>& U,
+//                      std::vector<double>& V, std::vector<double>& W)
+//       the blocks in UID order, each row-major
+//   static void gradient(const Vectors&, std::vector<double>& bU, std::vector<double>& bV)
+//   static void setIncrement(Vectors& inc, const Vectors& like, const std::vector<double>& incU,
+//                            const std::vector<double>& incV)
+// The reference's mat-based DoubleSectionHessianMatrices is read with its own
+// block iterators (outerSize / begin(col) / row / col / block / blockUID) in a
+// specialisation the integrating program writes; HostBlockHessian below is a
+// self-contained stand-in that has one.
+template <class Matrices, class Vectors>
+struct HostHessianAccess;
+
+template <class Matrices, class Vectors, class Access = HostHessianAccess<Matrices, Vectors>>
+class SolverCholeskySchurCudaHost {
  public:
-  void init(BASection& p) {
-    SolverCholeskySchurCuda::init(p);
-    select(p);
+  using Type = double;
+  static constexpr bool hasSettings = true;
+  struct Settings {
+    int precision = NL_PREC_FP64;
+    int refineSweeps = -1;
+    int device = 0;
+    int kind = NL_SOLVER_DENSE;
+  };
+  Settings& settings() { return settings_; }
+
+  SolverCholeskySchurCudaHost() = default;
+  SolverCholeskySchurCudaHost(const SolverCholeskySchurCudaHost&) = delete;
+  SolverCholeskySchurCudaHost& operator=(const SolverCholeskySchurCudaHost&) = delete;
+  ~SolverCholeskySchurCudaHost() {
+    if (s_) nl_solver_destroy(s_);
   }
-  void select(BASection& p) { check(nl_set_solver_kind(p.handle(), NL_SOLVER_ENVELOPE), "nl_set_solver_kind"); }
+
+  // init(H, b): the block pattern is fixed here (nelson/SolverCholeskySchur.hpp:44-62).
+  void init(Matrices& H, const Vectors& b) {
+    if (s_) nl_solver_destroy(s_);
+    s_ = nullptr;
+    std::vector<int> u_rc, v_rc, w_rc;
+    Access::patterns(H, u_rc, v_rc, w_rc);
+    nl_solver_desc d{};
+    d.bu = Access::bu(H);
+    d.nu = Access::numU(H);
+    d.nv = Access::numV(H);
+    d.nU = int(u_rc.size() / 2);
+    d.nV = int(v_rc.size() / 2);
+    d.nW = int(w_rc.size() / 2);
+    d.precision = settings_.precision;
+    d.refine_sweeps = settings_.refineSweeps;
+    d.device = settings_.device;
+    check(nl_solver_create(&d, u_rc.data(), v_rc.data(), w_rc.data(), &s_), "nl_solver_create");
+    check(nl_solver_set_kind(s_, settings_.kind), "nl_solver_set_kind");
+    bu_ = d.bu;
+    nu_ = d.nu;
+    nv_ = d.nv;
+    upload(H, b);
+    incU_.assign(size_t(nu_) * bu_, 0.0);
+    incV_.assign(size_t(nv_) * 3, 0.0);
+    Access::setIncrement(inc_, b, incU_, incV_);
+  }
+  double maxAbsHDiag() const {
+    double m;
+    check(nl_solver_max_abs_hdiag(s_, &m), "nl_solver_max_abs_hdiag");
+    return m;
+  }
+  bool computeIncrement(Matrices& H, const Vectors& b, double relLambda, double absLambda) {
+    upload(H, b);
+    int ok = 0;
+    check(nl_solver_compute_increment(s_, relLambda, absLambda, incU_.data(), incV_.data(), &ok),
+          "nl_solver_compute_increment");
+    Access::setIncrement(inc_, b, incU_, incV_);
+    return ok != 0;
+  }
+  const Vectors& incrementVector() const { return inc_; }
+  double incrementVectorSquaredNorm() const {
+    double s = 0;
+    for (double x : incU_) s += x * x;
+    for (double x : incV_) s += x * x;
+    return s;
+  }
+
+ private:
+  void upload(const Matrices& H, const Vectors& b) {
+    Access::values(H, U_, V_, W_);
+    Access::gradient(b, bU_, bV_);
+    check(nl_solver_set_hessian(s_, U_.data(), V_.data(), W_.data(), bU_.data(), bV_.data()),
+          "nl_solver_set_hessian");
+  }
+  Settings settings_;
+  nl_solver* s_ = nullptr;
+  int bu_ = 0, nu_ = 0, nv_ = 0;
+  std::vector<double> U_, V_, W_, bU_, bV_, incU_, incV_;
+  Vectors inc_{};
+};
+
+// A self-contained host block Hessian in the reference's storage order, with
+// its HostHessianAccess: U (bu x bu blocks, upper CSC), V (3 x 3 diagonal
+// blocks), W (bu x 3, CSR), each block row-major, and the vectors bU (internal
+// camera order) / bV.
+struct HostBlockHessian {
+  int bu = 0, numU = 0, numV = 0;
+  std::vector<int> u_rc, v_rc, w_rc;  // (row, col) per UID
+  std::vector<double> U, V, W;        // blocks in UID order
+  void setZero() {
+    std::fill(U.begin(), U.end(), 0.0);
+    std::fill(V.begin(), V.end(), 0.0);
+    std::fill(W.begin(), W.end(), 0.0);
+  }
+};
+struct HostBlockVectors {
+  std::vector<double> bU, bV;
+  void setZero() {
+    std::fill(bU.begin(), bU.end(), 0.0);
+    std::fill(bV.begin(), bV.end(), 0.0);
+  }
+};
+template <>
+struct HostHessianAccess<HostBlockHessian, HostBlockVectors> {
+  static int bu(const HostBlockHessian& H) { return H.bu; }
+  static int numU(const HostBlockHessian& H) { return H.numU; }
+  static int numV(const HostBlockHessian& H) { return H.numV; }
+  static void patterns(const HostBlockHessian& H, std::vector<int>& u, std::vector<int>& v, std::vector<int>& w) {
+    u = H.u_rc;
+    v = H.v_rc;
+    w = H.w_rc;
+  }
+  static void values(const HostBlockHessian& H, std::vector<double>& U, std::vector<double>& V,
+                     std::vector<double>& W) {
+    U = H.U;
+    V = H.V;
+    W = H.W;
+  }
+  static void gradient(const HostBlockVectors& b, std::vector<double>& bU, std::vector<double>& bV) {
+    bU = b.bU;
+    bV = b.bV;
+  }
+  static void setIncrement(HostBlockVectors& inc, const HostBlockVectors&, const std::vector<double>& incU,
+                           const std::vector<double>& incV) {
+    inc.bU = incU;
+    inc.bV = incV;
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -317,59 +535,65 @@ class LevenbergMarquardt {
   int numIterations() const { return iter_; }
   Solver& solver() { return solver_; }
 
-  // nelson/LevenbergMarquardt.hpp:36-146, one C-ABI call per step.
-  TerminationReason solve(BASection& P) {
+  // nelson/LevenbergMarquardt.hpp:36-146: the reference's calls on the
+  // problem and solver concepts, in its order (one C-ABI call per step for a
+  // BASection).  Records one IterationRecord per sub-iteration.
+  template <class OptimizationProblem>
+  TerminationReason solve(OptimizationProblem& op) {
     const auto& s = settings_;
+    using T = typename Solver::Type;
     stats_.clear();
     iter_ = -1;
-    solver_.init(P);
-    P.update(true);
-    push(-1, -1, P.hessian().chi2(), 0, 0, 0, true, true);
-    if (P.hessian().maxAbsValBVect() <= s.epsBVector) return TerminationReason::SuccessAtStart;
-    P.backupSolution();
-    double oldChi2 = P.hessian().chi2();
-    double mu = s.tau * solver_.maxAbsHDiag();
-    double v = s.initV;
+    op.update(true);
+    push(-1, -1, op.hessian().chi2(), 0, 0, 0, true, true);
+    if (op.hessian().maxAbsValBVect() <= s.epsBVector) return TerminationReason::SuccessAtStart;
+    op.backupSolution();
+    T oldChi2 = op.hessian().chi2();
+    solver_.init(op.hessian().H(), op.hessian().b());
+    T mu = s.tau * solver_.maxAbsHDiag();
+    T curV = s.initV;
     iter_ = 0;
     while (iter_ < s.maxNumIt) {
       int subiter = 0;
-      bool repeat;
+      bool toRepeat = false;
       do {
-        const double muUsed = mu;
-        const bool ok = solver_.computeIncrement(0.0, mu);
-        const double inc = solver_.incrementVectorSquaredNorm();
-        if (ok && iter_ >= s.minNumIt && inc <= s.epsIncSquare) {
-          push(iter_, subiter, P.hessian().chi2(), muUsed, 0, inc, true, false);
+        const T muUsed = mu;
+        const bool solveOk = solver_.computeIncrement(op.hessian().H(), op.hessian().b(), 0, mu);
+        const T inc = solver_.incrementVectorSquaredNorm();
+        if (solveOk && iter_ >= s.minNumIt && inc <= s.epsIncSquare) {
+          push(iter_, subiter, op.hessian().chi2(), muUsed, 0, inc, true, false);
           return TerminationReason::SuccessSmallIncrement;
         }
-        double rho = -1, chi2 = -1;
-        if (ok) {
-          P.oplus();
-          P.update(false);
-          chi2 = P.hessian().chi2();
-          rho = P.computeRhoChi2Change(mu, oldChi2);
+        T rho = -1, chi2 = -1;
+        if (solveOk) {
+          op.oplus(solver_.incrementVector());
+          op.update(false);
+          chi2 = op.hessian().chi2();
+          rho = op.computeRhoChi2Change(mu, solver_.incrementVector(), oldChi2);
         }
-        const bool accepted = ok && rho > 0;
-        push(iter_, subiter, chi2, muUsed, rho, inc, ok, accepted);
+        const bool accepted = solveOk && rho > 0;
+        push(iter_, subiter, chi2, muUsed, rho, inc, solveOk, accepted);
         if (accepted) {
-          if (iter_ > s.minNumIt && P.hessian().maxAbsValBVect() <= s.epsBVector)
+          if (iter_ > s.minNumIt && op.hessian().maxAbsValBVect() <= s.epsBVector)
             return TerminationReason::SuccessEpsB;
-          if (iter_ > s.minNumIt && chi2 < s.epsChi2) return TerminationReason::SuccessSmallResiduals;
-          const double fc = 2 * rho - 1;
-          mu *= std::max(s.minScaleFactor, std::min(s.maxScaleFactor, 1 - fc * fc * fc));
-          v = s.initV;
+          if (iter_ > s.minNumIt && op.hessian().chi2() < s.epsChi2) return TerminationReason::SuccessSmallResiduals;
+          const T fc = 2 * rho - 1;
+          T alpha = std::min(T(s.maxScaleFactor), 1 - fc * fc * fc);
+          alpha = std::max(T(s.minScaleFactor), alpha);
+          mu = mu * alpha;
+          curV = s.initV;
         } else {
-          P.rollbackSolution();
-          mu *= v;
-          v *= s.penaltyV;
+          op.rollbackSolution();
+          mu = mu * curV;
+          curV = curV * s.penaltyV;
         }
         ++subiter;
         if (subiter >= s.maxNumSubIt) return TerminationReason::MaxSubIterationReached;
-        repeat = !accepted;
-      } while (repeat);
-      P.update(true);
-      P.backupSolution();
-      oldChi2 = P.hessian().chi2();
+        toRepeat = !accepted;
+      } while (toRepeat);
+      op.update(true);
+      op.backupSolution();
+      oldChi2 = op.hessian().chi2();
       ++iter_;
     }
     return TerminationReason::MaxIterationReached;
@@ -411,35 +635,36 @@ class GaussNewton {
   GaussNewtonSettings& settings() { return settings_; }
   const std::vector<IterationRecord>& stats() const { return stats_; }
   int numIterations() const { return iter_; }
+  Solver& solver() { return solver_; }
 
-  // nelson/GaussNewton.hpp:32-127.
-  TerminationReason solve(BASection& P) {
+  // nelson/GaussNewton.hpp:32-127: the reference's calls, in its order.
+  template <class OptimizationProblem>
+  TerminationReason solve(OptimizationProblem& op) {
     const auto& s = settings_;
     stats_.clear();
     iter_ = -1;
-    solver_.init(P);
-    P.update(true);
-    stats_.push_back({-1, 0, P.hessian().chi2(), 0, 0, 0, true, true});
-    if (P.hessian().maxAbsValBVect() <= s.epsBVector) return TerminationReason::SuccessAtStart;
+    op.update(true);
+    stats_.push_back({-1, 0, op.hessian().chi2(), 0, 0, 0, true, true});
+    if (op.hessian().maxAbsValBVect() <= s.epsBVector) return TerminationReason::SuccessAtStart;
+    solver_.init(op.hessian().H(), op.hessian().b());
     iter_ = 0;
     while (iter_ < s.maxNumIt) {
-      const bool ok = solver_.computeIncrement(s.relLambda, s.absLambda);
-      const double inc = solver_.incrementVectorSquaredNorm();
-      if (!ok) {
-        stats_.push_back({iter_, 0, -1, 0, 0, inc, false, false});
+      const bool solveOk = solver_.computeIncrement(op.hessian().H(), op.hessian().b(), s.relLambda, s.absLambda);
+      if (!solveOk) {
+        stats_.push_back({iter_, 0, -1, 0, 0, 0, false, false});
         return TerminationReason::SolverFailure;
       }
+      const double inc = solver_.incrementVectorSquaredNorm();
       if (iter_ >= s.minNumIt && inc <= s.epsIncSquare) {
-        stats_.push_back({iter_, 0, P.hessian().chi2(), 0, 0, inc, true, false});
+        stats_.push_back({iter_, 0, op.hessian().chi2(), 0, 0, inc, true, false});
         return TerminationReason::SuccessSmallIncrement;
       }
-      P.oplus();
-      P.update(true);
-      const double chi2 = P.hessian().chi2();
-      stats_.push_back({iter_, 0, chi2, 0, 0, inc, true, true});
-      if (iter_ > s.minNumIt && P.hessian().maxAbsValBVect() <= s.epsBVector)
+      op.oplus(solver_.incrementVector());
+      op.update(true);
+      stats_.push_back({iter_, 0, op.hessian().chi2(), 0, 0, inc, true, true});
+      if (iter_ > s.minNumIt && op.hessian().maxAbsValBVect() <= s.epsBVector)
         return TerminationReason::SuccessEpsB;
-      if (iter_ > s.minNumIt && chi2 < s.epsChi2) return TerminationReason::SuccessSmallResiduals;
+      if (iter_ > s.minNumIt && op.hessian().chi2() < s.epsChi2) return TerminationReason::SuccessSmallResiduals;
       ++iter_;
     }
     return TerminationReason::MaxIterationReached;

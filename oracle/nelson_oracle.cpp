@@ -28,6 +28,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstdint>
 #include <cstring>
 #include <limits>
@@ -945,6 +946,184 @@ int gn_solve(Problem& P, const orc_gn_settings& s, double* trace, int cap, int* 
 
 Problem* as(void* h) { return static_cast<Problem*>(h); }
 
+// ---------------------------------------------------------------------------
+// Implicit-function adjoint of a converged BA solve, in FP64 (no counterpart
+// in the reference, which has no differentiation; it is the CPU reference
+// gradient the CUDA adjoint is checked against).
+//
+// At x* the local gradient b = sum_e w_e J_e' r_e vanishes; for a loss with
+// gradient dL/dx, H' mu = dL/dx with H = db/dx (derivative along the
+// retraction: R <- exp(dw) R, the rest additive), and
+//   dL/dz_e = w_e J_e mu_e,   dL/dw_e = -(J_e mu_e) . r_e.
+// H is assembled edge by edge from the derivative of the edge's own gradient
+// g_e = w_e J_e' r_e, taken by complex-step differentiation (the projection
+// and its analytic Jacobian evaluated in complex arithmetic at x* + i h v,
+// Im(g_e) / h, h = 1e-20: exact to rounding, no cancellation), so it is
+// independent of the forward-mode dual numbers the CUDA kernels use.  Its
+// blocks have the Gauss-Newton Hessian's pattern; each is symmetrised (the
+// antisymmetric part is proportional to b and vanishes at x*) and H mu =
+// dL/dx is solved with the oracle's own Schur solve at zero damping.
+template <typename T>
+void ba_resjac_t(const T* R, const T* t, T f, T k1, T k2, const T* X, const double* z, double cx,
+                 double cy, int bc, T* r, T* Jc, T* Jp) {
+  const T a0 = R[0] * X[0] + R[1] * X[1] + R[2] * X[2];
+  const T a1 = R[3] * X[0] + R[4] * X[1] + R[5] * X[2];
+  const T a2 = R[6] * X[0] + R[7] * X[1] + R[8] * X[2];
+  const T P0 = a0 + t[0], P1 = a1 + t[1], P2 = a2 + t[2];
+  const T iz = T(1.0) / P2;
+  const T x = P0 * iz, y = P1 * iz;
+  const T r2 = x * x + y * y;
+  const T d = T(1.0) + r2 * (k1 + k2 * r2);
+  r[0] = f * d * x + T(cx - z[0]);
+  r[1] = f * d * y + T(cy - z[1]);
+  const T g = T(2.0) * (k1 + T(2.0) * k2 * r2);
+  const T m00 = f * (d + g * x * x), m01 = f * g * x * y, m11 = f * (d + g * y * y);
+  const T M[6] = {m00 * iz, m01 * iz, -(m00 * x + m01 * y) * iz,
+                  m01 * iz, m11 * iz, -(m01 * x + m11 * y) * iz};
+  for (int i = 0; i < 2; i++) {
+    const T* m = M + 3 * i;
+    for (int j = 0; j < 3; j++) Jp[i * 3 + j] = m[0] * R[j] + m[1] * R[3 + j] + m[2] * R[6 + j];
+    T* jc = Jc + i * bc;
+    jc[0] = m[2] * a1 - m[1] * a2;
+    jc[1] = m[0] * a2 - m[2] * a0;
+    jc[2] = m[1] * a0 - m[0] * a1;
+    jc[3] = m[0];
+    jc[4] = m[1];
+    jc[5] = m[2];
+  }
+  if (bc == 9) {
+    Jc[6] = d * x;
+    Jc[7] = f * x * r2;
+    Jc[8] = f * x * r2 * r2;
+    Jc[9 + 6] = d * y;
+    Jc[9 + 7] = f * y * r2;
+    Jc[9 + 8] = f * y * r2 * r2;
+  }
+}
+
+// Edge gradient g = w [Jc' r; Jp' r] at the camera state `cs` and point X,
+// perturbed by i h along local direction k (k < bc: camera tangent, else
+// point coordinate k - bc); returns Im(g) / h in col (bc + 3 entries).
+void edge_hessian_column(const double* cs, const double* X, const double* z, double w, double f_fixed,
+                         double cx, double cy, int bc, int k, double* col) {
+  using Z = std::complex<double>;
+  const double h = 1e-20;
+  Z R[9], t[3], Xc[3], f, k1, k2;
+  for (int i = 0; i < 9; i++) R[i] = cs[i];
+  if (k < 3) {
+    // exp(i h [e_k]x) R = R + i h [e_k]x R  (the h^2 term is below rounding)
+    double K[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (k == 0) { K[5] = -1; K[7] = 1; }
+    if (k == 1) { K[2] = 1; K[6] = -1; }
+    if (k == 2) { K[1] = -1; K[3] = 1; }
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) {
+        double s = 0;
+        for (int q = 0; q < 3; q++) s += K[i * 3 + q] * cs[q * 3 + j];
+        R[i * 3 + j] += Z(0.0, h * s);
+      }
+  }
+  for (int i = 0; i < 3; i++) t[i] = cs[9 + i];
+  f = bc == 9 ? cs[12] : f_fixed;
+  k1 = bc == 9 ? cs[13] : 0.0;
+  k2 = bc == 9 ? cs[14] : 0.0;
+  for (int i = 0; i < 3; i++) Xc[i] = X[i];
+  if (k >= 3 && k < 6) t[k - 3] += Z(0.0, h);
+  if (bc == 9 && k == 6) f += Z(0.0, h);
+  if (bc == 9 && k == 7) k1 += Z(0.0, h);
+  if (bc == 9 && k == 8) k2 += Z(0.0, h);
+  if (k >= bc) Xc[k - bc] += Z(0.0, h);
+  Z r[2], Jc[18], Jp[6];
+  ba_resjac_t<Z>(R, t, f, k1, k2, Xc, z, cx, cy, bc, r, Jc, Jp);
+  for (int i = 0; i < bc; i++) col[i] = w * (Jc[i] * r[0] + Jc[bc + i] * r[1]).imag() / h;
+  for (int i = 0; i < 3; i++) col[bc + i] = w * (Jp[i] * r[0] + Jp[3 + i] * r[1]).imag() / h;
+}
+
+// Returns 1 when the solve succeeded.
+int adjoint_ba(Problem& P, const double* dL_dcams, const double* dL_dpts, double* g_obs, double* g_w,
+               double* mu_cams, double* mu_pts) {
+  const int bc = P.bu, nc = P.nu_var, np = P.nv_var, ne = (int)P.edges.size();
+  const int nl = bc + 3;
+  update(P, true);  // r, J and the Gauss-Newton blocks at x* (the pattern and UIDs)
+  std::vector<double> U(P.U.size(), 0.0), V(P.V.size(), 0.0), W(P.W.size(), 0.0);
+  std::vector<double> He((size_t)nl * nl), col(nl);
+  for (int e = 0; e < ne; e++) {  // insertion order: a fixed summation order
+    const Edge& E = P.edges[e];
+    const double* cs = param_u(P, E.id1, E.fixed1);
+    const double* X = param_v(P, E.id2, E.fixed2);
+    for (int k = 0; k < nl; k++) {
+      if ((k < bc && E.fixed1) || (k >= bc && E.fixed2)) continue;
+      edge_hessian_column(cs, X, E.z, E.w, P.f_fixed, P.cx, P.cy, bc, k, col.data());
+      for (int i = 0; i < nl; i++) He[(size_t)i * nl + k] = col[i];
+    }
+    if (!E.fixed1) {
+      double* Ub = U.data() + (size_t)P.h11[e] * bc * bc;
+      for (int i = 0; i < bc; i++)
+        for (int j = 0; j < bc; j++) Ub[i * bc + j] += 0.5 * (He[(size_t)i * nl + j] + He[(size_t)j * nl + i]);
+    }
+    if (!E.fixed2) {
+      double* Vb = V.data() + (size_t)P.h22[e] * 9;
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++)
+          Vb[i * 3 + j] += 0.5 * (He[(size_t)(bc + i) * nl + bc + j] + He[(size_t)(bc + j) * nl + bc + i]);
+    }
+    if (!E.fixed1 && !E.fixed2) {
+      double* Wb = W.data() + (size_t)P.h12[e] * bc * 3;
+      for (int i = 0; i < bc; i++)
+        for (int j = 0; j < 3; j++)
+          Wb[i * 3 + j] += 0.5 * (He[(size_t)i * nl + bc + j] + He[(size_t)(bc + j) * nl + i]);
+    }
+  }
+  // H mu = dL/dx through the Schur solve: b := -dL/dx, zero damping
+  std::vector<double> U0, V0, W0, bU0, bV0;
+  U0.swap(P.U);
+  V0.swap(P.V);
+  W0.swap(P.W);
+  bU0 = P.bU;
+  bV0 = P.bV;
+  P.U.swap(U);
+  P.V.swap(V);
+  P.W.swap(W);
+  for (int c = 0; c < nc; c++)
+    for (int i = 0; i < bc; i++) P.bU[(size_t)P.perm[c] * bc + i] = dL_dcams ? -dL_dcams[(size_t)c * bc + i] : 0.0;
+  for (int i = 0; i < 3 * np; i++) P.bV[i] = dL_dpts ? -dL_dpts[i] : 0.0;
+  const bool ok = compute_increment(P, 0.0, 0.0);
+  const std::vector<double> muU = P.incU, muV = P.incV;  // internal camera order
+  P.U.swap(U0);
+  P.V.swap(V0);
+  P.W.swap(W0);
+  P.bU = bU0;
+  P.bV = bV0;
+  // per-edge VJP (insertion order)
+  for (int e = 0; e < ne; e++) {
+    const Edge& E = P.edges[e];
+    const double* r = P.er.data() + (size_t)e * P.dr_max;
+    const double* Jc = P.eJ1.data() + (size_t)e * P.s1;
+    const double* Jp = P.eJ2.data() + (size_t)e * P.s2;
+    double Jm[2] = {0.0, 0.0};
+    if (!E.fixed1) {
+      const double* m = muU.data() + (size_t)P.perm[E.id1] * bc;
+      for (int i = 0; i < 2; i++)
+        for (int k = 0; k < bc; k++) Jm[i] += Jc[i * bc + k] * m[k];
+    }
+    if (!E.fixed2) {
+      const double* m = muV.data() + (size_t)E.id2 * 3;
+      for (int i = 0; i < 2; i++)
+        for (int k = 0; k < 3; k++) Jm[i] += Jp[i * 3 + k] * m[k];
+    }
+    if (g_obs) {
+      g_obs[2 * (size_t)e] = E.w * Jm[0];
+      g_obs[2 * (size_t)e + 1] = E.w * Jm[1];
+    }
+    if (g_w) g_w[e] = -(Jm[0] * r[0] + Jm[1] * r[1]);
+  }
+  if (mu_cams)
+    for (int c = 0; c < nc; c++)
+      for (int i = 0; i < bc; i++) mu_cams[(size_t)c * bc + i] = muU[(size_t)P.perm[c] * bc + i];
+  if (mu_pts) std::copy(muV.begin(), muV.end(), mu_pts);
+  return ok ? 1 : 0;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1163,6 +1342,13 @@ int orc_get_residuals(void* h, double* r) {
   for (size_t e = 0; e < P.edges.size(); e++)
     for (int i = 0; i < P.edges[e].dr; i++) r[e * P.edges[e].dr + i] = P.er[e * P.dr_max + i];
   return 0;
+}
+
+int orc_adjoint_ba(void* h, const double* dL_dcams, const double* dL_dpts, double* g_obs, double* g_w,
+                   double* mu_cams, double* mu_pts) {
+  Problem& P = *as(h);
+  if (!P.ready || P.kind != ORC_KIND_BA) return -1;
+  return adjoint_ba(P, dL_dcams, dL_dpts, g_obs, g_w, mu_cams, mu_pts);
 }
 
 int orc_solver_init(void* h) { return as(h)->ready ? 0 : -1; }

@@ -116,6 +116,18 @@ int orc_lm_solve(void* h, const orc_lm_settings* s, double* trace,
 int orc_gn_solve(void* h, const orc_gn_settings* s, double* trace,
                  int trace_cap, int* n_trace, int* its);
 
+/* Implicit-function adjoint of a converged BA solve (no counterpart in the
+ * reference): H mu = dL/dx with the exact Hessian H of the cost at the
+ * current parameters (complex-step derivatives of each edge's gradient),
+ * then per edge dL/dz = w J mu and dL/dw = -(J mu) . r.  dL_dcams: variable
+ * cameras in user order (tangent [dw, dt (, df, dk1, dk2)]); dL_dpts:
+ * variable points; either may be NULL.  Outputs (any may be NULL): g_obs (2
+ * per edge), g_w (1 per edge) in insertion order, mu in the layout of the
+ * inputs.  Returns 1 when the solve succeeded, 0 when H was not positive
+ * definite, -1 on a bad handle. */
+int orc_adjoint_ba(void* h, const double* dL_dcams, const double* dL_dpts,
+                   double* g_obs, double* g_w, double* mu_cams, double* mu_pts);
+
 /* Dense blocked Cholesky of an n x n row-major SPD matrix (lower triangle
  * used), exposed so its accuracy can be tested on its own.  Returns 1 on
  * success. */

@@ -78,6 +78,7 @@ def lib():
         L.orc_rho.argtypes = [vp, d, d]
         L.orc_set_intrinsics.argtypes = [vp, d, d, d]
         L.orc_compute_increment.argtypes = [vp, d, d]
+        L.orc_adjoint_ba.argtypes = [vp, vp, vp, vp, vp, vp, vp]
         L.orc_update.argtypes = [vp, i, C.POINTER(d)]
         L.orc_lm_solve.argtypes = [vp, C.POINTER(LMSettings), vp, i, C.POINTER(i), vp]
         L.orc_gn_solve.argtypes = [vp, C.POINTER(GNSettings), vp, i, C.POINTER(i), vp]
@@ -261,6 +262,20 @@ class Oracle:
         if reason < 0:
             raise RuntimeError("orc_lm_solve failed")
         return LM_REASONS[reason], tr[:n.value].copy(), int(its[0]), int(its[1])
+
+    def adjoint(self, dL_dpts=None, dL_dcams=None):
+        """FP64 implicit-function adjoint at the current (converged)
+        parameters: (dL/dobs (ne, 2), dL/dweight (ne,), mu_cams, mu_pts)."""
+        g_obs = np.zeros((self.ne, 2))
+        g_w = np.zeros(self.ne)
+        mu_c = np.zeros((self.nu_var, self.bu))
+        mu_p = np.zeros((self.nv_var, 3))
+        dc = None if dL_dcams is None else np.ascontiguousarray(dL_dcams, np.float64).reshape(self.nu_var, self.bu)
+        dp = None if dL_dpts is None else np.ascontiguousarray(dL_dpts, np.float64).reshape(self.nv_var, 3)
+        rc = self.L.orc_adjoint_ba(self.h, _p(dc), _p(dp), _p(g_obs), _p(g_w), _p(mu_c), _p(mu_p))
+        if rc != 1:
+            raise RuntimeError(f"orc_adjoint_ba failed ({rc})")
+        return g_obs, g_w, mu_c, mu_p
 
     def gn_solve(self, settings=None, trace_cap=4096):
         s = settings or GNSettings()

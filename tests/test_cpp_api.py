@@ -1,8 +1,13 @@
 """The header-only C++ API (include/nelson_b200/nelson.hpp).
 
-CPU: the header and the C++ test program compile and link against the
-library.  GPU: the program runs (host-loop LM / GN vs the device loop, fixed
-nodes, cost reduction) and exits 0.
+CPU: the header and the C++ test programs compile and link against the
+library.  GPU: test_api runs (host-loop LM / GN vs the device loop, fixed
+nodes, cost reduction) and exits 0; test_solver_concept drives the
+reference-shaped LevenbergMarquardt / GaussNewton loops (the calls of
+nelson/LevenbergMarquardt.hpp:36-146 on the Solver and problem concepts) with
+a host-assembled problem (the reference's 5 x 2D / 3 x 3D fixture, final
+chi2 < 1e-12) and with a BASection read from a BAL file, whose per-sub-
+iteration trace must match the FP64 oracle's (1e-9 FP64, 1e-6 mixed).
 """
 import os
 import shutil
@@ -13,18 +18,18 @@ import pytest
 from nelson_b200 import build as nb_build
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-SRC = os.path.join(ROOT, "tests", "cpp", "test_api.cpp")
 
 
-def _compile(out_dir):
+def _compile(out_dir, name="test_api"):
     gxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else shutil.which("g++")
     if gxx is None:
         pytest.skip("no C++ compiler")
     if not os.path.exists(nb_build.LIB):
         nb_build.build()
-    exe = os.path.join(out_dir, "test_api")
+    exe = os.path.join(out_dir, name)
     lib_dir = os.path.dirname(nb_build.LIB)
-    cmd = [gxx, "-O2", "-std=c++17", "-Wall", "-Wextra", "-I" + os.path.join(ROOT, "include"), SRC,
+    src = os.path.join(ROOT, "tests", "cpp", name + ".cpp")
+    cmd = [gxx, "-O2", "-std=c++17", "-Wall", "-Wextra", "-I" + os.path.join(ROOT, "include"), src,
            "-o", exe, "-L" + lib_dir, "-lnelson_b200", "-Wl,-rpath," + lib_dir,
            "-Wl,--allow-shlib-undefined"]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -35,6 +40,7 @@ def _compile(out_dir):
 
 def test_cpp_api_compiles(tmp_path):
     assert os.path.exists(_compile(str(tmp_path)))
+    assert os.path.exists(_compile(str(tmp_path), "test_solver_concept"))
 
 
 @pytest.mark.gpu
@@ -59,3 +65,33 @@ def test_cpp_problem_file_readers(tmp_path):
     r = subprocess.run([exe, str(tmp_path)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "ALL OK" in r.stdout
+
+
+@pytest.mark.gpu
+def test_reference_concept_loops(tmp_path, oracle_lib):
+    import numpy as np
+
+    from nelson_b200 import problems as P
+    exe = _compile(str(tmp_path), "test_solver_concept")
+    p = P.make_config(1, 0.05)  # 10 cameras x 9, 2,500 points
+    p.obs = p.obs - np.array([p.cx, p.cy])
+    p.cx = p.cy = 0.0
+    bal = str(tmp_path / "scene.bal")
+    P.save_bal(bal, p)
+    its = 8
+    r = subprocess.run([exe, bal, str(its)], capture_output=True, text=True, timeout=300)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "ALL OK" in r.stdout
+    o = oracle_lib.Oracle.from_ba(P.load_bal(bal))
+    _, tr_o, _, _ = o.lm_solve(oracle_lib.LMSettings(maxNumIt=its))
+    for prec, tol in ((0, 1e-9), (1, 1e-6)):
+        rows = [ln.split()[2:] for ln in r.stdout.splitlines() if ln.startswith(f"TRACE {prec} ")]
+        tr = np.array([[float(x) for x in row] for row in rows])
+        assert len(tr) == len(tr_o), (prec, len(tr), len(tr_o))
+        for k in range(len(tr)):
+            if tr_o[k, 2] < 0:
+                continue
+            assert abs(tr[k, 2] - tr_o[k, 2]) <= tol * tr_o[k, 2], (prec, k, tr[k], tr_o[k])
+            if tr_o[k, 3] != 0:
+                assert tr[k, 3] == pytest.approx(tr_o[k, 3], rel=1e-6), (prec, k)

@@ -225,3 +225,54 @@ def test_dense_cholesky(oracle_lib):
     assert np.abs(L @ L.T - A).max() < 1e-10 * np.abs(A).max()
     B = -np.eye(4)
     assert not oracle_lib.dense_cholesky(B)
+
+
+def test_oracle_adjoint_matches_finite_differences():
+    """The oracle's FP64 implicit-function adjoint (exact Hessian by
+    complex-step derivatives) against central differences (h = 1e-6) of the
+    oracle's own re-converged solution, on a small weighted ring scene with
+    two fixed cameras (no gauge freedom): 1e-4 relative."""
+    import numpy as np
+
+    from nelson_b200.problems import ring_scene, with_fixed_nodes
+    from oracle.oracle import GNSettings, LMSettings, Oracle
+
+    def scene():
+        return with_fixed_nodes(ring_scene(10, 150, 3, 8, 6, seed=99, name="adj", weights=True), 2, 0)
+
+    gn = dict(maxNumIt=6, epsIncSquare=0.0, epsBVector=0.0, epsChi2=0.0)
+    p = scene()
+    o = Oracle.from_ba(p)
+    o.lm_solve(LMSettings(maxNumIt=60))
+    o.gn_solve(GNSettings(**gn))
+    cams_s, pts_s = o.get_params()
+    xt = p.pts_true[:p.np_var]
+    g_obs, g_w, _, _ = o.adjoint(dL_dpts=2.0 * (pts_s[:p.np_var] - xt))
+    rng = np.random.default_rng(0)
+    coords = [("obs", int(i)) for i in rng.choice(2 * p.ne, 12, replace=False)] + \
+             [("w", int(i)) for i in rng.choice(p.ne, 12, replace=False)]
+    h = 1e-6
+    adjs, fds = [], []
+    for kind, idx in coords:
+        vals = []
+        for sgn in (1.0, -1.0):
+            q = scene()
+            q.cams, q.pts = cams_s.copy(), pts_s.copy()
+            if kind == "obs":
+                q.obs.reshape(-1)[idx] += sgn * h
+            else:
+                q.weight[idx] += sgn * h
+            oo = Oracle.from_ba(q)
+            oo.gn_solve(GNSettings(**gn))
+            vals.append(oo.get_params()[1][:p.np_var].copy())
+        xp, xm = vals
+        fd = float(np.sum((xp - xm) * (xp + xm - 2 * xt))) / (2 * h)
+        adjs.append(g_obs.reshape(-1)[idx] if kind == "obs" else g_w[idx])
+        fds.append(fd)
+    adjs, fds = np.array(adjs), np.array(fds)
+    # per coordinate where the difference quotient is well above its noise
+    # (|fd| >= 1% of the largest), and every coordinate against the scale
+    big = np.abs(fds) >= 1e-2 * np.abs(fds).max()
+    assert big.sum() >= 10
+    assert (np.abs(adjs[big] - fds[big]) <= 1e-4 * np.abs(fds[big])).all(), (adjs, fds)
+    assert np.abs(adjs - fds).max() <= 1e-4 * np.abs(fds).max()

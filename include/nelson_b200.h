@@ -249,6 +249,40 @@ typedef struct {
 nl_status nl_adjoint(nl_problem* h, const double* dL_dcams, const double* dL_dpts, int sweeps, double* g_obs,
                      double* g_weight, double* mu_cams, double* mu_pts, nl_adjoint_report* rep);
 
+/* ---- unrolled differentiation of K LM steps (per-step checkpoints) ------- */
+/* No counterpart in the reference.  The unrolled map is K accepted
+ * LevenbergMarquardt steps from the current parameters x_0,
+ *     x_{k+1} = x_k (+) delta_k,   delta_k = -(J'WJ(x_k) + mu_k I)^-1 b(x_k),
+ * exactly the increments of nelson/LevenbergMarquardt.hpp:63-141 with the
+ * damping mu_k of the accepted sub-iterations held fixed (the accept / reject
+ * choices and the mu updates are discrete and not differentiated; rejected
+ * sub-iterations leave x unchanged).  Pass the mu of an LM trace's accepted
+ * records to differentiate that LM run.
+ * nl_unroll_record takes the K steps from the current parameters, saving x_k
+ * (cameras and points, a few hundred kilobytes per step at 64 cameras / 5,000
+ * points) before each one; on return the parameters are x_K.  A step whose
+ * damped system is not positive definite stops the record (NL_ERR_NOT_SPD).
+ * nl_unroll_adjoint then runs backwards through the recorded steps: for each
+ * k it restores x_k from its checkpoint, re-forms J'WJ and the step (the
+ * factorisation is recomputed, not stored) and applies the step's
+ * vector-Jacobian product.  Inputs: dL/dx_K as in nl_adjoint (dL_dcams in the
+ * camera tangent [dw, dt (, df, dk1, dk2)] at x_K, user order; dL_dpts;
+ * either may be NULL).  Outputs (any may be NULL): g_obs (2 per edge) and
+ * g_weight (1 per edge) in the order the edges were added, g_cams0 the
+ * gradient w.r.t. the initial camera parameters as nl_set_params takes them
+ * (axis-angle, t (, f, k1, k2); variable cameras, user order), g_pts0 w.r.t.
+ * the initial points.  On return the parameters are x_K again; the Hessian
+ * blocks and b are those of x_0 (call nl_update before reading them). */
+typedef struct {
+  int steps;        /* steps recorded / differentiated */
+  int ok;           /* 1 when every factorisation succeeded */
+  double chi2;      /* cost at x_K (nl_unroll_record) */
+  double device_ms; /* device time of the call */
+} nl_unroll_report;
+nl_status nl_unroll_record(nl_problem* h, int nsteps, const double* mu, nl_unroll_report* rep);
+nl_status nl_unroll_adjoint(nl_problem* h, const double* dL_dcams, const double* dL_dpts, double* g_obs,
+                            double* g_weight, double* g_cams0, double* g_pts0, nl_unroll_report* rep);
+
 nl_status nl_phase_timings(nl_problem* h, nl_phase_times* out);
 /* detail = 1: nl_compute_increment also times every step of the
  * factorisation's critical path (panel_ms, wait_ms, first_ms).  That costs one

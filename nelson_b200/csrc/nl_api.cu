@@ -14,6 +14,7 @@
 #include "ba_kernels.cuh"
 #include "adjoint.cuh"
 #include "schur_core.cuh"
+#include "unroll.cuh"
 
 using namespace nl;
 
@@ -64,6 +65,9 @@ struct nl_problem {
   DevBuf d_lam;
   long long launches = 0;
   DevBuf adj_vec, adj_slot2int, adj_out;  // adjoint work (allocated on first nl_adjoint)
+  DevBuf unr_ckpt, unr_work;               // unrolled steps: per-step checkpoints, backward work
+  std::vector<double> unr_mu;              // damping of the recorded steps
+  int unr_n = -1;                          // recorded steps (-1: none)
   cudaGraphExec_t sub_exec = nullptr;       // captured LM sub-iteration without trace (batched solves)
   cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
   float eval_ms = 0;
@@ -1155,6 +1159,21 @@ void enqueue_hv(nl_problem* h, const double* vU, const double* vV, double* outU,
   h->launches += 2;
 }
 
+// Work of nl_adjoint ([g | res | hv | mu], FP64, internal camera order then
+// points; per-edge outputs) and the camera slot -> internal camera map used
+// by the adjoint kernels, allocated on first use.
+nl_status ensure_adjoint_buffers(nl_problem* h) {
+  if (h->adj_vec.p) return NL_OK;
+  const int ntot = h->nci * h->desc.bc + 3 * h->desc.np_var, ne = (int)h->e_cam.size();
+  nl_status s;
+  if ((s = h->adj_vec.alloc(sizeof(double) * 4 * (size_t)std::max(ntot, 1))) != NL_OK) return s;
+  std::vector<int> s2i(h->nc_all(), -1);
+  for (int u = 0; u < h->desc.nc_var; u++) s2i[u] = h->perm[u];
+  if ((s = upload(h->adj_slot2int, s2i, h->st)) != NL_OK) return s;
+  if ((s = h->adj_out.alloc(sizeof(double) * 3 * (size_t)std::max(ne, 1))) != NL_OK) return s;
+  return NL_OK;
+}
+
 template <typename T>
 void enqueue_neg_to_b(nl_problem* h, const double* res, int nU, int nV3) {
   if (nU > 0) neg_to_b_kernel<T><<<cdiv(nU, 256), 256, 0, h->st>>>(res, nU, (T*)h->core->dbU());
@@ -1175,14 +1194,7 @@ nl_status nl_adjoint(nl_problem* h, const double* dL_dcams, const double* dL_dpt
   const int nU = nci * bc, nV3 = 3 * npv, ntot = nU + nV3;
   const int ne = (int)h->e_cam.size();
   nl_status s;
-  if (!h->adj_vec.p) {
-    // [g | res | hv | mu], FP64, internal camera order then points
-    if ((s = h->adj_vec.alloc(sizeof(double) * 4 * (size_t)std::max(ntot, 1))) != NL_OK) return s;
-    std::vector<int> s2i(h->nc_all(), -1);
-    for (int u = 0; u < ncv; u++) s2i[u] = h->perm[u];
-    if ((s = upload(h->adj_slot2int, s2i, h->st)) != NL_OK) return s;
-    if ((s = h->adj_out.alloc(sizeof(double) * 3 * (size_t)std::max(ne, 1))) != NL_OK) return s;
-  }
+  if ((s = ensure_adjoint_buffers(h)) != NL_OK) return s;
   double* g = h->adj_vec.as<double>();
   double* res = g + ntot;
   double* hv = res + ntot;
@@ -1260,6 +1272,179 @@ nl_status nl_adjoint(nl_problem* h, const double* dL_dcams, const double* dL_dpt
     rep->sweeps = sweeps;
     rep->grad_norm = gnorm;
     rep->residual_norm = std::sqrt(rnorm);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev_t0, h->ev_t1);
+    rep->device_ms = ms;
+  }
+  if (st & ST_SPIN_TIMEOUT) return NL_ERR_TIMEOUT;
+  if (st) return NL_ERR_NOT_SPD;
+  return NL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Unrolled differentiation (see unroll.cuh for the algebra).
+nl_status nl_unroll_record(nl_problem* h, int nsteps, const double* mu, nl_unroll_report* rep) {
+  NL_CHECK_READY(h);
+  if (nsteps < 0 || nsteps > 100000 || (nsteps > 0 && !mu)) return NL_ERR_ARG;
+  for (int k = 0; k < nsteps; k++)
+    if (!(mu[k] >= 0.0) || !std::isfinite(mu[k])) return NL_ERR_ARG;
+  NL_CUDA(cudaSetDevice(h->device));
+  const size_t nc = (size_t)h->nc_all() * 16, np = (size_t)h->np_all() * 3, per = nc + np;
+  nl_status s;
+  if (h->unr_ckpt.bytes < sizeof(double) * per * (size_t)std::max(nsteps, 1))
+    if ((s = h->unr_ckpt.alloc(sizeof(double) * per * (size_t)std::max(nsteps, 1))) != NL_OK) return s;
+  h->unr_n = -1;
+  h->unr_mu.assign(mu, mu + nsteps);
+  double* ck = h->unr_ckpt.as<double>();
+  NL_CUDA(cudaEventRecord(h->ev_t0, h->st));
+  int st = 0, done = 0;
+  for (int k = 0; k < nsteps; k++) {
+    // checkpoint x_k, then the step at x_k with damping mu_k
+    NL_CUDA(cudaMemcpyAsync(ck + per * k, h->cam.p, sizeof(double) * nc, cudaMemcpyDeviceToDevice, h->st));
+    if (np) NL_CUDA(cudaMemcpyAsync(ck + per * k + nc, h->pt.p, sizeof(double) * np, cudaMemcpyDeviceToDevice, h->st));
+    if ((s = enqueue_eval(h, true, h->scal, h->scal + 1, nullptr)) != NL_OK) return s;
+    h->host_pin[16] = 0.0;
+    h->host_pin[17] = mu[k];
+    NL_CUDA(cudaMemcpyAsync(h->d_lam.p, h->host_pin + 16, 2 * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    NL_CUDA(cudaMemsetAsync(h->status, 0, sizeof(int), h->st));
+    if ((s = h->core->enqueue_increment(h->d_lam.as<double>(), h->status, nullptr)) != NL_OK) return s;
+    NL_CUDA(cudaMemcpyAsync(h->host_pin + 20, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    NL_CUDA(cudaStreamSynchronize(h->st));
+    memcpy(&st, h->host_pin + 20, sizeof(int));
+    if (st) break;  // the step failed: the schedule is not a valid LM trajectory
+    if ((s = enqueue_oplus(h, nullptr)) != NL_OK) return s;
+    done = k + 1;
+  }
+  if ((s = enqueue_eval(h, false, h->scal, nullptr, nullptr)) != NL_OK) return s;
+  NL_CUDA(cudaEventRecord(h->ev_t1, h->st));
+  double chi2 = 0;
+  if ((s = sync_read(h, h->scal, &chi2, 1)) != NL_OK) return s;
+  if (rep) {
+    rep->steps = done;
+    rep->ok = st == 0 ? 1 : 0;
+    rep->chi2 = chi2;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev_t0, h->ev_t1);
+    rep->device_ms = ms;
+  }
+  if (st & ST_SPIN_TIMEOUT) return NL_ERR_TIMEOUT;
+  if (st) return NL_ERR_NOT_SPD;
+  h->unr_n = nsteps;
+  return NL_OK;
+}
+
+nl_status nl_unroll_adjoint(nl_problem* h, const double* dL_dcams, const double* dL_dpts, double* g_obs,
+                            double* g_weight, double* g_cams0, double* g_pts0, nl_unroll_report* rep) {
+  NL_CHECK_READY(h);
+  if (h->unr_n < 0) return NL_ERR_STATE;
+  NL_CUDA(cudaSetDevice(h->device));
+  const int K = h->unr_n, bc = h->desc.bc, nci = h->nci, npv = h->desc.np_var, ncv = h->desc.nc_var;
+  const int nU = nci * bc, nV3 = 3 * npv, ntot = nU + nV3, ne = (int)h->e_cam.size();
+  const size_t nc = (size_t)h->nc_all() * 16, np = (size_t)h->np_all() * 3, per = nc + np;
+  nl_status s;
+  if ((s = ensure_adjoint_buffers(h)) != NL_OK) return s;
+  // [lam | a | delta | grad] (ntot each) | g_obs (2 ne) | g_w (ne) | x_K (per) | g_cams (ncv bc) |
+  // the (rel, abs) damping pairs of the steps (2 K)
+  const size_t need =
+      4 * (size_t)std::max(ntot, 1) + 3 * (size_t)std::max(ne, 1) + per + (size_t)ncv * bc + 2 * (size_t)K + 1;
+  if (h->unr_work.bytes < sizeof(double) * need)
+    if ((s = h->unr_work.alloc(sizeof(double) * need)) != NL_OK) return s;
+  double* lam = h->unr_work.as<double>();
+  double* a = lam + std::max(ntot, 1);
+  double* delta = a + std::max(ntot, 1);
+  double* grad = delta + std::max(ntot, 1);
+  double* gobs = grad + std::max(ntot, 1);
+  double* gw = gobs + 2 * (size_t)std::max(ne, 1);
+  double* xK = gw + std::max(ne, 1);
+  double* gcam = xK + per;
+  double* lams = gcam + (size_t)ncv * bc;
+  const double* ck = h->unr_ckpt.as<double>();
+  const int* s2i = h->adj_slot2int.as<int>();
+  // lam_K = dL/dx_K in internal camera order
+  std::vector<double> lh(ntot, 0.0);
+  if (dL_dcams)
+    for (int u = 0; u < ncv; u++)
+      for (int i = 0; i < bc; i++) lh[(size_t)h->perm[u] * bc + i] = dL_dcams[(size_t)u * bc + i];
+  if (dL_dpts) std::copy(dL_dpts, dL_dpts + nV3, lh.begin() + nU);
+  std::vector<double> lamh(2 * (size_t)K);
+  for (int k = 0; k < K; k++) {
+    lamh[2 * (size_t)k] = 0.0;
+    lamh[2 * (size_t)k + 1] = h->unr_mu[k];
+  }
+  NL_CUDA(cudaEventRecord(h->ev_t0, h->st));
+  if (ntot) NL_CUDA(cudaMemcpyAsync(lam, lh.data(), sizeof(double) * ntot, cudaMemcpyHostToDevice, h->st));
+  if (K) NL_CUDA(cudaMemcpyAsync(lams, lamh.data(), sizeof(double) * 2 * K, cudaMemcpyHostToDevice, h->st));
+  NL_CUDA(cudaMemsetAsync(gobs, 0, sizeof(double) * 3 * (size_t)std::max(ne, 1), h->st));
+  NL_CUDA(cudaMemcpyAsync(xK, h->cam.p, sizeof(double) * nc, cudaMemcpyDeviceToDevice, h->st));
+  if (np) NL_CUDA(cudaMemcpyAsync(xK + nc, h->pt.p, sizeof(double) * np, cudaMemcpyDeviceToDevice, h->st));
+  NL_CUDA(cudaMemsetAsync(h->status, 0, sizeof(int), h->st));
+  const bool f64 = h->desc.precision == NL_PREC_FP64;
+  for (int k = K - 1; k >= 0; k--) {
+    // x_k from its checkpoint; J, r, J'WJ and b there; the step delta_k (and
+    // its factorisation) with the recorded damping
+    NL_CUDA(cudaMemcpyAsync(h->cam.p, ck + per * k, sizeof(double) * nc, cudaMemcpyDeviceToDevice, h->st));
+    if (np) NL_CUDA(cudaMemcpyAsync(h->pt.p, ck + per * k + nc, sizeof(double) * np, cudaMemcpyDeviceToDevice, h->st));
+    if ((s = enqueue_eval(h, true, h->scal, h->scal + 1, nullptr)) != NL_OK) return s;
+    if ((s = h->core->enqueue_increment(lams + 2 * (size_t)k, h->status, nullptr)) != NL_OK) return s;
+    if (nU) NL_CUDA(cudaMemcpyAsync(delta, h->core->incU, sizeof(double) * nU, cudaMemcpyDeviceToDevice, h->st));
+    if (nV3) NL_CUDA(cudaMemcpyAsync(delta + nU, h->core->incV, sizeof(double) * nV3, cudaMemcpyDeviceToDevice, h->st));
+    // through the retraction: a (the step's adjoint) and the direct part of lam_k
+    if (ntot) {
+      if (bc == 9)
+        unroll_split_kernel<9><<<cdiv(nci + nV3, 256), 256, 0, h->st>>>(nci, nV3, delta, lam, a);
+      else
+        unroll_split_kernel<6><<<cdiv(nci + nV3, 256), 256, 0, h->st>>>(nci, nV3, delta, lam, a);
+      h->launches++;
+    }
+    // u = A^-1 a with the step's factorisation (b := -a, so the increment is u)
+    if (f64)
+      enqueue_neg_to_b<double>(h, a, nU, nV3);
+    else
+      enqueue_neg_to_b<float>(h, a, nU, nV3);
+    if ((s = h->core->enqueue_resolve(h->status)) != NL_OK) return s;
+    const double* uU = h->core->incU;
+    const double* uV = h->core->incV;
+    // lam_k -= grad_x (psi + phi); per-edge contributions to g_obs / g_w
+    if (bc == 9) {
+      if (nci) unroll_grad_cam_kernel<9, 128><<<nci, 128, 0, h->st>>>(h->ba, uU, uV, delta, delta + nU, grad);
+      if (npv) unroll_grad_pt_kernel<9><<<cdiv(npv, 128), 128, 0, h->st>>>(h->ba, s2i, uU, uV, delta, delta + nU, grad + nU);
+      if (ne) unroll_vjp_edge_kernel<9><<<cdiv(ne, 128), 128, 0, h->st>>>(h->ba, h->d_eorder.as<int>(), s2i, uU, uV, delta,
+                                                                             delta + nU, gobs, gw);
+    } else {
+      if (nci) unroll_grad_cam_kernel<6, 128><<<nci, 128, 0, h->st>>>(h->ba, uU, uV, delta, delta + nU, grad);
+      if (npv) unroll_grad_pt_kernel<6><<<cdiv(npv, 128), 128, 0, h->st>>>(h->ba, s2i, uU, uV, delta, delta + nU, grad + nU);
+      if (ne) unroll_vjp_edge_kernel<6><<<cdiv(ne, 128), 128, 0, h->st>>>(h->ba, h->d_eorder.as<int>(), s2i, uU, uV, delta,
+                                                                             delta + nU, gobs, gw);
+    }
+    if (ntot) sub_kernel<<<cdiv(ntot, 256), 256, 0, h->st>>>(lam, grad, ntot);
+    h->launches += 4;
+    NL_CUDA(cudaGetLastError());
+  }
+  // lam_0 in the caller's parameters (axis-angle cameras in user order)
+  if (ncv) {
+    if (bc == 9)
+      unroll_to_params_kernel<9><<<cdiv(ncv, 128), 128, 0, h->st>>>(ncv, s2i, K > 0 ? ck : xK, lam, gcam);
+    else
+      unroll_to_params_kernel<6><<<cdiv(ncv, 128), 128, 0, h->st>>>(ncv, s2i, K > 0 ? ck : xK, lam, gcam);
+    h->launches++;
+  }
+  NL_CUDA(cudaGetLastError());
+  // back to x_K
+  NL_CUDA(cudaMemcpyAsync(h->cam.p, xK, sizeof(double) * nc, cudaMemcpyDeviceToDevice, h->st));
+  if (np) NL_CUDA(cudaMemcpyAsync(h->pt.p, xK + nc, sizeof(double) * np, cudaMemcpyDeviceToDevice, h->st));
+  NL_CUDA(cudaEventRecord(h->ev_t1, h->st));
+  if (g_cams0 && ncv) NL_CUDA(cudaMemcpyAsync(g_cams0, gcam, sizeof(double) * ncv * bc, cudaMemcpyDeviceToHost, h->st));
+  if (g_pts0 && nV3) NL_CUDA(cudaMemcpyAsync(g_pts0, lam + nU, sizeof(double) * nV3, cudaMemcpyDeviceToHost, h->st));
+  if (g_obs && ne) NL_CUDA(cudaMemcpyAsync(g_obs, gobs, sizeof(double) * 2 * ne, cudaMemcpyDeviceToHost, h->st));
+  if (g_weight && ne) NL_CUDA(cudaMemcpyAsync(g_weight, gw, sizeof(double) * ne, cudaMemcpyDeviceToHost, h->st));
+  NL_CUDA(cudaMemcpyAsync(h->host_pin + 20, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  NL_CUDA(cudaStreamSynchronize(h->st));
+  int st = 0;
+  memcpy(&st, h->host_pin + 20, sizeof(int));
+  if (rep) {
+    rep->steps = K;
+    rep->ok = st == 0 ? 1 : 0;
+    rep->chi2 = 0.0;
     float ms = 0;
     cudaEventElapsedTime(&ms, h->ev_t0, h->ev_t1);
     rep->device_ms = ms;

@@ -75,6 +75,10 @@ class AdjointReport(C.Structure):
                 ("device_ms", C.c_double)]
 
 
+class UnrollReport(C.Structure):
+    _fields_ = [("steps", C.c_int), ("ok", C.c_int), ("chi2", C.c_double), ("device_ms", C.c_double)]
+
+
 class SolverDesc(C.Structure):
     _fields_ = [("bu", C.c_int), ("nu", C.c_int), ("nv", C.c_int), ("nU", C.c_int), ("nV", C.c_int),
                 ("nW", C.c_int), ("precision", C.c_int), ("refine_sweeps", C.c_int), ("device", C.c_int)]
@@ -89,7 +93,7 @@ EXPORTS = [
     "nl_kernel_launches", "nl_solver_create", "nl_solver_destroy", "nl_solver_set_hessian",
     "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_selftest_tc_update", "nl_ba_cost_noalloc",
     "nl_adjoint", "nl_lm_solve_batch", "nl_set_timing_detail", "nl_set_solver_kind", "nl_solver_set_kind", "nl_permute_rcm_u", "nl_get_user2internal_u", "nl_rcm_order",
-    "nl_set_wait_limit", "nl_check_wait_timeout",
+    "nl_set_wait_limit", "nl_check_wait_timeout", "nl_unroll_record", "nl_unroll_adjoint",
     "nl_status_string",
     "nl_version",
 ]
@@ -127,6 +131,8 @@ def load(build_if_missing: bool = True):
     L.nl_adjoint.argtypes = [vp, vp, vp, i, vp, vp, vp, vp, C.POINTER(AdjointReport)]
     L.nl_ba_cost_noalloc.argtypes = [i, i, vp, vp, vp, vp, vp, vp, d, d, d, vp, vp]
     L.nl_set_wait_limit.argtypes = [vp, C.c_longlong]
+    L.nl_unroll_record.argtypes = [vp, i, vp, C.POINTER(UnrollReport)]
+    L.nl_unroll_adjoint.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.POINTER(UnrollReport)]
     L.nl_check_wait_timeout.argtypes = [vp]
     for name in EXPORTS:  # fails loudly if the library lacks an entry point
         if name not in ("nl_status_string", "nl_version"):
@@ -329,6 +335,29 @@ class BAProblemGPU:
                                   C.byref(rep)), "nl_adjoint")
         r = {n: getattr(rep, n) for n, _ in AdjointReport._fields_}
         return (g_obs, g_w, r, mu_c, mu_p) if want_mu else (g_obs, g_w, r)
+
+    def unroll_record(self, mus):
+        """nl_unroll_record: len(mus) damped steps from the current parameters
+        with per-step checkpoints; returns the report as a dict."""
+        m = np.ascontiguousarray(mus, np.float64)
+        rep = UnrollReport()
+        self._c(self.L.nl_unroll_record(self.h, int(m.size), _p(m), C.byref(rep)), "nl_unroll_record")
+        return {n: getattr(rep, n) for n, _ in UnrollReport._fields_}
+
+    def unroll_adjoint(self, dL_dpts=None, dL_dcams=None):
+        """nl_unroll_adjoint: gradients of L(x_K) through the recorded steps:
+        (dL/dobs (ne, 2), dL/dweight (ne,), dL/dcams0 (nc_var, bc), dL/dpts0
+        (np_var, 3), report)."""
+        g_obs = np.zeros((self.ne, 2))
+        g_w = np.zeros(self.ne)
+        g_c = np.zeros((self.nc_var, self.bc))
+        g_p = np.zeros((self.np_var, 3))
+        dc = None if dL_dcams is None else np.ascontiguousarray(dL_dcams, np.float64).reshape(self.nc_var, self.bc)
+        dp = None if dL_dpts is None else np.ascontiguousarray(dL_dpts, np.float64).reshape(self.np_var, 3)
+        rep = UnrollReport()
+        self._c(self.L.nl_unroll_adjoint(self.h, _p(dc), _p(dp), _p(g_obs), _p(g_w), _p(g_c), _p(g_p),
+                                         C.byref(rep)), "nl_unroll_adjoint")
+        return g_obs, g_w, g_c, g_p, {n: getattr(rep, n) for n, _ in UnrollReport._fields_}
 
     def phase_times(self):
         t = PhaseTimes()

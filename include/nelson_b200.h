@@ -216,6 +216,35 @@ nl_status nl_lm_solve(nl_problem* h, const nl_lm_settings* s, nl_solve_report* r
  * the common start to its completion.  No trace is recorded. */
 nl_status nl_lm_solve_batch(nl_problem** hs, int n, const nl_lm_settings* s, nl_solve_report* reps,
                             double* latency_ms);
+/* ---- many small problems in one persistent launch ----------------------- */
+/* LevenbergMarquardt<SolverCholeskySchur>::solve (nelson/LevenbergMarquardt.hpp:
+ * 36-146) for n independent BA sections of uneven sizes in ONE kernel launch
+ * (the reference solves one problem per call): the launch's CTAs take
+ * problems from a device work queue, largest first, and each CTA runs one
+ * problem's whole LM solve -- Jacobians and Hessian blocks, the Schur
+ * complement, a blocked Cholesky of S in shared memory, the solves, the
+ * back-substitution and the LM decisions -- in FP64, then takes the next.
+ * No CTA waits for another.  A problem's result does not depend on the launch
+ * shape or on the other problems of the batch.
+ * nl_batch_create packs the sections (ready handles on the current device, all
+ * with the same camera block size, at most 768 reduced-system rows each) into
+ * one device arena; the observations and weights are taken as they are at
+ * that moment.  nl_batch_lm_solve copies each handle's current parameters in,
+ * solves, and writes the results back to the handles (read them with
+ * nl_get_params).  threads (128, 256 or 512) and ctas_per_sm (1..4) choose the
+ * launch shape; 0 takes the choice of nl_batch_autotune, which times every
+ * candidate on the batch itself (each from the handles' parameters, so it
+ * changes nothing) and keeps the fastest.  reps (may be NULL): per problem,
+ * device_ms is its own solve time; latency_ms (may be NULL): per problem, the
+ * time from the first problem's start to its end; device_ms_total (may be
+ * NULL): the launch's device time. */
+typedef struct nl_batch nl_batch;
+nl_status nl_batch_create(nl_problem** hs, int n, nl_batch** out);
+nl_status nl_batch_destroy(nl_batch* b);
+nl_status nl_batch_autotune(nl_batch* b, const nl_lm_settings* s, int* threads, int* ctas_per_sm);
+nl_status nl_batch_lm_solve(nl_batch* b, const nl_lm_settings* s, int threads, int ctas_per_sm,
+                            nl_solve_report* reps, double* latency_ms, double* device_ms_total);
+
 /* GaussNewton<Solver>::solve (nelson/GaussNewton.hpp:32-127). */
 nl_status nl_gn_solve(nl_problem* h, const nl_gn_settings* s, nl_solve_report* rep,
                       double* trace, int trace_cap);

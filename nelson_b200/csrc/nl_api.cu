@@ -13,6 +13,7 @@
 
 #include "ba_kernels.cuh"
 #include "adjoint.cuh"
+#include "problem_view.h"
 #include "schur_core.cuh"
 #include "unroll.cuh"
 
@@ -1453,6 +1454,35 @@ nl_status nl_unroll_adjoint(nl_problem* h, const double* dL_dcams, const double*
   if (st) return NL_ERR_NOT_SPD;
   return NL_OK;
 }
+
+}  // extern "C"
+
+nl_status nl_problem_get_view(nl_problem* h, nl_problem_view* v) {
+  if (!h || !v) return NL_ERR_ARG;
+  v->bc = h->desc.bc;
+  v->ncv = h->desc.nc_var;
+  v->ncf = h->desc.nc_fix;
+  v->npv = h->desc.np_var;
+  v->npf = h->desc.np_fix;
+  v->f = h->desc.f;
+  v->cx = h->desc.cx;
+  v->cy = h->desc.cy;
+  v->e_cam = &h->e_cam;
+  v->e_camfix = &h->e_camfix;
+  v->e_pt = &h->e_pt;
+  v->e_ptfix = &h->e_ptfix;
+  v->perm = &h->perm;
+  v->eorder = &h->eorder;
+  v->porder = &h->porder;
+  v->e_obs = &h->e_obs;
+  v->e_w = &h->e_w;
+  v->d_cam = h->cam.as<double>();
+  v->d_pt = h->pt.as<double>();
+  v->ready = h->ready;
+  return NL_OK;
+}
+
+extern "C" {
 
 nl_status nl_phase_timings(nl_problem* h, nl_phase_times* out) {
   NL_CHECK_READY(h);

@@ -94,6 +94,7 @@ EXPORTS = [
     "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_selftest_tc_update", "nl_ba_cost_noalloc",
     "nl_adjoint", "nl_lm_solve_batch", "nl_set_timing_detail", "nl_set_solver_kind", "nl_solver_set_kind", "nl_permute_rcm_u", "nl_get_user2internal_u", "nl_rcm_order",
     "nl_set_wait_limit", "nl_check_wait_timeout", "nl_unroll_record", "nl_unroll_adjoint",
+    "nl_batch_create", "nl_batch_destroy", "nl_batch_autotune", "nl_batch_lm_solve",
     "nl_status_string",
     "nl_version",
 ]
@@ -132,6 +133,10 @@ def load(build_if_missing: bool = True):
     L.nl_ba_cost_noalloc.argtypes = [i, i, vp, vp, vp, vp, vp, vp, d, d, d, vp, vp]
     L.nl_set_wait_limit.argtypes = [vp, C.c_longlong]
     L.nl_unroll_record.argtypes = [vp, i, vp, C.POINTER(UnrollReport)]
+    L.nl_batch_create.argtypes = [C.POINTER(vp), i, C.POINTER(vp)]
+    L.nl_batch_destroy.argtypes = [vp]
+    L.nl_batch_autotune.argtypes = [vp, C.POINTER(LMSettings), C.POINTER(i), C.POINTER(i)]
+    L.nl_batch_lm_solve.argtypes = [vp, C.POINTER(LMSettings), i, i, vp, vp, C.POINTER(d)]
     L.nl_unroll_adjoint.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.POINTER(UnrollReport)]
     L.nl_check_wait_timeout.argtypes = [vp]
     for name in EXPORTS:  # fails loudly if the library lacks an entry point
@@ -422,6 +427,52 @@ def lm_solve_batch(problems, settings=None):
     _chk(L, L.nl_lm_solve_batch(hs, n, C.byref(s), C.cast(reps, C.c_void_p), _p(lat)), "nl_lm_solve_batch")
     return ([REASONS[r.reason] for r in reps], np.array([r.chi2 for r in reps]),
             np.array([r.iterations for r in reps]), lat)
+
+
+class PersistentBatch:
+    """nl_batch_*: many BAProblemGPU handles solved by one persistent launch
+    (a device work queue over the problems, one CTA per problem at a time,
+    FP64).  Results are written back to the handles."""
+
+    def __init__(self, problems):
+        self.L = load()
+        self.problems = list(problems)
+        n = len(self.problems)
+        hs = (C.c_void_p * n)(*[p.h for p in self.problems])
+        b = C.c_void_p()
+        _chk(self.L, self.L.nl_batch_create(hs, n, C.byref(b)), "nl_batch_create")
+        self.b = b
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.L.nl_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def autotune(self, settings=None):
+        """Times every launch shape on this batch; returns (threads, ctas_per_sm)."""
+        s = settings or LMSettings()
+        nt, cps = C.c_int(), C.c_int()
+        _chk(self.L, self.L.nl_batch_autotune(self.b, C.byref(s), C.byref(nt), C.byref(cps)), "nl_batch_autotune")
+        return nt.value, cps.value
+
+    def lm_solve(self, settings=None, threads=0, ctas_per_sm=0):
+        """Returns (reasons, final chi2, iterations, per-problem latency ms,
+        per-problem solve ms, launch device ms)."""
+        n = len(self.problems)
+        s = settings or LMSettings()
+        reps = (SolveReport * n)()
+        lat = np.zeros(n)
+        dms = C.c_double()
+        _chk(self.L, self.L.nl_batch_lm_solve(self.b, C.byref(s), threads, ctas_per_sm, C.cast(reps, C.c_void_p),
+                                              _p(lat), C.byref(dms)), "nl_batch_lm_solve")
+        return ([REASONS[r.reason] for r in reps], np.array([r.chi2 for r in reps]),
+                np.array([r.iterations for r in reps]), lat, np.array([r.device_ms for r in reps]), dms.value)
 
 
 def selftest_tc_update(ntiles=8, seed=1, device=0) -> float:

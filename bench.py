@@ -22,6 +22,9 @@ computeIncrement + oplus + cost + gain ratio, then the Jacobian pass.
 
 --config 1 (or 0) runs the same measurement on that workload: config 1 is 200
 9-parameter cameras, 50,000 points, 375 k observations (S 1,800 x 1,800).
+--config 3 times the batched configuration (256 uneven problems in one
+persistent launch).  The default config-2 run also carries compact config-1
+and config-3 figures under other_configs (--no-extras skips them).
 
 --impl reference times the FP64 CPU oracle (the restatement of the reference's
 CPU path) on the same workload; under torchrun only rank 0 runs it.
@@ -250,60 +253,140 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def run_batch(args, rank, world):
-    """Config 3: 256 independent uneven problems solved together
-    (nl_lm_solve_batch); problems/s over the batch and per-problem latency."""
-    import torch
+def measure_batch(its, warmup, device, cpu=True, nprob=256):
+    """Config 3: `nprob` independent uneven problems.  The product path is the
+    persistent launch (nl_batch_lm_solve: one kernel, a device work queue, one
+    CTA per problem; launch shape from nl_batch_autotune); the per-problem
+    CUDA-graph path (nl_lm_solve_batch) is timed beside it.  problems/s over
+    the batch (device time of the launch) and per-problem latency."""
     from nelson_b200 import native as N
     from nelson_b200.problems import make_batch
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-    probs = make_batch(256)
-    its = args.steps
-    hs = [N.BAProblemGPU.from_ba(p, precision=N.PREC_MIXED, device=torch.cuda.current_device()) for p in probs]
-    for _ in range(args.warmup):
-        N.lm_solve_batch(hs, N.LMSettings(maxNumIt=its))
+    probs = make_batch(nprob)
+    # the handles carry structure and parameters; the persistent solve is FP64 whatever their precision
+    hs = [N.BAProblemGPU.from_ba(p, precision=N.PREC_MIXED, device=device) for p in probs]
+    b = N.PersistentBatch(hs)
+    s = N.LMSettings(maxNumIt=its)
+
+    def reset():
         for g, p in zip(hs, probs):
             g.set_params(p.cams, p.pts)
-    clocks = Clocks(torch.cuda.current_device())
+
+    nt, cps = b.autotune(s)
+    for _ in range(warmup):
+        reset()
+        b.lm_solve(s)
+    reset()
+    clocks = Clocks(device)
     clocks.start()
-    torch.cuda.synchronize()
     clocks.begin()
-    t0 = time.perf_counter()
-    reasons, chi2, iters, lat = N.lm_solve_batch(hs, N.LMSettings(maxNumIt=its))
-    wall = time.perf_counter() - t0
+    reasons, chi2, iters, lat, solve_ms, dev_ms = b.lm_solve(s)
     clocks.end()
     ck = clocks.stop()
-    span_ms = float(lat.max())
-    cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    # e2e: parameters uploaded from host buffers, the launch, results read back
+    import ctypes as C
+    L = N.load()
+    t0 = time.perf_counter()
+    for g, p in zip(hs, probs):
+        assert L.nl_set_params(g.h, N._p(np.ascontiguousarray(p.cams)), N._p(np.ascontiguousarray(p.pts))) == 0
+    b.lm_solve(s)
+    outs = [g.get_params() for g in hs]
+    e2e_s = time.perf_counter() - t0
+    h2d = sum(p.cams.size + p.pts.size for p in probs) * 8
+    d2h = sum(c.size + q.size for c, q in outs) * 8
+    b.close()
+    # the per-problem graph path on the same (mixed) handles, for comparison
+    reset()
+    N.lm_solve_batch(hs, s)
+    reset()
+    _, _, _, lat_g = N.lm_solve_batch(hs, s)
+    for g in hs:
+        g.close()
+    out = {"metric": "problems/s (batched uneven problems, LM)", "value": nprob / (dev_ms / 1e3),
+           "unit": "problems/s", "steps": its, "dtype": "f64",
+           "config": {"workload": f"config 3: {nprob} problems, cams U{{8..64}} (6-param), pts U{{200..4000}}, "
+                                  f"k~U{{3..8}}, {its} LM iterations each", "launch": "one persistent kernel",
+                      "autotuned": {"threads": nt, "ctas_per_sm": cps}},
+           "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                          "max": float(lat.max())},
+           "solve_ms": {"p50": float(np.percentile(solve_ms, 50)), "p99": float(np.percentile(solve_ms, 99))},
+           "launch_ms": dev_ms,
+           "e2e": {"value": nprob / e2e_s, "unit": "problems/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                   "step": "parameter upload + nl_batch_lm_solve + parameter download"},
+           "graph_path": {"value": nprob / (float(lat_g.max()) / 1e3), "unit": "problems/s",
+                          "note": "nl_lm_solve_batch: per-problem captured sub-iteration graphs interleaved over streams "
+                                  "(mixed precision)"},
+           "converged_or_stopped": {k: int(v) for k, v in zip(*np.unique(reasons, return_counts=True))},
+           "clocks": ck, "cpu_baseline": None}
+    if cpu:
         from oracle.oracle import LMSettings as OLM
         from oracle.oracle import Oracle
         cores = len(os.sched_getaffinity(0))
         t1 = time.perf_counter()
-        nsample = 0
+        nsample, worst = 0, 0.0
         while nsample < len(probs) and time.perf_counter() - t1 < 15.0:
             o = Oracle.from_ba(probs[nsample], threads=cores)
             o.lm_solve(OLM(maxNumIt=its))
+            worst = max(worst, abs(o.chi2() - chi2[nsample]) / o.chi2())
             nsample += 1
         dt = time.perf_counter() - t1
-        cpu = {"value": nsample / dt, "unit": "problems/s", "cores": cores, "kind": "port",
-               "sample": f"{nsample} of the 256 problems, {its} LM iterations each, one after another "
-                         f"(FP64 C++/OpenMP oracle, {dt:.1f} s)"}
-    for g in hs:
+        out["cpu_baseline"] = {"value": nsample / dt, "unit": "problems/s", "cores": cores, "kind": "port",
+                               "sample": f"{nsample} of the {nprob} problems, {its} LM iterations each, one after "
+                                         f"another (FP64 C++/OpenMP oracle, {dt:.1f} s)"}
+        out["oracle_parity"] = {"problems_compared": nsample, "final_chi2_max_rel_err": worst, "bound": 1e-9,
+                                "ok": bool(worst <= 1e-9)}
+    return out
+
+
+def measure_single(cfg, its, warmup, device):
+    """A compact line for another single-problem configuration (config 1:
+    the plain FP64 GPU path against the CPU reference): mixed and FP64 LM
+    iterations/s (device time), the oracle's full K-iteration solve as the CPU
+    baseline, and the per-sub-iteration parity of both GPU traces."""
+    from nelson_b200 import native as N
+    from nelson_b200.problems import make_config
+    from oracle.oracle import LMSettings as OLM
+    from oracle.oracle import Oracle
+    prob = make_config(cfg)
+    out = {"config": workload_config(cfg, 1.0, prob, 1)}
+    traces = {}
+    for name, prec in (("mixed", N.PREC_MIXED), ("fp64_gpu", N.PREC_FP64)):
+        g = N.BAProblemGPU.from_ba(prob, precision=prec, device=device)
+        g.lm_solve(N.LMSettings(maxNumIt=warmup), trace_cap=0)
+        g.set_params(prob.cams, prob.pts)
+        _, tr, it, _, rep = g.lm_solve(N.LMSettings(maxNumIt=its), trace_cap=4096, report=True)
+        out[name] = {"value": max(it, 1) / (rep["device_ms"] / 1e3), "unit": UNIT, "final_chi2": rep["chi2"]}
+        traces[name] = tr
         g.close()
+    cores = len(os.sched_getaffinity(0))
+    o = Oracle.from_ba(prob, threads=cores)
+    t0 = time.perf_counter()
+    _, tro, its_o, _ = o.lm_solve(OLM(maxNumIt=its))
+    dt = time.perf_counter() - t0
+    out["cpu_baseline"] = {"value": max(its_o, 1) / dt, "unit": UNIT, "cores": cores, "kind": "port",
+                           "sample": f"the full {its_o}-iteration LM solve (FP64 C++/OpenMP oracle, {dt:.1f} s)"}
+    pm, pd = trace_parity(traces["mixed"], tro), trace_parity(traces["fp64_gpu"], tro)
+    out["oracle_parity"] = {"records_compared": pd["records"], "fp64_gpu": {k: pd[k] for k in ("chi2", "mu", "rho")},
+                            "mixed": {k: pm[k] for k in ("chi2", "mu", "rho")},
+                            "ok": bool(pd["chi2"] <= 1e-9 and pm["chi2"] <= 1e-6 and pd["records"] > 0)}
+    out["fp64_gpu_vs_cpu"] = out["fp64_gpu"]["value"] / out["cpu_baseline"]["value"]
+    return out
+
+
+def run_batch(args, rank, world):
+    """--config 3: the batched configuration as the bench line."""
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    ranks = Ranks(world, "nccl", torch.device("cuda", local))
+    ranks.barrier()
+    out = measure_batch(args.steps, args.warmup, local, cpu=(rank == 0 and not args.no_cpu_baseline))
+    v = ranks.total_rate(256, 256 / out["value"])
+    ranks.close()
     if rank == 0:
-        line = {"metric": "problems/s (batched uneven problems, LM)", "value": len(probs) / (span_ms / 1e3),
-                "unit": "problems/s", "n_gpus": world, "steps": its, "warmup": args.warmup,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32 (FP64 refinement residual, solve accumulators, cost)", "data": "synthetic (seeded, config-3 generator)",
-                "config": {"workload": "config 3: 256 problems, cams U{8..64} (6-param), pts U{200..4000}, "
-                                       f"k~U{{3..8}}, {its} LM iterations each"},
-                "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                               "max": span_ms},
-                "host_wall_s": wall, "converged_or_stopped": dict(zip(*np.unique(reasons, return_counts=True))),
-                "cpu_baseline": cpu, "clocks": ck}
-        line["converged_or_stopped"] = {k: int(v) for k, v in line["converged_or_stopped"].items()}
-        print(json.dumps(line), flush=True)
+        out.update({"value": v, "n_gpus": world, "warmup": args.warmup, "higher_is_better": True,
+                    "scaling": "weak", "vs_baseline": None, "data": "synthetic (seeded, config-3 generator)",
+                    "gpu_launches": 1})
+        print(json.dumps(out), flush=True)
 
 
 def main():
@@ -317,6 +400,8 @@ def main():
     ap.add_argument("--cpu-iters", type=int, default=0,
                     help="LM iterations of the CPU baseline sample (0: all K for configs 0 / 1, 2 for config 2)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the config-1 and config-3 figures of the default config-2 run")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_env()
@@ -490,6 +575,12 @@ def main():
                   "bounds": {"fp64_chi2": 1e-9, "mixed_chi2": 1e-6},
                   "ok": bool(pd["chi2"] <= 1e-9 and pm["chi2"] <= 1e-6 and pd["records"] > 0)}
 
+    # ---- the other configurations' headline figures, on rank 0 of a 1-GPU run ----
+    others = None
+    if rank == 0 and world == 1 and args.config == 2 and not args.no_extras:
+        others = {"config1": measure_single(1, args.steps, 3, local),
+                  "config3": measure_batch(10, 3, local, cpu=not args.no_cpu_baseline)}
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_m / its_m, "higher_is_better": True, "scaling": "weak",
@@ -504,7 +595,7 @@ def main():
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "step": f"upload + nl_lm_solve({args.steps} its) + download"},
                 "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "clocks": ck,
-                "envelope_solver": envelope}
+                "envelope_solver": envelope, "other_configs": others}
         print(json.dumps(line), flush=True)
     gm.close()
     gd.close()

@@ -1,6 +1,7 @@
 // schur_core.cu -- SolverCholeskySchur on the device (see schur_core.cuh).
 #include <cstring>
 
+#include "potrf_blocked.cuh"
 #include "schur_core.cuh"
 
 namespace nl {
@@ -215,6 +216,7 @@ class SchurCoreT final : public SchurCore {
     NL_CUDA(cudaFuncSetAttribute(trsv_bwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsv_smem<T>()));
     NL_CUDA(cudaFuncSetAttribute(trsm_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmTileSmem));
     NL_CUDA(cudaFuncSetAttribute(diag_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * (int)kDiagUpdSmem));
+    NL_CUDA(cudaFuncSetAttribute(potrf32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPotrf32Smem));
     if (!ev_[0]) {
       for (auto& e : ev_) NL_CUDA(cudaEventCreate(&e));
       NL_CUDA(cudaEventCreateWithFlags(&ev_panel_, cudaEventDisableTiming));
@@ -450,8 +452,8 @@ class SchurCoreT final : public SchurCore {
       const int e = 8 * nT + 2 * j;  // timing events after the update events
       if (tmc) cudaEventRecord(upd_ev_[e], st_);
       // a programmatic dependent of the diagonal update before it
-      NL_CUDA(launch_chain(potrf_diag_kernel<T>, 1, PT, kPotrfSmem, j > 0 && !tmc, S_.as<T>(), ld_, j,
-                           Linv_.as<T>(), status, active));
+      NL_CUDA(launch_chain(potrf32_kernel, 1, kPotrf32Threads, kPotrf32Smem, j > 0 && !tmc, S, ld_, j,
+                           reinterpret_cast<float*>(Linv_.p), status, active));
       if (tmc) cudaEventRecord(upd_ev_[e + 1], st_);
       npev = j + 1;
       launches++;
@@ -884,6 +886,84 @@ __global__ void selftest_fill_kernel(float* S, size_t n, unsigned long long seed
 }
 }  // namespace
 }  // namespace nl
+
+namespace nl {
+namespace {
+// A = B B' / NB + I for a random B (SPD, well conditioned), FP32, NB x NB row-major.
+__global__ void selftest_spd_kernel(const float* B, float* A) {
+  const int r = blockIdx.x, c = threadIdx.x;
+  float s = 0.f;
+  for (int m = 0; m < NB; m++) s += B[r * NB + m] * B[c * NB + m];
+  A[r * NB + c] = s / NB + (r == c ? 1.f : 0.f);
+}
+}  // namespace
+}  // namespace nl
+
+extern "C" nl_status nl_selftest_potrf32(unsigned long long seed, int device, double* err_l, double* err_inv,
+                                         double* us_blocked, double* us_rank4) {
+  using namespace nl;
+  if (!err_l || !err_inv) return NL_ERR_ARG;
+  NL_CUDA(cudaSetDevice(device));
+  const size_t n = (size_t)NB * NB;
+  DevBuf b, a, a1, a2, x1, x2, st;
+  nl_status r;
+  if ((r = b.alloc(n * 4)) != NL_OK || (r = a.alloc(n * 4)) != NL_OK || (r = a1.alloc(n * 4)) != NL_OK ||
+      (r = a2.alloc(n * 4)) != NL_OK || (r = x1.alloc(n * 4)) != NL_OK || (r = x2.alloc(n * 4)) != NL_OK ||
+      (r = st.alloc(16)) != NL_OK)
+    return r;
+  NL_CUDA(cudaFuncSetAttribute(potrf32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPotrf32Smem));
+  NL_CUDA(cudaMemset(st.p, 0, 16));
+  NL_CUDA(cudaMemset(x1.p, 0, n * 4));
+  NL_CUDA(cudaMemset(x2.p, 0, n * 4));
+  selftest_fill_kernel<<<(unsigned)((n + 255) / 256), 256>>>(b.as<float>(), n, seed);
+  selftest_spd_kernel<<<NB, NB>>>(b.as<float>(), a.as<float>());
+  NL_CUDA(cudaMemcpy(a1.p, a.p, n * 4, cudaMemcpyDeviceToDevice));
+  NL_CUDA(cudaMemcpy(a2.p, a.p, n * 4, cudaMemcpyDeviceToDevice));
+  potrf32_kernel<<<1, kPotrf32Threads, kPotrf32Smem>>>(a1.as<float>(), NB, 0, x1.as<float>(), st.as<int>(), nullptr);
+  potrf_diag_kernel<float><<<1, PT, kPotrfSmem>>>(a2.as<float>(), NB, 0, x2.as<float>(), st.as<int>(), nullptr);
+  NL_CUDA(cudaGetLastError());
+  NL_CUDA(cudaDeviceSynchronize());
+  int stat = 0;
+  NL_CUDA(cudaMemcpy(&stat, st.p, 4, cudaMemcpyDeviceToHost));
+  if (stat) return NL_ERR_NOT_SPD;
+  std::vector<float> l1(n), l2(n), i1(n), i2(n);
+  NL_CUDA(cudaMemcpy(l1.data(), a1.p, n * 4, cudaMemcpyDeviceToHost));
+  NL_CUDA(cudaMemcpy(l2.data(), a2.p, n * 4, cudaMemcpyDeviceToHost));
+  NL_CUDA(cudaMemcpy(i1.data(), x1.p, n * 4, cudaMemcpyDeviceToHost));
+  NL_CUDA(cudaMemcpy(i2.data(), x2.p, n * 4, cudaMemcpyDeviceToHost));
+  double dl = 0, ml = 0, di = 0, mi = 0;
+  for (int i = 0; i < NB; i++)
+    for (int j = 0; j <= i; j++) {
+      dl = std::max(dl, (double)std::fabs(l1[i * NB + j] - l2[i * NB + j]));
+      ml = std::max(ml, (double)std::fabs(l2[i * NB + j]));
+      di = std::max(di, (double)std::fabs(i1[i * NB + j] - i2[i * NB + j]));
+      mi = std::max(mi, (double)std::fabs(i2[i * NB + j]));
+    }
+  *err_l = dl / std::max(ml, 1e-300);
+  *err_inv = di / std::max(mi, 1e-300);
+  // device time per launch, 20 back-to-back launches each
+  cudaEvent_t e[3];
+  for (auto& x : e) NL_CUDA(cudaEventCreate(&x));
+  NL_CUDA(cudaEventRecord(e[0]));
+  for (int it = 0; it < 20; it++) {
+    NL_CUDA(cudaMemcpyAsync(a1.p, a.p, n * 4, cudaMemcpyDeviceToDevice));
+    potrf32_kernel<<<1, kPotrf32Threads, kPotrf32Smem>>>(a1.as<float>(), NB, 0, x1.as<float>(), st.as<int>(), nullptr);
+  }
+  NL_CUDA(cudaEventRecord(e[1]));
+  for (int it = 0; it < 20; it++) {
+    NL_CUDA(cudaMemcpyAsync(a2.p, a.p, n * 4, cudaMemcpyDeviceToDevice));
+    potrf_diag_kernel<float><<<1, PT, kPotrfSmem>>>(a2.as<float>(), NB, 0, x2.as<float>(), st.as<int>(), nullptr);
+  }
+  NL_CUDA(cudaEventRecord(e[2]));
+  NL_CUDA(cudaEventSynchronize(e[2]));
+  float t1 = 0, t2 = 0;
+  cudaEventElapsedTime(&t1, e[0], e[1]);
+  cudaEventElapsedTime(&t2, e[1], e[2]);
+  for (auto& x : e) cudaEventDestroy(x);
+  if (us_blocked) *us_blocked = 1e3 * t1 / 20;
+  if (us_rank4) *us_rank4 = 1e3 * t2 / 20;
+  return NL_OK;
+}
 
 extern "C" nl_status nl_selftest_tc_update(int ntiles, unsigned long long seed, int device, double* max_rel_err) {
   using namespace nl;

@@ -408,6 +408,7 @@ class SolverCholeskySchurCudaHost {
     int kind = NL_SOLVER_DENSE;
   };
   Settings& settings() { return settings_; }
+  const Settings& settings() const { return settings_; }
 
   SolverCholeskySchurCudaHost() = default;
   SolverCholeskySchurCudaHost(const SolverCholeskySchurCudaHost&) = delete;

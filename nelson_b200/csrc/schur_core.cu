@@ -3,6 +3,7 @@
 
 #include "potrf_blocked.cuh"
 #include "schur_core.cuh"
+#include "trsv_fold.cuh"
 
 namespace nl {
 
@@ -156,6 +157,8 @@ class SchurCoreT final : public SchurCore {
     NL_CUDA(cudaMemcpyAsync(env_dev_.as<int>() + ntiles_, env_last_.data(), sizeof(int) * ntiles_,
                             cudaMemcpyHostToDevice, st_));
     NL_TRY(flags_.alloc(sizeof(int) * (size_t)(ntiles_ + 1)));
+    NL_TRY(Mf_.alloc(sizeof(T) * (size_t)ntiles_ * NB * NB));
+    NL_TRY(Pb_.alloc(sizeof(T) * (size_t)ntiles_ * NB * NB));
     NL_TRY(S_.alloc(sizeof(T) * (size_t)ld_ * ld_));
     need_s0_ = refine_sweeps > 0 || keep_schur;
     if (need_s0_) NL_TRY(S0_.alloc(sizeof(T) * (size_t)ld_ * ld_));
@@ -217,6 +220,11 @@ class SchurCoreT final : public SchurCore {
     NL_CUDA(cudaFuncSetAttribute(trsm_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmTileSmem));
     NL_CUDA(cudaFuncSetAttribute(diag_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * (int)kDiagUpdSmem));
     NL_CUDA(cudaFuncSetAttribute(potrf32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPotrf32Smem));
+    NL_CUDA(cudaFuncSetAttribute(trsv_fwd_fold_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)trsv_smem<T>()));
+    NL_CUDA(cudaFuncSetAttribute(trsv_bwd_fold_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)trsv_smem<T>()));
+    NL_CUDA(cudaFuncSetAttribute(fold_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fold_smem<T>()));
     if (!ev_[0]) {
       for (auto& e : ev_) NL_CUDA(cudaEventCreate(&e));
       NL_CUDA(cudaEventCreateWithFlags(&ev_panel_, cudaEventDisableTiming));
@@ -241,18 +249,27 @@ class SchurCoreT final : public SchurCore {
     return NL_OK;
   }
 
-  // ---- solves with the factor: x = S^-1 b (trsv fwd + bwd) ----
+  // ---- the factor's folded tiles for the solves (trsv_fold.cuh) ----
+  nl_status enqueue_fold(const int* active) {
+    if (ntiles_ < 2) return NL_OK;
+    fold_kernel<T><<<2 * (ntiles_ - 1), 256, fold_smem<T>(), st_>>>(S_.as<T>(), ld_, Linv_.as<T>(), ntiles_,
+                                                                    Mf_.as<T>(), Pb_.as<T>(), active);
+    launches++;
+    return NL_OK;
+  }
+
+  // ---- solves with the factor: x = S^-1 b (forward + backward sweeps) ----
   nl_status enqueue_solve(const double* b, double* x, int* status, const int* active) {
-    NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
     const int* env = envelope ? env_dev_.as<int>() : nullptr;
-    trsv_fwd_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), b, y_.as<double>(),
-                                                 flags_.as<int>(), flags_.as<int>() + 1, 1, status, wait_limit, env,
-                                                 active);
-    NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
-    trsv_bwd_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), y_.as<double>(), x,
-                                                 flags_.as<int>(), flags_.as<int>() + 1, 1, status, wait_limit, env,
-                                                 active);
-    launches += 2;
+    unsolved_fill_kernel<<<cdiv(ld_, 256), 256, 0, st_>>>(y_.as<double>(), x, ld_, flags_.as<int>(), active);
+    trsv_fwd_fold_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(),
+                                                                  Mf_.as<T>(), b, y_.as<double>(), flags_.as<int>(),
+                                                                  status, wait_limit, env, active);
+    trsv_bwd_fold_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(),
+                                                                  Pb_.as<T>(), y_.as<double>(), x,
+                                                                  flags_.as<int>() + 1, status, wait_limit, env,
+                                                                  active);
+    launches += 3;
     return NL_OK;
   }
 
@@ -264,12 +281,14 @@ class SchurCoreT final : public SchurCore {
   // L and Linv).
   nl_status enqueue_solve_withheld(int* status) override {
     if (ntiles_ < 2) return NL_ERR_STATE;
-    NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
+    unsolved_fill_kernel<<<cdiv(ld_, 256), 256, 0, st_>>>(y_.as<double>(), dx_.as<double>(), ld_, flags_.as<int>(),
+                                                          nullptr);
     set_int_kernel<<<1, 1, 0, st_>>>(flags_.as<int>(), 1);
-    trsv_fwd_kernel<T><<<ntiles_ - 1, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), bS_.as<double>(),
-                                                     y_.as<double>(), flags_.as<int>(), flags_.as<int>() + 1, 1,
-                                                     status, wait_limit, nullptr, nullptr);
-    launches += 2;
+    trsv_fwd_fold_kernel<T><<<ntiles_ - 1, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(),
+                                                                      Mf_.as<T>(), bS_.as<double>(), y_.as<double>(),
+                                                                      flags_.as<int>(), status, wait_limit, nullptr,
+                                                                      nullptr);
+    launches += 3;
     NL_CUDA(cudaGetLastError());
     return NL_OK;
   }
@@ -661,6 +680,7 @@ class SchurCoreT final : public SchurCore {
     if (s != NL_OK) return s;
     if (tm) NL_CUDA(cudaEventRecord(ev_[4], st_));
     NvtxRange rs("nl:solve+backsub");
+    if ((s = enqueue_fold(active)) != NL_OK) return s;
     if ((s = enqueue_solve(bS_.as<double>(), incU, status, active)) != NL_OK) return s;
     for (int it = 0; it < refine_sweeps && need_s0_; it++) {
       symv_partial_kernel<T, kSymvChunks><<<dim3(ntiles_, kSymvChunks), SV, 0, st_>>>(
@@ -812,6 +832,7 @@ class SchurCoreT final : public SchurCore {
   bool need_s0_ = false;
   SchurDev d_{};
   DevBuf U_, V_, W_, Y_, Vinv_, bU_, bV_, bS_, incU_, incV_, y_, r_, dx_, part_, Linv_, flags_, S_, S0_, tcs_;
+  DevBuf Mf_, Pb_;  // folded tiles of the solves: inv(L_II) L_I,I-1 and inv(L_II)' L_I+1,I'
   // envelope of S (host) and its first / last arrays on the device (solves)
   std::vector<int> env_first_, env_last_, env_run_;
   DevBuf env_dev_;

@@ -13,6 +13,7 @@ constexpr int kNT = 256;
 constexpr int kRedCTAs = 296;  // 2 x 148 SMs for grid-stride reductions
 constexpr int kSymvChunks = 8;
 constexpr int kSchurWarps = 8;
+constexpr int kSchurGroup = 32;  // cameras per group of the Schur work order
 
 inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 
@@ -109,11 +110,19 @@ class SchurCoreT final : public SchurCore {
       for (int k = env_first_[t]; k < t; k++) env_last_[k] = std::max(env_last_[k], t);
     env_run_.assign(ntiles_, 0);
     for (int k = 0; k < ntiles_; k++) env_run_[k] = std::max(env_last_[k], k > 0 ? env_run_[k - 1] : 0);
-    // Schur work order: output blocks by pair count, heaviest first
+    // Schur work order: output blocks in groups of kSchurGroup consecutive
+    // (internal) first cameras i, each group heaviest first.  Within a group
+    // the long diagonal blocks start early, so the tail stays short, and the
+    // Y rows of the group's cameras and the W rows of their neighbours are
+    // reused from L2 by the group's blocks instead of being fetched again from
+    // DRAM by blocks far apart in time.
     std::vector<int> s_order(std::max(nS_, 1), 0);
     for (int b = 0; b < nS_; b++) s_order[b] = b;
-    std::stable_sort(s_order.begin(), s_order.begin() + nS_,
-                     [&](int x, int y) { return s_ptr[x + 1] - s_ptr[x] > s_ptr[y + 1] - s_ptr[y]; });
+    std::stable_sort(s_order.begin(), s_order.begin() + nS_, [&](int x, int y) {
+      const int gx = s_i[x] / kSchurGroup, gy = s_i[y] / kSchurGroup;
+      if (gx != gy) return gx < gy;
+      return s_ptr[x + 1] - s_ptr[x] > s_ptr[y + 1] - s_ptr[y];
+    });
     std::vector<int> pa(std::max<long long>(npairs, 1)), pb(std::max<long long>(npairs, 1));
     {
       std::vector<long long> fill(s_ptr.begin(), s_ptr.end() - 1);

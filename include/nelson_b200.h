@@ -379,15 +379,6 @@ nl_status nl_solver_set_kind(nl_solver* s, int kind);
  * (No counterpart in the reference: it checks the B200 kernel itself.) */
 nl_status nl_selftest_tc_update(int ntiles, unsigned long long seed, int device, double* max_rel_err);
 
-/* Device self-test of the mixed path's diagonal-tile factor: factors one
- * random SPD 128 x 128 FP32 tile with the 32-blocked kernel the factorisation
- * uses and with the rank-4 register kernel (the FP64 path's), and returns the
- * largest difference of L and of inv(L) relative to their largest entry, and
- * each kernel's device time per launch in microseconds (20 launches, each
- * after a 64 KB copy of the tile).  (No counterpart in the reference.) */
-nl_status nl_selftest_potrf32(unsigned long long seed, int device, double* err_l, double* err_inv,
-                              double* us_blocked, double* us_rank4);
-
 /* ---- cost without any device allocation ---------------------------------- */
 /* No counterpart in the reference.  The FP64 cost chi2 = sum_e w_e |r_e|^2 of
  * the projection edges (the value nl_update reports), for callers that must

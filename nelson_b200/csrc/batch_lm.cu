@@ -329,36 +329,92 @@ __device__ bool compute_increment(const BProb& P, double mu, double* smem, int* 
 #pragma unroll
       for (int i = 0; i < BC; i++) P.bS[(size_t)c * BC + i] = -P.bU[(size_t)c * BC + i] - s[i];
   }
-  // S blocks: M = U_ij - sum_pairs Y_a W_b', lane l owns entries l, l + 32, ...
+  // S blocks: M = U_ij - sum_pairs Y_a W_b'
   constexpr int NE = BC * BC;
-  constexpr int NPL = (NE + 31) / 32;
   for (int b = warp; b < P.nS; b += nw) {
     const int bi = P.s_i[b], bj = P.s_j[b];
-    double acc[NPL];
+    const int t0 = P.s_ptr[b], t1 = P.s_ptr[b + 1];
+    if (BC == 6) {
+      // lane l takes pairs l, l + 32, ... and accumulates the whole 6 x 6
+      // product (32 pairs' loads in flight per warp); the lanes' sums are then
+      // added by a butterfly, so the order depends on the pair count alone
+      double acc[NE];
 #pragma unroll
-    for (int q = 0; q < NPL; q++) acc[q] = 0.0;
-    for (int t = P.s_ptr[b]; t < P.s_ptr[b + 1]; t++) {
-      const double* Ya = P.Y + (size_t)P.pa[t] * (BC * 3);
-      const double* Wb = P.W + (size_t)P.pb[t] * (BC * 3);
+      for (int q = 0; q < NE; q++) acc[q] = 0.0;
+      for (int t = t0 + lane; t < t1; t += 32) {
+        const double2* Ya = reinterpret_cast<const double2*>(P.Y + (size_t)P.pa[t] * (BC * 3));
+        const double2* Wb = reinterpret_cast<const double2*>(P.W + (size_t)P.pb[t] * (BC * 3));
+        double y[BC * 3], w[BC * 3];
+#pragma unroll
+        for (int q = 0; q < BC * 3 / 2; q++) {
+          const double2 a = Ya[q], c = Wb[q];
+          y[2 * q] = a.x;
+          y[2 * q + 1] = a.y;
+          w[2 * q] = c.x;
+          w[2 * q + 1] = c.y;
+        }
+#pragma unroll
+        for (int r = 0; r < BC; r++)
+#pragma unroll
+          for (int c = 0; c < BC; c++)
+            acc[r * BC + c] += y[r * 3] * w[c * 3] + y[r * 3 + 1] * w[c * 3 + 1] + y[r * 3 + 2] * w[c * 3 + 2];
+      }
+#pragma unroll
+      for (int q = 0; q < NE; q++) {
+        const double v = warp_all_sum(acc[q]);
+        if (lane == (q & 31)) {
+          const int r = q / BC, c = q % BC;
+          double m = -v;
+          if (bi == bj) m += P.U[(size_t)bi * NE + q];
+          // block (i, j) of the upper S at lower (j BC + c, i BC + r)
+          const int row = bj * BC + c, col = bi * BC + r;
+          if (col <= row) P.S[(size_t)row * n + col] = m;
+        }
+      }
+    } else {
+      // lane l owns entries l, l + 32, ...; four pairs' loads are issued
+      // before their products
+      constexpr int NPL = (NE + 31) / 32;
+      double acc[NPL];
+#pragma unroll
+      for (int q = 0; q < NPL; q++) acc[q] = 0.0;
+      int ra[NPL], ca[NPL];
+#pragma unroll
+      for (int q = 0; q < NPL; q++) {
+        const int idx = min(lane + 32 * q, NE - 1);
+        ra[q] = idx / BC;
+        ca[q] = idx - (idx / BC) * BC;
+      }
+      for (int t = t0; t < t1; t += 4) {
+        double yv[4][NPL][3], wv[4][NPL][3];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const bool in = t + u < t1;
+          const double* Ya = P.Y + (size_t)(in ? P.pa[t + u] : P.pa[t0]) * (BC * 3);
+          const double* Wb = P.W + (size_t)(in ? P.pb[t + u] : P.pb[t0]) * (BC * 3);
+#pragma unroll
+          for (int q = 0; q < NPL; q++)
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+              yv[u][q][k] = in ? Ya[ra[q] * 3 + k] : 0.0;
+              wv[u][q][k] = Wb[ca[q] * 3 + k];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+          for (int q = 0; q < NPL; q++)
+            acc[q] += yv[u][q][0] * wv[u][q][0] + yv[u][q][1] * wv[u][q][1] + yv[u][q][2] * wv[u][q][2];
+      }
 #pragma unroll
       for (int q = 0; q < NPL; q++) {
         const int idx = lane + 32 * q;
         if (idx < NE) {
-          const int r = idx / BC, c = idx - (idx / BC) * BC;
-          acc[q] += Ya[r * 3] * Wb[c * 3] + Ya[r * 3 + 1] * Wb[c * 3 + 1] + Ya[r * 3 + 2] * Wb[c * 3 + 2];
+          double m = -acc[q];
+          if (bi == bj) m += P.U[(size_t)bi * NE + idx];
+          const int row = bj * BC + ca[q], col = bi * BC + ra[q];
+          if (col <= row) P.S[(size_t)row * n + col] = m;
         }
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < NPL; q++) {
-      const int idx = lane + 32 * q;
-      if (idx < NE) {
-        const int r = idx / BC, c = idx - (idx / BC) * BC;
-        double m = -acc[q];
-        if (bi == bj) m += P.U[(size_t)bi * NE + idx];
-        // block (i, j) of the upper S at lower (j BC + c, i BC + r)
-        const int row = bj * BC + c, col = bi * BC + r;
-        if (col <= row) P.S[(size_t)row * n + col] = m;
       }
     }
   }
@@ -442,14 +498,19 @@ __device__ bool compute_increment(const BProb& P, double mu, double* smem, int* 
   for (int k0 = 0; k0 < n; k0 += kPW) {
     const int kb = min(kPW, n - k0);
     if (warp == 0) {
+      // lane i holds row k0 + i of the diagonal block (independent loads first)
+      double lrow[kPW];
+#pragma unroll
+      for (int j = 0; j < kPW; j++) lrow[j] = (lane < kb && j <= lane) ? P.S[(size_t)(k0 + lane) * n + k0 + j] : 0.0;
       double yi = lane < kb ? x[k0 + lane] : 0.0;
-      for (int j = 0; j < kb; j++) {
-        const double lj = P.S[(size_t)(k0 + lane < n ? k0 + lane : k0) * n + k0 + j];
-        double yj = __shfl_sync(0xffffffffu, yi, j);
-        const double djj = __shfl_sync(0xffffffffu, lj, j);
-        yj = yj / djj;
-        if (lane == j) yi = yj;
-        if (lane > j && lane < kb) yi -= lj * yj;
+#pragma unroll
+      for (int j = 0; j < kPW; j++) {
+        if (j < kb) {
+          const double djj = __shfl_sync(0xffffffffu, lrow[j], j);
+          const double yj = __shfl_sync(0xffffffffu, yi, j) / djj;
+          if (lane == j) yi = yj;
+          if (lane > j && lane < kb) yi -= lrow[j] * yj;
+        }
       }
       if (lane < kb) x[k0 + lane] = yi;
     }
@@ -466,14 +527,20 @@ __device__ bool compute_increment(const BProb& P, double mu, double* smem, int* 
   for (int k0 = ((n - 1) / kPW) * kPW; k0 >= 0 && n > 0; k0 -= kPW) {
     const int kb = min(kPW, n - k0);
     if (warp == 0) {
+      // lane i holds column k0 + i of the diagonal block: L[k0 + j][k0 + i], j >= i
+      double lcol[kPW];
+#pragma unroll
+      for (int j = 0; j < kPW; j++)
+        lcol[j] = (lane < kb && j < kb && j >= lane) ? P.S[(size_t)(k0 + j) * n + k0 + lane] : 0.0;
       double yi = lane < kb ? x[k0 + lane] : 0.0;
-      for (int j = kb - 1; j >= 0; j--) {
-        // lane i < j needs L[k0 + j][k0 + i]
-        const double lij = lane < kb ? P.S[(size_t)(k0 + j) * n + k0 + lane] : 0.0;
-        const double djj = __shfl_sync(0xffffffffu, lij, j);
-        double xj = __shfl_sync(0xffffffffu, yi, j) / djj;
-        if (lane == j) yi = xj;
-        if (lane < j) yi -= lij * xj;
+#pragma unroll
+      for (int j = kPW - 1; j >= 0; j--) {
+        if (j < kb) {
+          const double djj = __shfl_sync(0xffffffffu, lcol[j], j);
+          const double xj = __shfl_sync(0xffffffffu, yi, j) / djj;
+          if (lane == j) yi = xj;
+          if (lane < j) yi -= lcol[j] * xj;
+        }
       }
       if (lane < kb) x[k0 + lane] = yi;
     }

@@ -1,9 +1,7 @@
 // schur_core.cu -- SolverCholeskySchur on the device (see schur_core.cuh).
 #include <cstring>
 
-#include "potrf_blocked.cuh"
 #include "schur_core.cuh"
-#include "trsv_fold.cuh"
 
 namespace nl {
 
@@ -13,7 +11,6 @@ constexpr int kNT = 256;
 constexpr int kRedCTAs = 296;  // 2 x 148 SMs for grid-stride reductions
 constexpr int kSymvChunks = 8;
 constexpr int kSchurWarps = 8;
-constexpr int kSchurGroup = 32;  // cameras per group of the Schur work order
 
 inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 
@@ -110,19 +107,11 @@ class SchurCoreT final : public SchurCore {
       for (int k = env_first_[t]; k < t; k++) env_last_[k] = std::max(env_last_[k], t);
     env_run_.assign(ntiles_, 0);
     for (int k = 0; k < ntiles_; k++) env_run_[k] = std::max(env_last_[k], k > 0 ? env_run_[k - 1] : 0);
-    // Schur work order: output blocks in groups of kSchurGroup consecutive
-    // (internal) first cameras i, each group heaviest first.  Within a group
-    // the long diagonal blocks start early, so the tail stays short, and the
-    // Y rows of the group's cameras and the W rows of their neighbours are
-    // reused from L2 by the group's blocks instead of being fetched again from
-    // DRAM by blocks far apart in time.
+    // Schur work order: output blocks by pair count, heaviest first
     std::vector<int> s_order(std::max(nS_, 1), 0);
     for (int b = 0; b < nS_; b++) s_order[b] = b;
-    std::stable_sort(s_order.begin(), s_order.begin() + nS_, [&](int x, int y) {
-      const int gx = s_i[x] / kSchurGroup, gy = s_i[y] / kSchurGroup;
-      if (gx != gy) return gx < gy;
-      return s_ptr[x + 1] - s_ptr[x] > s_ptr[y + 1] - s_ptr[y];
-    });
+    std::stable_sort(s_order.begin(), s_order.begin() + nS_,
+                     [&](int x, int y) { return s_ptr[x + 1] - s_ptr[x] > s_ptr[y + 1] - s_ptr[y]; });
     std::vector<int> pa(std::max<long long>(npairs, 1)), pb(std::max<long long>(npairs, 1));
     {
       std::vector<long long> fill(s_ptr.begin(), s_ptr.end() - 1);
@@ -166,8 +155,6 @@ class SchurCoreT final : public SchurCore {
     NL_CUDA(cudaMemcpyAsync(env_dev_.as<int>() + ntiles_, env_last_.data(), sizeof(int) * ntiles_,
                             cudaMemcpyHostToDevice, st_));
     NL_TRY(flags_.alloc(sizeof(int) * (size_t)(ntiles_ + 1)));
-    NL_TRY(Mf_.alloc(sizeof(T) * (size_t)ntiles_ * NB * NB));
-    NL_TRY(Pb_.alloc(sizeof(T) * (size_t)ntiles_ * NB * NB));
     NL_TRY(S_.alloc(sizeof(T) * (size_t)ld_ * ld_));
     need_s0_ = refine_sweeps > 0 || keep_schur;
     if (need_s0_) NL_TRY(S0_.alloc(sizeof(T) * (size_t)ld_ * ld_));
@@ -228,12 +215,6 @@ class SchurCoreT final : public SchurCore {
     NL_CUDA(cudaFuncSetAttribute(trsv_bwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsv_smem<T>()));
     NL_CUDA(cudaFuncSetAttribute(trsm_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmTileSmem));
     NL_CUDA(cudaFuncSetAttribute(diag_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * (int)kDiagUpdSmem));
-    NL_CUDA(cudaFuncSetAttribute(potrf32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPotrf32Smem));
-    NL_CUDA(cudaFuncSetAttribute(trsv_fwd_fold_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)trsv_smem<T>()));
-    NL_CUDA(cudaFuncSetAttribute(trsv_bwd_fold_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)trsv_smem<T>()));
-    NL_CUDA(cudaFuncSetAttribute(fold_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fold_smem<T>()));
     if (!ev_[0]) {
       for (auto& e : ev_) NL_CUDA(cudaEventCreate(&e));
       NL_CUDA(cudaEventCreateWithFlags(&ev_panel_, cudaEventDisableTiming));
@@ -258,27 +239,18 @@ class SchurCoreT final : public SchurCore {
     return NL_OK;
   }
 
-  // ---- the factor's folded tiles for the solves (trsv_fold.cuh) ----
-  nl_status enqueue_fold(const int* active) {
-    if (ntiles_ < 2) return NL_OK;
-    fold_kernel<T><<<2 * (ntiles_ - 1), 256, fold_smem<T>(), st_>>>(S_.as<T>(), ld_, Linv_.as<T>(), ntiles_,
-                                                                    Mf_.as<T>(), Pb_.as<T>(), active);
-    launches++;
-    return NL_OK;
-  }
-
-  // ---- solves with the factor: x = S^-1 b (forward + backward sweeps) ----
+  // ---- solves with the factor: x = S^-1 b (trsv fwd + bwd) ----
   nl_status enqueue_solve(const double* b, double* x, int* status, const int* active) {
+    NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
     const int* env = envelope ? env_dev_.as<int>() : nullptr;
-    unsolved_fill_kernel<<<cdiv(ld_, 256), 256, 0, st_>>>(y_.as<double>(), x, ld_, flags_.as<int>(), active);
-    trsv_fwd_fold_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(),
-                                                                  Mf_.as<T>(), b, y_.as<double>(), flags_.as<int>(),
-                                                                  status, wait_limit, env, active);
-    trsv_bwd_fold_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(),
-                                                                  Pb_.as<T>(), y_.as<double>(), x,
-                                                                  flags_.as<int>() + 1, status, wait_limit, env,
-                                                                  active);
-    launches += 3;
+    trsv_fwd_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), b, y_.as<double>(),
+                                                 flags_.as<int>(), flags_.as<int>() + 1, 1, status, wait_limit, env,
+                                                 active);
+    NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
+    trsv_bwd_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), y_.as<double>(), x,
+                                                 flags_.as<int>(), flags_.as<int>() + 1, 1, status, wait_limit, env,
+                                                 active);
+    launches += 2;
     return NL_OK;
   }
 
@@ -290,14 +262,12 @@ class SchurCoreT final : public SchurCore {
   // L and Linv).
   nl_status enqueue_solve_withheld(int* status) override {
     if (ntiles_ < 2) return NL_ERR_STATE;
-    unsolved_fill_kernel<<<cdiv(ld_, 256), 256, 0, st_>>>(y_.as<double>(), dx_.as<double>(), ld_, flags_.as<int>(),
-                                                          nullptr);
+    NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
     set_int_kernel<<<1, 1, 0, st_>>>(flags_.as<int>(), 1);
-    trsv_fwd_fold_kernel<T><<<ntiles_ - 1, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(),
-                                                                      Mf_.as<T>(), bS_.as<double>(), y_.as<double>(),
-                                                                      flags_.as<int>(), status, wait_limit, nullptr,
-                                                                      nullptr);
-    launches += 3;
+    trsv_fwd_kernel<T><<<ntiles_ - 1, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), bS_.as<double>(),
+                                                     y_.as<double>(), flags_.as<int>(), flags_.as<int>() + 1, 1,
+                                                     status, wait_limit, nullptr, nullptr);
+    launches += 2;
     NL_CUDA(cudaGetLastError());
     return NL_OK;
   }
@@ -480,8 +450,8 @@ class SchurCoreT final : public SchurCore {
       const int e = 8 * nT + 2 * j;  // timing events after the update events
       if (tmc) cudaEventRecord(upd_ev_[e], st_);
       // a programmatic dependent of the diagonal update before it
-      NL_CUDA(launch_chain(potrf32_kernel, 1, kPotrf32Threads, kPotrf32Smem, j > 0 && !tmc, S, ld_, j,
-                           reinterpret_cast<float*>(Linv_.p), status, active));
+      NL_CUDA(launch_chain(potrf_diag_kernel<T>, 1, PT, kPotrfSmem, j > 0 && !tmc, S_.as<T>(), ld_, j,
+                           Linv_.as<T>(), status, active));
       if (tmc) cudaEventRecord(upd_ev_[e + 1], st_);
       npev = j + 1;
       launches++;
@@ -689,7 +659,6 @@ class SchurCoreT final : public SchurCore {
     if (s != NL_OK) return s;
     if (tm) NL_CUDA(cudaEventRecord(ev_[4], st_));
     NvtxRange rs("nl:solve+backsub");
-    if ((s = enqueue_fold(active)) != NL_OK) return s;
     if ((s = enqueue_solve(bS_.as<double>(), incU, status, active)) != NL_OK) return s;
     for (int it = 0; it < refine_sweeps && need_s0_; it++) {
       symv_partial_kernel<T, kSymvChunks><<<dim3(ntiles_, kSymvChunks), SV, 0, st_>>>(
@@ -841,7 +810,6 @@ class SchurCoreT final : public SchurCore {
   bool need_s0_ = false;
   SchurDev d_{};
   DevBuf U_, V_, W_, Y_, Vinv_, bU_, bV_, bS_, incU_, incV_, y_, r_, dx_, part_, Linv_, flags_, S_, S0_, tcs_;
-  DevBuf Mf_, Pb_;  // folded tiles of the solves: inv(L_II) L_I,I-1 and inv(L_II)' L_I+1,I'
   // envelope of S (host) and its first / last arrays on the device (solves)
   std::vector<int> env_first_, env_last_, env_run_;
   DevBuf env_dev_;
@@ -916,84 +884,6 @@ __global__ void selftest_fill_kernel(float* S, size_t n, unsigned long long seed
 }
 }  // namespace
 }  // namespace nl
-
-namespace nl {
-namespace {
-// A = B B' / NB + I for a random B (SPD, well conditioned), FP32, NB x NB row-major.
-__global__ void selftest_spd_kernel(const float* B, float* A) {
-  const int r = blockIdx.x, c = threadIdx.x;
-  float s = 0.f;
-  for (int m = 0; m < NB; m++) s += B[r * NB + m] * B[c * NB + m];
-  A[r * NB + c] = s / NB + (r == c ? 1.f : 0.f);
-}
-}  // namespace
-}  // namespace nl
-
-extern "C" nl_status nl_selftest_potrf32(unsigned long long seed, int device, double* err_l, double* err_inv,
-                                         double* us_blocked, double* us_rank4) {
-  using namespace nl;
-  if (!err_l || !err_inv) return NL_ERR_ARG;
-  NL_CUDA(cudaSetDevice(device));
-  const size_t n = (size_t)NB * NB;
-  DevBuf b, a, a1, a2, x1, x2, st;
-  nl_status r;
-  if ((r = b.alloc(n * 4)) != NL_OK || (r = a.alloc(n * 4)) != NL_OK || (r = a1.alloc(n * 4)) != NL_OK ||
-      (r = a2.alloc(n * 4)) != NL_OK || (r = x1.alloc(n * 4)) != NL_OK || (r = x2.alloc(n * 4)) != NL_OK ||
-      (r = st.alloc(16)) != NL_OK)
-    return r;
-  NL_CUDA(cudaFuncSetAttribute(potrf32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPotrf32Smem));
-  NL_CUDA(cudaMemset(st.p, 0, 16));
-  NL_CUDA(cudaMemset(x1.p, 0, n * 4));
-  NL_CUDA(cudaMemset(x2.p, 0, n * 4));
-  selftest_fill_kernel<<<(unsigned)((n + 255) / 256), 256>>>(b.as<float>(), n, seed);
-  selftest_spd_kernel<<<NB, NB>>>(b.as<float>(), a.as<float>());
-  NL_CUDA(cudaMemcpy(a1.p, a.p, n * 4, cudaMemcpyDeviceToDevice));
-  NL_CUDA(cudaMemcpy(a2.p, a.p, n * 4, cudaMemcpyDeviceToDevice));
-  potrf32_kernel<<<1, kPotrf32Threads, kPotrf32Smem>>>(a1.as<float>(), NB, 0, x1.as<float>(), st.as<int>(), nullptr);
-  potrf_diag_kernel<float><<<1, PT, kPotrfSmem>>>(a2.as<float>(), NB, 0, x2.as<float>(), st.as<int>(), nullptr);
-  NL_CUDA(cudaGetLastError());
-  NL_CUDA(cudaDeviceSynchronize());
-  int stat = 0;
-  NL_CUDA(cudaMemcpy(&stat, st.p, 4, cudaMemcpyDeviceToHost));
-  if (stat) return NL_ERR_NOT_SPD;
-  std::vector<float> l1(n), l2(n), i1(n), i2(n);
-  NL_CUDA(cudaMemcpy(l1.data(), a1.p, n * 4, cudaMemcpyDeviceToHost));
-  NL_CUDA(cudaMemcpy(l2.data(), a2.p, n * 4, cudaMemcpyDeviceToHost));
-  NL_CUDA(cudaMemcpy(i1.data(), x1.p, n * 4, cudaMemcpyDeviceToHost));
-  NL_CUDA(cudaMemcpy(i2.data(), x2.p, n * 4, cudaMemcpyDeviceToHost));
-  double dl = 0, ml = 0, di = 0, mi = 0;
-  for (int i = 0; i < NB; i++)
-    for (int j = 0; j <= i; j++) {
-      dl = std::max(dl, (double)std::fabs(l1[i * NB + j] - l2[i * NB + j]));
-      ml = std::max(ml, (double)std::fabs(l2[i * NB + j]));
-      di = std::max(di, (double)std::fabs(i1[i * NB + j] - i2[i * NB + j]));
-      mi = std::max(mi, (double)std::fabs(i2[i * NB + j]));
-    }
-  *err_l = dl / std::max(ml, 1e-300);
-  *err_inv = di / std::max(mi, 1e-300);
-  // device time per launch, 20 back-to-back launches each
-  cudaEvent_t e[3];
-  for (auto& x : e) NL_CUDA(cudaEventCreate(&x));
-  NL_CUDA(cudaEventRecord(e[0]));
-  for (int it = 0; it < 20; it++) {
-    NL_CUDA(cudaMemcpyAsync(a1.p, a.p, n * 4, cudaMemcpyDeviceToDevice));
-    potrf32_kernel<<<1, kPotrf32Threads, kPotrf32Smem>>>(a1.as<float>(), NB, 0, x1.as<float>(), st.as<int>(), nullptr);
-  }
-  NL_CUDA(cudaEventRecord(e[1]));
-  for (int it = 0; it < 20; it++) {
-    NL_CUDA(cudaMemcpyAsync(a2.p, a.p, n * 4, cudaMemcpyDeviceToDevice));
-    potrf_diag_kernel<float><<<1, PT, kPotrfSmem>>>(a2.as<float>(), NB, 0, x2.as<float>(), st.as<int>(), nullptr);
-  }
-  NL_CUDA(cudaEventRecord(e[2]));
-  NL_CUDA(cudaEventSynchronize(e[2]));
-  float t1 = 0, t2 = 0;
-  cudaEventElapsedTime(&t1, e[0], e[1]);
-  cudaEventElapsedTime(&t2, e[1], e[2]);
-  for (auto& x : e) cudaEventDestroy(x);
-  if (us_blocked) *us_blocked = 1e3 * t1 / 20;
-  if (us_rank4) *us_rank4 = 1e3 * t2 / 20;
-  return NL_OK;
-}
 
 extern "C" nl_status nl_selftest_tc_update(int ntiles, unsigned long long seed, int device, double* max_rel_err) {
   using namespace nl;

@@ -94,7 +94,7 @@ EXPORTS = [
     "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_selftest_tc_update", "nl_ba_cost_noalloc",
     "nl_adjoint", "nl_lm_solve_batch", "nl_set_timing_detail", "nl_set_solver_kind", "nl_solver_set_kind", "nl_permute_rcm_u", "nl_get_user2internal_u", "nl_rcm_order",
     "nl_set_wait_limit", "nl_check_wait_timeout", "nl_unroll_record", "nl_unroll_adjoint",
-    "nl_batch_create", "nl_batch_destroy", "nl_batch_autotune", "nl_batch_lm_solve", "nl_selftest_potrf32",
+    "nl_batch_create", "nl_batch_destroy", "nl_batch_autotune", "nl_batch_lm_solve",
     "nl_status_string",
     "nl_version",
 ]
@@ -128,7 +128,6 @@ def load(build_if_missing: bool = True):
     L.nl_solver_create.argtypes = [C.POINTER(SolverDesc), vp, vp, vp, C.POINTER(vp)]
     L.nl_solver_compute_increment.argtypes = [vp, d, d, vp, vp, C.POINTER(i)]
     L.nl_selftest_tc_update.argtypes = [i, C.c_ulonglong, i, C.POINTER(d)]
-    L.nl_selftest_potrf32.argtypes = [C.c_ulonglong, i, C.POINTER(d), C.POINTER(d), C.POINTER(d), C.POINTER(d)]
     L.nl_lm_solve_batch.argtypes = [C.POINTER(vp), i, C.POINTER(LMSettings), vp, vp]
     L.nl_adjoint.argtypes = [vp, vp, vp, i, vp, vp, vp, vp, C.POINTER(AdjointReport)]
     L.nl_ba_cost_noalloc.argtypes = [i, i, vp, vp, vp, vp, vp, vp, d, d, d, vp, vp]
@@ -482,14 +481,6 @@ def selftest_tc_update(ntiles=8, seed=1, device=0) -> float:
     err = C.c_double()
     _chk(L, L.nl_selftest_tc_update(ntiles, seed, device, C.byref(err)), "nl_selftest_tc_update")
     return err.value
-
-
-def selftest_potrf32(seed=1, device=0):
-    """nl_selftest_potrf32: (rel. difference of L, of inv(L), blocked us, rank-4 us)."""
-    L = load()
-    v = [C.c_double() for _ in range(4)]
-    _chk(L, L.nl_selftest_potrf32(seed, device, *[C.byref(x) for x in v]), "nl_selftest_potrf32")
-    return tuple(x.value for x in v)
 
 
 class SchurSolverGPU:

@@ -11,10 +11,16 @@ damping updates are held fixed).  The loss is L = |X_10 - X_true|^2.
 * The replayed record reproduces the LM run (same kernels, same order).
 * Gradients w.r.t. observations, edge weights, the initial camera parameters
   (axis-angle, t) and the initial points, from the FP64 and the mixed handles,
-  against central differences (h = 1e-6) of the FP64 replay on 200 random
-  coordinates (50 per group), to 1e-4 relative: per coordinate where the
-  difference is at least 1% of its group's largest, and for every coordinate
-  against that scale.
+  against central differences of the FP64 replay on 200 random coordinates
+  (50 per group), to 1e-4 relative plus an absolute 1e-5 of the group's
+  largest difference (the quotient's own noise floor, see `_check`).  The
+  step is h = 1e-4.  The last of the 10 steps are damped by
+  mu ~ 0.2 only, and their rounding makes the difference quotient of the
+  10-step map noisy at h = 1e-6: on the largest observation coordinate the
+  oracle's replay gives -0.20245428, -0.20245414 and -0.20245553 at
+  h = 1e-3, 1e-4 and 1e-5, but -0.20242395 at h = 1e-6 and -0.20230839 at
+  h = 1e-7, while the adjoint gives -0.20245431.  The truncation error at
+  h = 1e-4 is below 1e-8 relative.
 * A few coordinates against the same difference taken with the FP64 CPU
   oracle's own replay (update(true), computeIncrement(0, mu_k), oplus).
 """
@@ -26,7 +32,7 @@ from nelson_b200.problems import make_config, with_fixed_nodes
 
 pytestmark = pytest.mark.gpu
 
-H = 1e-6
+H = 1e-4
 TOL = 1e-4
 K_ITERS = 10
 
@@ -101,18 +107,21 @@ def _pick(g_obs, g_w, g_c, g_p, p, coords):
 
 
 def _check(adj, fd, coords):
+    """Per coordinate |adj - fd| <= 1e-4 |fd| + 1e-5 s, s the group's largest
+    |fd|.  The absolute part is the difference quotient's own noise floor at
+    h = 1e-4: measured as 1.2e-5 of s on the initial-parameter groups after 10
+    steps, where the gradient is small (the map has nearly converged), and
+    below 1e-7 of s on the observation and weight groups."""
     kinds = np.array([k for k, _ in coords])
     for kind in ("obs", "w", "cam", "pt"):
         m = kinds == kind
         a, f = adj[m], fd[m]
         scale = np.abs(f).max()
+        err = np.abs(a - f)
         big = np.abs(f) >= 1e-2 * scale
-        rel = np.abs(a[big] - f[big]) / np.abs(f[big])
-        print(kind, "scale", scale, "n_big", int(big.sum()), "max rel", rel.max() if big.any() else None,
-              "max abs / scale", np.abs(a - f).max() / scale)
-        assert big.sum() >= 10, kind
-        assert rel.max() <= TOL, (kind, rel.max())
-        assert np.abs(a - f).max() <= TOL * scale, kind
+        print(kind, "scale", scale, "max rel (|fd| >= 1% of scale)", (err[big] / np.abs(f[big])).max(),
+              "max abs / scale", err.max() / scale)
+        assert (err <= TOL * np.abs(f) + 1e-5 * scale).all(), (kind, (err / (TOL * np.abs(f) + 1e-5 * scale)).max())
 
 
 def test_replay_reproduces_lm(unrolled):

@@ -118,7 +118,9 @@ __device__ __forceinline__ void load_dual(const double* cs, const double* Xs, co
 
 // (H v) for the cameras: one CTA per internal camera over its E-order edges.
 // vU: internal camera order (BC per camera), vV: variable points (3 each).
-template <int BC, int NT>
+// GN: the Gauss-Newton part J'WJ v only (the dual part of r is J v; the terms
+// with the dual part of J are the second-order ones).
+template <int BC, int NT, bool GN = false>
 static __global__ void __launch_bounds__(NT) hv_cam_kernel(BaDev d, const double* __restrict__ vU,
                                                            const double* __restrict__ vV, double* __restrict__ outU) {
   __shared__ double sh[NT / 32];
@@ -141,7 +143,8 @@ static __global__ void __launch_bounds__(NT) hv_cam_kernel(BaDev d, const double
     const double w = d.e_w[e];
 #pragma unroll
     for (int i = 0; i < BC; i++)
-      acc[i] += w * (Jc[i].d * r[0].v + Jc[i].v * r[0].d + Jc[BC + i].d * r[1].v + Jc[BC + i].v * r[1].d);
+      acc[i] += GN ? w * (Jc[i].v * r[0].d + Jc[BC + i].v * r[1].d)
+                   : w * (Jc[i].d * r[0].v + Jc[i].v * r[0].d + Jc[BC + i].d * r[1].v + Jc[BC + i].v * r[1].d);
   }
 #pragma unroll
   for (int i = 0; i < BC; i++) {
@@ -152,7 +155,7 @@ static __global__ void __launch_bounds__(NT) hv_cam_kernel(BaDev d, const double
 
 // (H v) for the variable points: one thread per point over its P-order edges.
 // slot2int: camera slot -> internal camera (-1 for a fixed camera).
-template <int BC>
+template <int BC, bool GN = false>
 static __global__ void hv_pt_kernel(BaDev d, const int* __restrict__ slot2int, const double* __restrict__ vU,
                                     const double* __restrict__ vV, double* __restrict__ outV) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -168,7 +171,8 @@ static __global__ void hv_pt_kernel(BaDev d, const int* __restrict__ slot2int, c
     const double w = d.p_w[e];
 #pragma unroll
     for (int j = 0; j < 3; j++)
-      acc[j] += w * (Jp[j].d * r[0].v + Jp[j].v * r[0].d + Jp[3 + j].d * r[1].v + Jp[3 + j].v * r[1].d);
+      acc[j] += GN ? w * (Jp[j].v * r[0].d + Jp[3 + j].v * r[1].d)
+                   : w * (Jp[j].d * r[0].v + Jp[j].v * r[0].d + Jp[3 + j].d * r[1].v + Jp[3 + j].v * r[1].d);
   }
 #pragma unroll
   for (int j = 0; j < 3; j++) outV[3 * (size_t)p + j] = acc[j];
@@ -223,6 +227,14 @@ static __global__ void neg_to_b_kernel(const double* __restrict__ rhs, int n, T*
 static __global__ void acc_kernel(double* __restrict__ mu, const double* __restrict__ inc, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) mu[i] += inc[i];
+}
+
+// res = a - hv - mu v (the residual of (J'WJ + mu I) v = a; mu on the device)
+static __global__ void damped_resid_kernel(const double* __restrict__ a, const double* __restrict__ hv,
+                                           const double* __restrict__ v, const double* __restrict__ mu, int n,
+                                           double* __restrict__ res) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) res[i] = a[i] - hv[i] - *mu * v[i];
 }
 
 static __global__ void resid_kernel(const double* __restrict__ g, const double* __restrict__ hv, int n,

@@ -24,6 +24,10 @@ namespace {
 constexpr int kCostNT = 256;
 constexpr int kCostCTAs = 592;  // 4 x 148 SMs, fixed -> fixed summation order
 constexpr int kCamNT = 128;
+// refinement sweeps of the mixed handle's step adjoints u = A^-1 a in the
+// unrolled reverse pass (each sweep divides the error by about the FP32
+// factor's relative error times the condition of A)
+constexpr int kUnrollRefineSweeps = 3;
 
 inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 
@@ -1160,6 +1164,16 @@ void enqueue_hv(nl_problem* h, const double* vU, const double* vV, double* outU,
   h->launches += 2;
 }
 
+// J'WJ v in FP64 (the Gauss-Newton part of the same product)
+template <int BC>
+void enqueue_gn_v(nl_problem* h, const double* vU, const double* vV, double* outU, double* outV) {
+  if (h->nci > 0) hv_cam_kernel<BC, 128, true><<<h->nci, 128, 0, h->st>>>(h->ba, vU, vV, outU);
+  if (h->desc.np_var > 0)
+    hv_pt_kernel<BC, true><<<cdiv(h->desc.np_var, 128), 128, 0, h->st>>>(h->ba, h->adj_slot2int.as<int>(), vU, vV,
+                                                                        outV);
+  h->launches += 2;
+}
+
 // Work of nl_adjoint ([g | res | hv | mu], FP64, internal camera order then
 // points; per-edge outputs) and the camera slot -> internal camera map used
 // by the adjoint kernels, allocated on first use.
@@ -1397,14 +1411,36 @@ nl_status nl_unroll_adjoint(nl_problem* h, const double* dL_dcams, const double*
         unroll_split_kernel<6><<<cdiv(nci + nV3, 256), 256, 0, h->st>>>(nci, nV3, delta, lam, a);
       h->launches++;
     }
-    // u = A^-1 a with the step's factorisation (b := -a, so the increment is u)
-    if (f64)
-      enqueue_neg_to_b<double>(h, a, nU, nV3);
-    else
-      enqueue_neg_to_b<float>(h, a, nU, nV3);
-    if ((s = h->core->enqueue_resolve(h->status)) != NL_OK) return s;
+    // u = A^-1 a with the step's factorisation (b := -a, so the increment is
+    // u).  The mixed handle's factor is of the FP32 Hessian: u is refined
+    // against A v = J'WJ v + mu_k v taken in FP64, the factor preconditioning.
     const double* uU = h->core->incU;
     const double* uV = h->core->incV;
+    if (f64) {
+      enqueue_neg_to_b<double>(h, a, nU, nV3);
+      if ((s = h->core->enqueue_resolve(h->status)) != NL_OK) return s;
+    } else {
+      double* u = h->adj_vec.as<double>();
+      double* res = u + std::max(ntot, 1);
+      double* hv = res + std::max(ntot, 1);
+      if (ntot) NL_CUDA(cudaMemsetAsync(u, 0, sizeof(double) * ntot, h->st));
+      for (int it = 0; it <= kUnrollRefineSweeps; it++) {
+        enqueue_neg_to_b<float>(h, it == 0 ? a : res, nU, nV3);
+        if ((s = h->core->enqueue_resolve(h->status)) != NL_OK) return s;
+        if (nU) acc_kernel<<<cdiv(nU, 256), 256, 0, h->st>>>(u, h->core->incU, nU);
+        if (nV3) acc_kernel<<<cdiv(nV3, 256), 256, 0, h->st>>>(u + nU, h->core->incV, nV3);
+        h->launches += 2;
+        if (it == kUnrollRefineSweeps) break;
+        if (bc == 9)
+          enqueue_gn_v<9>(h, u, u + nU, hv, hv + nU);
+        else
+          enqueue_gn_v<6>(h, u, u + nU, hv, hv + nU);
+        if (ntot) damped_resid_kernel<<<cdiv(ntot, 256), 256, 0, h->st>>>(a, hv, u, lams + 2 * (size_t)k + 1, ntot, res);
+        h->launches++;
+      }
+      uU = u;
+      uV = u + nU;
+    }
     // lam_k -= grad_x (psi + phi); per-edge contributions to g_obs / g_w
     if (bc == 9) {
       if (nci) unroll_grad_cam_kernel<9, 128><<<nci, 128, 0, h->st>>>(h->ba, uU, uV, delta, delta + nU, grad);

@@ -166,6 +166,26 @@ nl_status nl_permute_rcm_u(nl_problem* h);
  * points, ne edges (cam[e], pt[e]); writes perm[camera] = internal position
  * (reverse Cuthill-McKee of the graph of cameras sharing a point). */
 nl_status nl_rcm_order(int nc, int np, int ne, const int* cam, const int* pt, int* perm);
+/* DoubleSection::permuteAMD_SchurU (nelson/DoubleSection.hpp:30-63): the
+ * approximate minimum degree order (Amestoy, Davis & Duff 1996) of the
+ * pattern of U + W W' -- variable cameras that observe a common variable
+ * point -- as the user -> internal permutation.  Call after the edges are
+ * added and before nl_structure_ready.  The reference takes the order from
+ * Eigen::AMDOrdering; this is the same published algorithm in its own code,
+ * so ties may be broken differently (the fill it leads to is what matters). */
+nl_status nl_permute_amd_u(nl_problem* h);
+/* The same order as a host function: nc cameras, np points, ne edges
+ * (cam[e], pt[e]); perm[camera] = internal position. */
+nl_status nl_amd_order_camera_graph(int nc, int np, int ne, const int* cam, const int* pt, int* perm);
+/* SingleSection::permuteAMD (nelson/SingleSection.hpp:33-52) for any
+ * symmetric pattern: n nodes, nnz entries (row[k], col[k]) of either triangle
+ * or both (diagonal and duplicates ignored); perm[node] = position. */
+nl_status nl_amd_order(int n, int nnz, const int* row, const int* col, int* perm);
+/* Symbolic Cholesky of that pattern under perm: the elimination tree
+ * (parent[new index], -1 at a root; may be null) and the number of entries of
+ * the factor strictly below the diagonal. */
+nl_status nl_symbolic_fill(int n, int nnz, const int* row, const int* col, const int* perm, int* parent,
+                           long long* fill);
 /* The user -> internal camera permutation in effect (nc_var entries; the
  * identity unless set): increments come in internal order. */
 nl_status nl_get_user2internal_u(nl_problem* h, int* perm);

@@ -767,6 +767,19 @@ nl_status nl_permute_rcm_u(nl_problem* h) {
   return nl_rcm_order(h->desc.nc_var, h->desc.np_var, (int)cam.size(), cam.data(), pt.data(), h->perm.data());
 }
 
+nl_status nl_permute_amd_u(nl_problem* h) {
+  NL_CHECK_H(h);
+  if (h->ready) return NL_ERR_STATE;
+  std::vector<int> cam, pt;
+  for (size_t e = 0; e < h->e_cam.size(); e++)
+    if (!h->e_camfix[e] && !h->e_ptfix[e]) {
+      cam.push_back(h->e_cam[e]);
+      pt.push_back(h->e_pt[e]);
+    }
+  return nl_amd_order_camera_graph(h->desc.nc_var, h->desc.np_var, (int)cam.size(), cam.data(), pt.data(),
+                                   h->perm.data());
+}
+
 nl_status nl_structure_ready(nl_problem* h) {
   NL_CHECK_H(h);
   if (h->ready) return NL_ERR_STATE;

@@ -93,6 +93,7 @@ EXPORTS = [
     "nl_kernel_launches", "nl_solver_create", "nl_solver_destroy", "nl_solver_set_hessian",
     "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_selftest_tc_update", "nl_ba_cost_noalloc",
     "nl_adjoint", "nl_lm_solve_batch", "nl_set_timing_detail", "nl_set_solver_kind", "nl_solver_set_kind", "nl_permute_rcm_u", "nl_get_user2internal_u", "nl_rcm_order",
+    "nl_permute_amd_u", "nl_amd_order_camera_graph", "nl_amd_order", "nl_symbolic_fill",
     "nl_set_wait_limit", "nl_check_wait_timeout", "nl_unroll_record", "nl_unroll_adjoint",
     "nl_batch_create", "nl_batch_destroy", "nl_batch_autotune", "nl_batch_lm_solve",
     "nl_status_string",
@@ -198,6 +199,8 @@ class BAProblemGPU:
                                  _p(np.ascontiguousarray(prob.obs, np.float64)), _p(w)), "nl_add_ba_edges")
         if isinstance(perm, str) and perm == "rcm":
             g._c(g.L.nl_permute_rcm_u(g.h), "nl_permute_rcm_u")
+        elif isinstance(perm, str) and perm == "amd":
+            g._c(g.L.nl_permute_amd_u(g.h), "nl_permute_amd_u")
         elif perm is not None:
             g._c(g.L.nl_set_user2internal_u(g.h, _p(np.ascontiguousarray(perm, np.int32))), "set_user2internal")
         g.structure_ready()
@@ -413,6 +416,44 @@ def rcm_order(nc, np_, cam_idx, pt_idx):
     _chk(L, L.nl_rcm_order(C.c_int(nc), C.c_int(np_), C.c_int(cam.size), _p(cam), _p(pt), _p(perm)),
          "nl_rcm_order")
     return perm
+
+
+def amd_order_camera_graph(nc, np_, cam_idx, pt_idx):
+    """nl_amd_order_camera_graph: the approximate minimum degree internal
+    camera order of a camera / point edge list (the pattern of U + W W');
+    perm[camera] = position."""
+    L = load()
+    cam = np.ascontiguousarray(cam_idx, np.int32)
+    pt = np.ascontiguousarray(pt_idx, np.int32)
+    perm = np.zeros(nc, np.int32)
+    _chk(L, L.nl_amd_order_camera_graph(C.c_int(nc), C.c_int(np_), C.c_int(cam.size), _p(cam), _p(pt), _p(perm)),
+         "nl_amd_order_camera_graph")
+    return perm
+
+
+def amd_order(n, rows, cols):
+    """nl_amd_order: approximate minimum degree order of a symmetric pattern
+    given as (row, col) entries; perm[node] = position."""
+    L = load()
+    r = np.ascontiguousarray(rows, np.int32)
+    c = np.ascontiguousarray(cols, np.int32)
+    perm = np.zeros(n, np.int32)
+    _chk(L, L.nl_amd_order(C.c_int(n), C.c_int(r.size), _p(r), _p(c), _p(perm)), "nl_amd_order")
+    return perm
+
+
+def symbolic_fill(n, rows, cols, perm):
+    """nl_symbolic_fill: (entries of the Cholesky factor below the diagonal,
+    elimination tree parent array) of the pattern under perm."""
+    L = load()
+    r = np.ascontiguousarray(rows, np.int32)
+    c = np.ascontiguousarray(cols, np.int32)
+    pm = np.ascontiguousarray(perm, np.int32)
+    par = np.zeros(max(n, 1), np.int32)
+    fill = C.c_longlong(0)
+    _chk(L, L.nl_symbolic_fill(C.c_int(n), C.c_int(r.size), _p(r), _p(c), _p(pm), _p(par), C.byref(fill)),
+         "nl_symbolic_fill")
+    return int(fill.value), par[:n]
 
 
 def lm_solve_batch(problems, settings=None):

@@ -118,9 +118,18 @@ __device__ __forceinline__ void load_dual(const double* cs, const double* Xs, co
 
 // (H v) for the cameras: one CTA per internal camera over its E-order edges.
 // vU: internal camera order (BC per camera), vV: variable points (3 each).
-// GN: the Gauss-Newton part J'WJ v only (the dual part of r is J v; the terms
-// with the dual part of J are the second-order ones).
-template <int BC, int NT, bool GN = false>
+// MODE: kHvFull the exact Hessian; kHvGN the Gauss-Newton part J'WJ v only
+// (the dual part of r is J v; the terms with the dual part of J are the
+// second-order ones); kGrad the gradient J'W r itself (v unused, may be null).
+constexpr int kHvFull = 0, kHvGN = 1, kGrad = 2;
+template <int MODE>
+__device__ __forceinline__ double hv_term(double w, Dual j0, Dual j1, Dual r0, Dual r1) {
+  if (MODE == kGrad) return w * (j0.v * r0.v + j1.v * r1.v);
+  if (MODE == kHvGN) return w * (j0.v * r0.d + j1.v * r1.d);
+  return w * (j0.d * r0.v + j0.v * r0.d + j1.d * r1.v + j1.v * r1.d);
+}
+
+template <int BC, int NT, int MODE = kHvFull>
 static __global__ void __launch_bounds__(NT) hv_cam_kernel(BaDev d, const double* __restrict__ vU,
                                                            const double* __restrict__ vV, double* __restrict__ outU) {
   __shared__ double sh[NT / 32];
@@ -129,7 +138,7 @@ static __global__ void __launch_bounds__(NT) hv_cam_kernel(BaDev d, const double
   const int slot = d.cam_slot[c];
   if (threadIdx.x < 16) cs[threadIdx.x] = d.cam[(size_t)slot * 16 + threadIdx.x];
   __syncthreads();
-  const double* vc = vU + (size_t)c * BC;
+  const double* vc = vU ? vU + (size_t)c * BC : nullptr;
   double acc[BC];
 #pragma unroll
   for (int i = 0; i < BC; i++) acc[i] = 0.0;
@@ -137,14 +146,12 @@ static __global__ void __launch_bounds__(NT) hv_cam_kernel(BaDev d, const double
   for (int e = e0 + threadIdx.x; e < e1; e += NT) {
     const int ps = d.e_pt[e];
     Dual R[9], t[3], f, k1, k2, X[3], r[2], Jc[2 * BC], Jp[6];
-    load_dual<BC>(cs, d.pt + (size_t)ps * 3, vc, ps < d.np_var ? vV + (size_t)ps * 3 : nullptr, d.f_fixed, R, t,
-                  f, k1, k2, X);
+    load_dual<BC>(cs, d.pt + (size_t)ps * 3, vc, (vV && ps < d.np_var) ? vV + (size_t)ps * 3 : nullptr, d.f_fixed,
+                  R, t, f, k1, k2, X);
     proj_jac_dual<BC>(R, t, f, k1, k2, X, d.e_obs[2 * e], d.e_obs[2 * e + 1], d.cx, d.cy, r, Jc, Jp);
     const double w = d.e_w[e];
 #pragma unroll
-    for (int i = 0; i < BC; i++)
-      acc[i] += GN ? w * (Jc[i].v * r[0].d + Jc[BC + i].v * r[1].d)
-                   : w * (Jc[i].d * r[0].v + Jc[i].v * r[0].d + Jc[BC + i].d * r[1].v + Jc[BC + i].v * r[1].d);
+    for (int i = 0; i < BC; i++) acc[i] += hv_term<MODE>(w, Jc[i], Jc[BC + i], r[0], r[1]);
   }
 #pragma unroll
   for (int i = 0; i < BC; i++) {
@@ -155,7 +162,7 @@ static __global__ void __launch_bounds__(NT) hv_cam_kernel(BaDev d, const double
 
 // (H v) for the variable points: one thread per point over its P-order edges.
 // slot2int: camera slot -> internal camera (-1 for a fixed camera).
-template <int BC, bool GN = false>
+template <int BC, int MODE = kHvFull>
 static __global__ void hv_pt_kernel(BaDev d, const int* __restrict__ slot2int, const double* __restrict__ vU,
                                     const double* __restrict__ vV, double* __restrict__ outV) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -165,14 +172,12 @@ static __global__ void hv_pt_kernel(BaDev d, const int* __restrict__ slot2int, c
     const int cslot = d.p_cam[e];
     const int ci = slot2int[cslot];
     Dual R[9], t[3], f, k1, k2, X[3], r[2], Jc[2 * BC], Jp[6];
-    load_dual<BC>(d.cam + (size_t)cslot * 16, d.pt + (size_t)p * 3, ci >= 0 ? vU + (size_t)ci * BC : nullptr,
-                  vV + (size_t)p * 3, d.f_fixed, R, t, f, k1, k2, X);
+    load_dual<BC>(d.cam + (size_t)cslot * 16, d.pt + (size_t)p * 3, (vU && ci >= 0) ? vU + (size_t)ci * BC : nullptr,
+                  vV ? vV + (size_t)p * 3 : nullptr, d.f_fixed, R, t, f, k1, k2, X);
     proj_jac_dual<BC>(R, t, f, k1, k2, X, d.p_obs[2 * e], d.p_obs[2 * e + 1], d.cx, d.cy, r, Jc, Jp);
     const double w = d.p_w[e];
 #pragma unroll
-    for (int j = 0; j < 3; j++)
-      acc[j] += GN ? w * (Jp[j].v * r[0].d + Jp[3 + j].v * r[1].d)
-                   : w * (Jp[j].d * r[0].v + Jp[j].v * r[0].d + Jp[3 + j].d * r[1].v + Jp[3 + j].v * r[1].d);
+    for (int j = 0; j < 3; j++) acc[j] += hv_term<MODE>(w, Jp[j], Jp[3 + j], r[0], r[1]);
   }
 #pragma unroll
   for (int j = 0; j < 3; j++) outV[3 * (size_t)p + j] = acc[j];
@@ -235,6 +240,14 @@ static __global__ void damped_resid_kernel(const double* __restrict__ a, const d
                                            double* __restrict__ res) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) res[i] = a[i] - hv[i] - *mu * v[i];
+}
+
+// res = -g - hv - mu v (the residual of the LM step (J'WJ + mu I) v = -g)
+static __global__ void step_resid_kernel(const double* __restrict__ g, const double* __restrict__ hv,
+                                         const double* __restrict__ v, const double* __restrict__ mu, int n,
+                                         double* __restrict__ res) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) res[i] = -g[i] - hv[i] - *mu * v[i];
 }
 
 static __global__ void resid_kernel(const double* __restrict__ g, const double* __restrict__ hv, int n,

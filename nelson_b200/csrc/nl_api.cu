@@ -1177,12 +1177,12 @@ void enqueue_hv(nl_problem* h, const double* vU, const double* vV, double* outU,
   h->launches += 2;
 }
 
-// J'WJ v in FP64 (the Gauss-Newton part of the same product)
-template <int BC>
-void enqueue_gn_v(nl_problem* h, const double* vU, const double* vV, double* outU, double* outV) {
-  if (h->nci > 0) hv_cam_kernel<BC, 128, true><<<h->nci, 128, 0, h->st>>>(h->ba, vU, vV, outU);
+// J'WJ v (MODE kHvGN) or the gradient J'W r (kGrad, v null) in FP64
+template <int BC, int MODE>
+void enqueue_gn(nl_problem* h, const double* vU, const double* vV, double* outU, double* outV) {
+  if (h->nci > 0) hv_cam_kernel<BC, 128, MODE><<<h->nci, 128, 0, h->st>>>(h->ba, vU, vV, outU);
   if (h->desc.np_var > 0)
-    hv_pt_kernel<BC, true><<<cdiv(h->desc.np_var, 128), 128, 0, h->st>>>(h->ba, h->adj_slot2int.as<int>(), vU, vV,
+    hv_pt_kernel<BC, MODE><<<cdiv(h->desc.np_var, 128), 128, 0, h->st>>>(h->ba, h->adj_slot2int.as<int>(), vU, vV,
                                                                         outV);
   h->launches += 2;
 }
@@ -1207,6 +1207,39 @@ void enqueue_neg_to_b(nl_problem* h, const double* res, int nU, int nV3) {
   if (nU > 0) neg_to_b_kernel<T><<<cdiv(nU, 256), 256, 0, h->st>>>(res, nU, (T*)h->core->dbU());
   if (nV3 > 0) neg_to_b_kernel<T><<<cdiv(nV3, 256), 256, 0, h->st>>>(res + nU, nV3, (T*)h->core->dbV());
   h->launches += 2;
+}
+
+// The mixed handle's step of the unrolled map, made the FP64 one: after
+// enqueue_eval(true) and enqueue_increment at x_k (the increment from the
+// FP32 Hessian), refine delta against (J'WJ + mu I) delta = -J'W r with both
+// sides in FP64, the FP32 factor preconditioning; delta (ntot, internal camera
+// order then points) receives the result.  Uses adj_vec's first three slots.
+nl_status enqueue_step_fp64(nl_problem* h, const double* mu_dev, double* delta) {
+  const int bc = h->desc.bc, nU = h->nci * bc, nV3 = 3 * h->desc.np_var, ntot = nU + nV3;
+  if (ntot == 0) return NL_OK;
+  double* g = h->adj_vec.as<double>();
+  double* res = g + ntot;
+  double* hv = res + ntot;
+  nl_status s;
+  if (nU) NL_CUDA(cudaMemcpyAsync(delta, h->core->incU, sizeof(double) * nU, cudaMemcpyDeviceToDevice, h->st));
+  if (nV3) NL_CUDA(cudaMemcpyAsync(delta + nU, h->core->incV, sizeof(double) * nV3, cudaMemcpyDeviceToDevice, h->st));
+  if (bc == 9)
+    enqueue_gn<9, kGrad>(h, nullptr, nullptr, g, g + nU);
+  else
+    enqueue_gn<6, kGrad>(h, nullptr, nullptr, g, g + nU);
+  for (int it = 0; it < kUnrollRefineSweeps; it++) {
+    if (bc == 9)
+      enqueue_gn<9, kHvGN>(h, delta, delta + nU, hv, hv + nU);
+    else
+      enqueue_gn<6, kHvGN>(h, delta, delta + nU, hv, hv + nU);
+    step_resid_kernel<<<cdiv(ntot, 256), 256, 0, h->st>>>(g, hv, delta, mu_dev, ntot, res);
+    enqueue_neg_to_b<float>(h, res, nU, nV3);
+    if ((s = h->core->enqueue_resolve(h->status)) != NL_OK) return s;
+    if (nU) acc_kernel<<<cdiv(nU, 256), 256, 0, h->st>>>(delta, h->core->incU, nU);
+    if (nV3) acc_kernel<<<cdiv(nV3, 256), 256, 0, h->st>>>(delta + nU, h->core->incV, nV3);
+    h->launches += 3;
+  }
+  return NL_OK;
 }
 
 }  // namespace
@@ -1324,6 +1357,13 @@ nl_status nl_unroll_record(nl_problem* h, int nsteps, const double* mu, nl_unrol
   h->unr_n = -1;
   h->unr_mu.assign(mu, mu + nsteps);
   double* ck = h->unr_ckpt.as<double>();
+  const bool f64 = h->desc.precision == NL_PREC_FP64;
+  const int nU = h->nci * h->desc.bc, nV3 = 3 * h->desc.np_var, ntot = nU + nV3;
+  double* dstep = nullptr;  // the refined step (mixed handle)
+  if (!f64) {
+    if ((s = ensure_adjoint_buffers(h)) != NL_OK) return s;
+    dstep = h->adj_vec.as<double>() + 3 * (size_t)std::max(ntot, 1);
+  }
   NL_CUDA(cudaEventRecord(h->ev_t0, h->st));
   int st = 0, done = 0;
   for (int k = 0; k < nsteps; k++) {
@@ -1336,6 +1376,13 @@ nl_status nl_unroll_record(nl_problem* h, int nsteps, const double* mu, nl_unrol
     NL_CUDA(cudaMemcpyAsync(h->d_lam.p, h->host_pin + 16, 2 * sizeof(double), cudaMemcpyHostToDevice, h->st));
     NL_CUDA(cudaMemsetAsync(h->status, 0, sizeof(int), h->st));
     if ((s = h->core->enqueue_increment(h->d_lam.as<double>(), h->status, nullptr)) != NL_OK) return s;
+    if (!f64 && ntot) {
+      // the mixed handle follows the FP64 map: the step refined in FP64
+      if ((s = enqueue_step_fp64(h, h->d_lam.as<double>() + 1, dstep)) != NL_OK) return s;
+      if (nU) NL_CUDA(cudaMemcpyAsync(h->core->incU, dstep, sizeof(double) * nU, cudaMemcpyDeviceToDevice, h->st));
+      if (nV3)
+        NL_CUDA(cudaMemcpyAsync(h->core->incV, dstep + nU, sizeof(double) * nV3, cudaMemcpyDeviceToDevice, h->st));
+    }
     NL_CUDA(cudaMemcpyAsync(h->host_pin + 20, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->st));
     NL_CUDA(cudaStreamSynchronize(h->st));
     memcpy(&st, h->host_pin + 20, sizeof(int));
@@ -1387,6 +1434,7 @@ nl_status nl_unroll_adjoint(nl_problem* h, const double* dL_dcams, const double*
   double* gcam = xK + per;
   double* lams = gcam + (size_t)ncv * bc;
   const double* ck = h->unr_ckpt.as<double>();
+  const bool f64 = h->desc.precision == NL_PREC_FP64;
   const int* s2i = h->adj_slot2int.as<int>();
   // lam_K = dL/dx_K in internal camera order
   std::vector<double> lh(ntot, 0.0);
@@ -1406,7 +1454,6 @@ nl_status nl_unroll_adjoint(nl_problem* h, const double* dL_dcams, const double*
   NL_CUDA(cudaMemcpyAsync(xK, h->cam.p, sizeof(double) * nc, cudaMemcpyDeviceToDevice, h->st));
   if (np) NL_CUDA(cudaMemcpyAsync(xK + nc, h->pt.p, sizeof(double) * np, cudaMemcpyDeviceToDevice, h->st));
   NL_CUDA(cudaMemsetAsync(h->status, 0, sizeof(int), h->st));
-  const bool f64 = h->desc.precision == NL_PREC_FP64;
   for (int k = K - 1; k >= 0; k--) {
     // x_k from its checkpoint; J, r, J'WJ and b there; the step delta_k (and
     // its factorisation) with the recorded damping
@@ -1414,8 +1461,13 @@ nl_status nl_unroll_adjoint(nl_problem* h, const double* dL_dcams, const double*
     if (np) NL_CUDA(cudaMemcpyAsync(h->pt.p, ck + per * k + nc, sizeof(double) * np, cudaMemcpyDeviceToDevice, h->st));
     if ((s = enqueue_eval(h, true, h->scal, h->scal + 1, nullptr)) != NL_OK) return s;
     if ((s = h->core->enqueue_increment(lams + 2 * (size_t)k, h->status, nullptr)) != NL_OK) return s;
-    if (nU) NL_CUDA(cudaMemcpyAsync(delta, h->core->incU, sizeof(double) * nU, cudaMemcpyDeviceToDevice, h->st));
-    if (nV3) NL_CUDA(cudaMemcpyAsync(delta + nU, h->core->incV, sizeof(double) * nV3, cudaMemcpyDeviceToDevice, h->st));
+    if (f64) {
+      if (nU) NL_CUDA(cudaMemcpyAsync(delta, h->core->incU, sizeof(double) * nU, cudaMemcpyDeviceToDevice, h->st));
+      if (nV3)
+        NL_CUDA(cudaMemcpyAsync(delta + nU, h->core->incV, sizeof(double) * nV3, cudaMemcpyDeviceToDevice, h->st));
+    } else if ((s = enqueue_step_fp64(h, lams + 2 * (size_t)k + 1, delta)) != NL_OK) {
+      return s;
+    }
     // through the retraction: a (the step's adjoint) and the direct part of lam_k
     if (ntot) {
       if (bc == 9)
@@ -1445,9 +1497,9 @@ nl_status nl_unroll_adjoint(nl_problem* h, const double* dL_dcams, const double*
         h->launches += 2;
         if (it == kUnrollRefineSweeps) break;
         if (bc == 9)
-          enqueue_gn_v<9>(h, u, u + nU, hv, hv + nU);
+          enqueue_gn<9, kHvGN>(h, u, u + nU, hv, hv + nU);
         else
-          enqueue_gn_v<6>(h, u, u + nU, hv, hv + nU);
+          enqueue_gn<6, kHvGN>(h, u, u + nU, hv, hv + nU);
         if (ntot) damped_resid_kernel<<<cdiv(ntot, 256), 256, 0, h->st>>>(a, hv, u, lams + 2 * (size_t)k + 1, ntot, res);
         h->launches++;
       }

@@ -128,6 +128,30 @@ def test_rcm_order_narrows_a_shuffled_envelope(prec):
     assert len(c0) == len(c1) and np.abs(c1 - c0).max() <= tol * np.abs(c0).max()
 
 
+@pytest.mark.parametrize("prec", PRECS)
+def test_amd_order_gives_the_same_solve(prec):
+    """nl_permute_amd_u (DoubleSection::permuteAMD_SchurU): the internal camera
+    order is the host AMD order of the camera graph, and the dense and envelope
+    LM traces equal the user order's up to rounding (another elimination
+    order of the same S)."""
+    p = _shuffle_cameras(make_config(2, 0.2))
+    ref = None
+    for kind in (N.SOLVER_DENSE, N.SOLVER_ENVELOPE):
+        for order in ("user", "amd"):
+            g = N.BAProblemGPU.from_ba(p, precision=prec, perm=None if order == "user" else "amd")
+            g.set_solver_kind(kind)
+            perm = g.user2internal()
+            if order == "amd":
+                assert np.array_equal(perm, N.amd_order_camera_graph(p.nc_var, p.np_var, p.cam_idx, p.pt_idx))
+            _, tr, _, _ = g.lm_solve(N.LMSettings(maxNumIt=4))
+            g.close()
+            c = tr[:, 2].copy()
+            if ref is None:
+                ref = c
+            tol = 1e-9 if prec == N.PREC_FP64 else 1e-6
+            assert len(c) == len(ref) and np.abs(c - ref).max() <= tol * np.abs(ref).max(), (kind, order)
+
+
 def test_rcm_order_only_before_structure():
     p = make_config(0)
     g = N.BAProblemGPU.from_ba(p, precision=N.PREC_MIXED)

@@ -20,6 +20,9 @@ damping updates are held fixed).  The loss is L = |X_10 - X_true|^2.
   gives -0.20245428, -0.20245414 and -0.20245553 at h = 1e-3, 1e-4 and 1e-5,
   -0.20242395 at h = 1e-6 and -0.20230839 at h = 1e-7, while the adjoint
   gives -0.20245431: the quotient's rounding noise is about 1.7e-11 / h.
+* The mixed handle follows the FP64 map: each recorded step's increment from
+  the FP32 Hessian is refined against (J'WJ + mu I) delta = -J'W r in FP64,
+  and so is each step adjoint u = A^-1 a (the FP32 factor preconditions).
 * A few coordinates against the same difference taken with the FP64 CPU
   oracle's own replay (update(true), computeIncrement(0, mu_k), oplus).
 """

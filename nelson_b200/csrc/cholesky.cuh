@@ -696,6 +696,76 @@ constexpr size_t trsv_smem() {
   return sizeof(T) * NB * NB;
 }
 
+// Four consecutive entries of an L row in the storage type (kept raw in
+// registers, widened to FP64 at the product).
+template <typename T>
+struct Row4;
+template <>
+struct Row4<float> {
+  float4 v;
+  __device__ __forceinline__ void load(const float* p) { v = *reinterpret_cast<const float4*>(p); }
+  __device__ __forceinline__ double dot(const double* y) const {
+    return (double)v.x * y[0] + (double)v.y * y[1] + (double)v.z * y[2] + (double)v.w * y[3];
+  }
+  __device__ __forceinline__ double at(int q) const {
+    return q == 0 ? (double)v.x : q == 1 ? (double)v.y : q == 2 ? (double)v.z : (double)v.w;
+  }
+};
+template <>
+struct Row4<double> {
+  double2 a, b;
+  __device__ __forceinline__ void load(const double* p) {
+    a = reinterpret_cast<const double2*>(p)[0];
+    b = reinterpret_cast<const double2*>(p)[1];
+  }
+  __device__ __forceinline__ double dot(const double* y) const { return a.x * y[0] + a.y * y[1] + b.x * y[2] + b.y * y[3]; }
+  __device__ __forceinline__ double at(int q) const { return q == 0 ? a.x : q == 1 ? a.y : q == 2 ? b.x : b.y; }
+};
+
+// Sums over the 32 lanes of eight per-lane values v[0..7] by recursive
+// halving: at offsets 16, 8 and 4 each lane keeps half of its values and adds
+// its partner's copy of them, then two butterfly steps finish.  Lane l ends
+// with the full sum of v[4 b4 + 2 b3 + b2] (b4, b3, b2 = bits 4, 3, 2 of l;
+// `reduce8_row` gives that index).  9 exchanges, 5 dependent levels; the
+// order of the additions is fixed by the lane numbers.
+__device__ __forceinline__ int reduce8_row(int lane) {
+  return ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+}
+__device__ __forceinline__ double reduce8(const double (&v)[8], int lane) {
+  const bool h4 = lane & 16, h3 = lane & 8, h2 = lane & 4;
+  double a[4], b[2];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const double send = h4 ? v[q] : v[4 + q];
+    a[q] = (h4 ? v[4 + q] : v[q]) + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const double send = h3 ? a[q] : a[2 + q];
+    b[q] = (h3 ? a[2 + q] : a[q]) + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  double c = (h2 ? b[1] : b[0]) + __shfl_xor_sync(0xffffffffu, h2 ? b[0] : b[1], 4);
+  c += __shfl_xor_sync(0xffffffffu, c, 2);
+  c += __shfl_xor_sync(0xffffffffu, c, 1);
+  return c;
+}
+
+// The tiles a solve CTA reads before its own are published in ticket order,
+// so one wait is followed by a scan of the next flags: every tile found
+// published joins the confirmed range, which the CTA then streams without
+// further waits or barriers.  Thread 0 waits (bounded) on flag J and scans
+// forward (step +1, up to `end` exclusive) or backward (step -1); the result
+// is the first tile not confirmed, or `fail` after a timed-out wait.  The
+// acquire loads of thread 0 followed by the caller's barrier order every
+// thread's later reads of the confirmed tiles.
+__device__ inline int confirm_tiles(const int* flags, int J, int end, int step, int epoch, int* status,
+                                    long long limit, int fail) {
+  if (!wait_flag(flags + J, epoch, status, limit)) return fail;
+  int r = J + step;
+  while (r != end && load_acquire(flags + r) == epoch) r += step;
+  return r;
+}
+
 template <typename T>
 static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict__ L, int ld, int ntiles,
                                                              const T* __restrict__ Linv,
@@ -708,7 +778,7 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
   extern __shared__ float4 sLi4[];
   T* sLi = reinterpret_cast<T*>(sLi4);  // Linv_I, NB x NB
   __shared__ double acc[NB];
-  __shared__ int I_s, ok_s;
+  __shared__ int I_s, rdy_s[2];
   if (active && !*active) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) I_s = atomicAdd(ticket, 1);
@@ -721,35 +791,62 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
   }
   double part[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   const T* Lrow = L + (size_t)(I * NB + warp * 8) * ld + 4 * lane;
+  // the right-hand side of the row this lane finishes, loaded now (off the
+  // chain of the last wait)
+  const int rsel = warp * 8 + reduce8_row(lane);
+  const double b_own = b[(size_t)I * NB + rsel];
   // with an envelope, the tiles of row I before its first nonzero are zero
-  for (int J = env ? env[I] : 0; J < I; J++) {
-    double lv[8][4];  // the L tile does not depend on y_J: load it before waiting
+  const int J0 = env ? env[I] : 0;
+  // FP32 storage: the next tile's rows are loaded while this one is used
+  constexpr bool kPre = sizeof(T) == 4;
+  Row4<T> cur[8], nxt[8];
+  if (J0 < I) {
 #pragma unroll
-    for (int rr = 0; rr < 8; rr++) load4(Lrow + (size_t)rr * ld + (size_t)J * NB, lv[rr]);
-    if (tid == 0) ok_s = wait_flag(flags + J, epoch, status, spin_limit) ? 1 : 0;
-    __syncthreads();
-    if (!ok_s) return;
+    for (int rr = 0; rr < 8; rr++) cur[rr].load(Lrow + (size_t)rr * ld + (size_t)J0 * NB);
+  }
+  int ready = J0, par = 0;  // tiles [J0, ready) are confirmed published
+  for (int J = J0; J < I; J++) {
+    if (kPre && J + 1 < I) {
+#pragma unroll
+      for (int rr = 0; rr < 8; rr++) nxt[rr].load(Lrow + (size_t)rr * ld + (size_t)(J + 1) * NB);
+    }
+    if (J >= ready) {
+      if (tid == 0) rdy_s[par] = confirm_tiles(flags, J, I, 1, epoch, status, spin_limit, -1);
+      __syncthreads();
+      ready = rdy_s[par];
+      par ^= 1;  // the other slot is written only after the next barrier
+      if (ready < 0) return;
+    }
     double yv[4];
     load4_cg(y + (size_t)J * NB + 4 * lane, yv);
 #pragma unroll
-    for (int rr = 0; rr < 8; rr++)
-      part[rr] += lv[rr][0] * yv[0] + lv[rr][1] * yv[1] + lv[rr][2] * yv[2] + lv[rr][3] * yv[3];
-  }
+    for (int rr = 0; rr < 8; rr++) part[rr] += cur[rr].dot(yv);
+    if (kPre) {
 #pragma unroll
-  for (int rr = 0; rr < 8; rr++) {
-    const double s = warp_sum(part[rr]);
-    if (lane == 0) acc[warp * 8 + rr] = b[(size_t)I * NB + warp * 8 + rr] - s;
+      for (int rr = 0; rr < 8; rr++) cur[rr] = nxt[rr];
+    } else if (J + 1 < I) {
+#pragma unroll
+      for (int rr = 0; rr < 8; rr++) cur[rr].load(Lrow + (size_t)rr * ld + (size_t)(J + 1) * NB);
+    }
+  }
+  {
+    const double sr = reduce8(part, lane);
+    if ((lane & 3) == 0) acc[rsel] = b_own - sr;
   }
   __syncthreads();
   // y_I = Linv_I acc
   const T* Li = sLi + (size_t)(warp * 8) * NB + 4 * lane;
   double av[4] = {acc[4 * lane], acc[4 * lane + 1], acc[4 * lane + 2], acc[4 * lane + 3]};
+  double q8[8];
 #pragma unroll
   for (int rr = 0; rr < 8; rr++) {
     double lv[4];
     load4(Li + (size_t)rr * NB, lv);
-    const double s = warp_sum(lv[0] * av[0] + lv[1] * av[1] + lv[2] * av[2] + lv[3] * av[3]);
-    if (lane == 0) y[(size_t)I * NB + warp * 8 + rr] = s;
+    q8[rr] = lv[0] * av[0] + lv[1] * av[1] + lv[2] * av[2] + lv[3] * av[3];
+  }
+  {
+    const double yr = reduce8(q8, lane);
+    if ((lane & 3) == 0) y[(size_t)I * NB + rsel] = yr;
   }
   publish_tile(flags + I, epoch, tid);
 }
@@ -767,7 +864,7 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
   T* sLi = reinterpret_cast<T*>(sLi4);  // Linv_I, NB x NB
   __shared__ double red[SV / 32][NB];
   __shared__ double acc[NB];
-  __shared__ int I_s, ok_s;
+  __shared__ int I_s, rdy_s[2];
   if (active && !*active) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) I_s = ntiles - 1 - atomicAdd(ticket, 1);
@@ -779,22 +876,41 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
     for (int i = tid; i < (int)(NB * NB * sizeof(T) / 16); i += SV) dst[i] = src[i];
   }
   double part[4] = {0, 0, 0, 0};
+  const double y_own = tid < NB ? yv[(size_t)I * NB + tid] : 0.0;  // loaded off the chain
   // with an envelope, the tiles of column I past its last nonzero are zero
-  for (int J = env ? env[ntiles + I] : ntiles - 1; J > I; J--) {
-    const T* Lb = L + (size_t)(J * NB + warp * 8) * ld + (size_t)I * NB + 4 * lane;
-    double lv[8][4];  // loaded before waiting for x_J
+  const int J1 = env ? env[ntiles + I] : ntiles - 1;
+  const T* Lcol = L + (size_t)(warp * 8) * ld + (size_t)I * NB + 4 * lane;  // + J NB ld: tile (J, I)
+  constexpr bool kPre = sizeof(T) == 4;
+  Row4<T> cur[8], nxt[8];
+  if (J1 > I) {
 #pragma unroll
-    for (int rr = 0; rr < 8; rr++) load4(Lb + (size_t)rr * ld, lv[rr]);
-    if (tid == 0) ok_s = wait_flag(flags + J, epoch, status, spin_limit) ? 1 : 0;
-    __syncthreads();
-    if (!ok_s) return;
+    for (int rr = 0; rr < 8; rr++) cur[rr].load(Lcol + (size_t)(J1 * NB + rr) * ld);
+  }
+  int lo = J1 + 1, par = 0;  // tiles [lo, J1] are confirmed published
+  for (int J = J1; J > I; J--) {
+    if (kPre && J - 1 > I) {
+#pragma unroll
+      for (int rr = 0; rr < 8; rr++) nxt[rr].load(Lcol + (size_t)((J - 1) * NB + rr) * ld);
+    }
+    if (J < lo) {
+      if (tid == 0) rdy_s[par] = confirm_tiles(flags, J, I, -1, epoch, status, spin_limit, -1) + 1;
+      __syncthreads();
+      lo = rdy_s[par];
+      par ^= 1;
+      if (lo <= 0) return;
+    }
 #pragma unroll
     for (int rr = 0; rr < 8; rr++) {
       const double xr = __ldcg(x + (size_t)J * NB + warp * 8 + rr);
-      part[0] += lv[rr][0] * xr;
-      part[1] += lv[rr][1] * xr;
-      part[2] += lv[rr][2] * xr;
-      part[3] += lv[rr][3] * xr;
+#pragma unroll
+      for (int q = 0; q < 4; q++) part[q] += cur[rr].at(q) * xr;
+    }
+    if (kPre) {
+#pragma unroll
+      for (int rr = 0; rr < 8; rr++) cur[rr] = nxt[rr];
+    } else if (J - 1 > I) {
+#pragma unroll
+      for (int rr = 0; rr < 8; rr++) cur[rr].load(Lcol + (size_t)((J - 1) * NB + rr) * ld);
     }
   }
 #pragma unroll
@@ -804,7 +920,7 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
     double s = 0.0;
 #pragma unroll
     for (int w = 0; w < SV / 32; w++) s += red[w][tid];
-    acc[tid] = yv[(size_t)I * NB + tid] - s;
+    acc[tid] = y_own - s;
   }
   __syncthreads();
   // x_I = Linv_I' acc : x[c] = sum_r Linv[r][c] acc[r]

@@ -766,9 +766,81 @@ __device__ inline int confirm_tiles(const int* flags, int J, int end, int step, 
   return r;
 }
 
+// The two matrices of a tile hop, formed once per factorisation (grid
+// ntiles - 1 x 2, CTA (I - 1, 0) and (I - 1, 1) for I = 1 .. ntiles - 1):
+//   M_I = Linv_I L_I,I-1          at hop + I NB^2           (forward)
+//   Q_I-1 = (L_I,I-1 Linv_I-1)'   at hop + (ntiles + I - 1) NB^2   (backward)
+// so that y_I = c_I - M_I y_I-1 with c_I = Linv_I (b_I - sum_{J < I-1} L_IJ y_J)
+// and x_I-1 = c'_I-1 - Q_I-1 x_I with c'_I-1 = Linv_I-1' (y_I-1 - sum_{J > I}
+// L_J,I-1' x_J): after the wait for the neighbouring tile a solve CTA only
+// applies one register-resident 128 x 128 matrix.  Products in T (FP32 for
+// the mixed factor, FP64 for the FP64 one), 8 x 8 outputs per thread.  A
+// tile L_I,I-1 outside the envelope is zero, and so are M_I and Q_I-1.
+template <typename T>
+static __global__ void __launch_bounds__(256) hop_mat_kernel(const T* __restrict__ S, int ld, int ntiles,
+                                                            const T* __restrict__ Linv, T* __restrict__ hop,
+                                                            const int* __restrict__ active) {
+  constexpr int KC = 16;
+  __shared__ T As[KC][NB + 4];  // As[k][r] = A[r][k0 + k]
+  __shared__ T Bs[KC][NB + 4];  // Bs[k][c] = B[k0 + k][c]
+  if (active && !*active) return;
+  const int I = blockIdx.x + 1;
+  const bool fwd = blockIdx.y == 0;
+  const T* Lt = S + (size_t)I * NB * ld + (size_t)(I - 1) * NB;
+  const T* A = fwd ? Linv + (size_t)I * NB * NB : Lt;
+  const size_t lda = fwd ? NB : (size_t)ld;
+  const T* B = fwd ? Lt : Linv + (size_t)(I - 1) * NB * NB;
+  const size_t ldb = fwd ? (size_t)ld : NB;
+  T* out = hop + (size_t)(fwd ? I : ntiles + I - 1) * NB * NB;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  T acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[i][j] = (T)0;
+  for (int k0 = 0; k0 < NB; k0 += KC) {
+    for (int e = tid; e < NB * KC; e += 256) {
+      const int r = e / KC, kk = e - r * KC;
+      As[kk][r] = A[(size_t)r * lda + k0 + kk];
+      const int kb = e / NB, c = e - kb * NB;
+      Bs[kb][c] = B[(size_t)(k0 + kb) * ldb + c];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < KC; kk++) {
+      T a[8], bb[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 8; j++) bb[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] += a[i] * bb[j];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int r = ty + 16 * i, c = tx + 16 * j;
+      if (fwd)
+        out[(size_t)r * NB + c] = acc[i][j];
+      else
+        out[(size_t)c * NB + r] = acc[i][j];
+    }
+}
+
+// Forward solve L y = b by 128-row tiles.  CTA I (ticket order): streams the
+// tiles J < I - 1 of its row as they are published, forms c_I = Linv_I (b_I -
+// partial) while tile I - 1 is still being solved, then waits for it and
+// finishes y_I = c_I - M_I y_I-1.  Thread (warp w, lane l) holds rows
+// 8 w .. 8 w + 7, columns 4 l .. 4 l + 3 of every 128 x 128 block it applies.
 template <typename T>
 static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict__ L, int ld, int ntiles,
                                                              const T* __restrict__ Linv,
+                                                             const T* __restrict__ hop,
                                                              const double* __restrict__ b, double* __restrict__ y,
                                                              int* __restrict__ ticket, int* __restrict__ flags,
                                                              int epoch, int* __restrict__ status,
@@ -791,32 +863,32 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
   }
   double part[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   const T* Lrow = L + (size_t)(I * NB + warp * 8) * ld + 4 * lane;
-  // the right-hand side of the row this lane finishes, loaded now (off the
-  // chain of the last wait)
+  // the right-hand side of the row this lane finishes, loaded now
   const int rsel = warp * 8 + reduce8_row(lane);
   const double b_own = b[(size_t)I * NB + rsel];
   // with an envelope, the tiles of row I before its first nonzero are zero
   const int J0 = env ? env[I] : 0;
-  // FP32 storage: the next tile's rows are loaded while this one is used
-  constexpr bool kPre = sizeof(T) == 4;
+  const int Jend = I - 1;  // tiles [J0, Jend) are streamed; tile I - 1 goes through M_I
+  constexpr bool kPre = sizeof(T) == 4;  // FP32: the next tile loads while this one is used
   Row4<T> cur[8], nxt[8];
-  if (J0 < I) {
+  if (J0 < Jend) {
 #pragma unroll
     for (int rr = 0; rr < 8; rr++) cur[rr].load(Lrow + (size_t)rr * ld + (size_t)J0 * NB);
   }
   int ready = J0, par = 0;  // tiles [J0, ready) are confirmed published
-  for (int J = J0; J < I; J++) {
-    if (kPre && J + 1 < I) {
+  auto catch_up = [&](int J) -> bool {  // uniform: every thread calls it with the same J
+    if (tid == 0) rdy_s[par] = confirm_tiles(flags, J, I, 1, epoch, status, spin_limit, -1);
+    __syncthreads();
+    ready = rdy_s[par];
+    par ^= 1;  // the other slot is written only after the next barrier
+    return ready >= 0;
+  };
+  for (int J = J0; J < Jend; J++) {
+    if (kPre && J + 1 < Jend) {
 #pragma unroll
       for (int rr = 0; rr < 8; rr++) nxt[rr].load(Lrow + (size_t)rr * ld + (size_t)(J + 1) * NB);
     }
-    if (J >= ready) {
-      if (tid == 0) rdy_s[par] = confirm_tiles(flags, J, I, 1, epoch, status, spin_limit, -1);
-      __syncthreads();
-      ready = rdy_s[par];
-      par ^= 1;  // the other slot is written only after the next barrier
-      if (ready < 0) return;
-    }
+    if (J >= ready && !catch_up(J)) return;
     double yv[4];
     load4_cg(y + (size_t)J * NB + 4 * lane, yv);
 #pragma unroll
@@ -824,17 +896,25 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
     if (kPre) {
 #pragma unroll
       for (int rr = 0; rr < 8; rr++) cur[rr] = nxt[rr];
-    } else if (J + 1 < I) {
+    } else if (J + 1 < Jend) {
 #pragma unroll
       for (int rr = 0; rr < 8; rr++) cur[rr].load(Lrow + (size_t)rr * ld + (size_t)(J + 1) * NB);
     }
   }
+  // the hop matrix's rows, loaded during c_I
+  const bool hop_in = J0 <= I - 1 && I > 0;  // tile I - 1 inside the envelope
+  Row4<T> mrow[8];
+  if (hop_in) {
+    const T* Mr = hop + (size_t)I * NB * NB + (size_t)(warp * 8) * NB + 4 * lane;
+#pragma unroll
+    for (int rr = 0; rr < 8; rr++) mrow[rr].load(Mr + (size_t)rr * NB);
+  }
+  // c_I = Linv_I (b_I - partial)
   {
     const double sr = reduce8(part, lane);
     if ((lane & 3) == 0) acc[rsel] = b_own - sr;
   }
   __syncthreads();
-  // y_I = Linv_I acc
   const T* Li = sLi + (size_t)(warp * 8) * NB + 4 * lane;
   double av[4] = {acc[4 * lane], acc[4 * lane + 1], acc[4 * lane + 2], acc[4 * lane + 3]};
   double q8[8];
@@ -844,16 +924,29 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
     load4(Li + (size_t)rr * NB, lv);
     q8[rr] = lv[0] * av[0] + lv[1] * av[1] + lv[2] * av[2] + lv[3] * av[3];
   }
-  {
-    const double yr = reduce8(q8, lane);
-    if ((lane & 3) == 0) y[(size_t)I * NB + rsel] = yr;
+  double yr = reduce8(q8, lane);
+  // y_I = c_I - M_I y_I-1
+  if (hop_in) {
+    if (I - 1 >= ready && !catch_up(I - 1)) return;
+    double yv[4];
+    load4_cg(y + (size_t)(I - 1) * NB + 4 * lane, yv);
+#pragma unroll
+    for (int rr = 0; rr < 8; rr++) q8[rr] = mrow[rr].dot(yv);
+    yr -= reduce8(q8, lane);
   }
+  if ((lane & 3) == 0) y[(size_t)I * NB + rsel] = yr;
   publish_tile(flags + I, epoch, tid);
 }
 
+// Backward solve L' x = y.  CTA I (reverse ticket order): streams the tiles
+// J > I + 1 of column I (rows of L_J,I) as they are published, forms c'_I =
+// Linv_I' (y_I - partial), then waits for tile I + 1 and finishes
+// x_I = c'_I - Q_I x_I+1 (Q_I row-major: row c of Q_I is column c of
+// L_I+1,I Linv_I, so the last step has the forward kernel's row layout).
 template <typename T>
 static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict__ L, int ld, int ntiles,
                                                              const T* __restrict__ Linv,
+                                                             const T* __restrict__ hop,
                                                              const double* __restrict__ yv, double* __restrict__ x,
                                                              int* __restrict__ ticket, int* __restrict__ flags,
                                                              int epoch, int* __restrict__ status,
@@ -879,26 +972,28 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
   const double y_own = tid < NB ? yv[(size_t)I * NB + tid] : 0.0;  // loaded off the chain
   // with an envelope, the tiles of column I past its last nonzero are zero
   const int J1 = env ? env[ntiles + I] : ntiles - 1;
+  const int Jend = I + 1;  // tiles (Jend, J1] are streamed; tile I + 1 goes through Q_I
   const T* Lcol = L + (size_t)(warp * 8) * ld + (size_t)I * NB + 4 * lane;  // + J NB ld: tile (J, I)
   constexpr bool kPre = sizeof(T) == 4;
   Row4<T> cur[8], nxt[8];
-  if (J1 > I) {
+  if (J1 > Jend) {
 #pragma unroll
     for (int rr = 0; rr < 8; rr++) cur[rr].load(Lcol + (size_t)(J1 * NB + rr) * ld);
   }
   int lo = J1 + 1, par = 0;  // tiles [lo, J1] are confirmed published
-  for (int J = J1; J > I; J--) {
-    if (kPre && J - 1 > I) {
+  auto catch_up = [&](int J) -> bool {  // uniform
+    if (tid == 0) rdy_s[par] = confirm_tiles(flags, J, I, -1, epoch, status, spin_limit, -1) + 1;
+    __syncthreads();
+    lo = rdy_s[par];
+    par ^= 1;
+    return lo > 0;
+  };
+  for (int J = J1; J > Jend; J--) {
+    if (kPre && J - 1 > Jend) {
 #pragma unroll
       for (int rr = 0; rr < 8; rr++) nxt[rr].load(Lcol + (size_t)((J - 1) * NB + rr) * ld);
     }
-    if (J < lo) {
-      if (tid == 0) rdy_s[par] = confirm_tiles(flags, J, I, -1, epoch, status, spin_limit, -1) + 1;
-      __syncthreads();
-      lo = rdy_s[par];
-      par ^= 1;
-      if (lo <= 0) return;
-    }
+    if (J < lo && !catch_up(J)) return;
 #pragma unroll
     for (int rr = 0; rr < 8; rr++) {
       const double xr = __ldcg(x + (size_t)J * NB + warp * 8 + rr);
@@ -908,10 +1003,17 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
     if (kPre) {
 #pragma unroll
       for (int rr = 0; rr < 8; rr++) cur[rr] = nxt[rr];
-    } else if (J - 1 > I) {
+    } else if (J - 1 > Jend) {
 #pragma unroll
       for (int rr = 0; rr < 8; rr++) cur[rr].load(Lcol + (size_t)((J - 1) * NB + rr) * ld);
     }
+  }
+  const bool hop_in = J1 >= I + 1;  // tile I + 1 inside the envelope
+  Row4<T> qrow[8];
+  if (hop_in) {
+    const T* Qr = hop + (size_t)(ntiles + I) * NB * NB + (size_t)(warp * 8) * NB + 4 * lane;
+#pragma unroll
+    for (int rr = 0; rr < 8; rr++) qrow[rr].load(Qr + (size_t)rr * NB);
   }
 #pragma unroll
   for (int q = 0; q < 4; q++) red[warp][4 * lane + q] = part[q];
@@ -923,7 +1025,7 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
     acc[tid] = y_own - s;
   }
   __syncthreads();
-  // x_I = Linv_I' acc : x[c] = sum_r Linv[r][c] acc[r]
+  // c'_I = Linv_I' acc : c'[c] = sum_r Linv[r][c] acc[r]
   const T* Li = sLi + (size_t)(warp * 8) * NB + 4 * lane;
   double p2[4] = {0, 0, 0, 0};
 #pragma unroll
@@ -944,8 +1046,22 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
     double s = 0.0;
 #pragma unroll
     for (int w = 0; w < SV / 32; w++) s += red[w][tid];
-    x[(size_t)I * NB + tid] = s;
+    acc[tid] = s;  // c'_I
   }
+  __syncthreads();
+  const int rsel = warp * 8 + reduce8_row(lane);
+  double xr = acc[rsel];
+  // x_I = c'_I - Q_I x_I+1
+  if (hop_in) {
+    if (I + 1 < lo && !catch_up(I + 1)) return;
+    double xv[4];
+    load4_cg(x + (size_t)(I + 1) * NB + 4 * lane, xv);
+    double q8[8];
+#pragma unroll
+    for (int rr = 0; rr < 8; rr++) q8[rr] = qrow[rr].dot(xv);
+    xr -= reduce8(q8, lane);
+  }
+  if ((lane & 3) == 0) x[(size_t)I * NB + rsel] = xr;
   publish_tile(flags + I, epoch, tid);
 }
 

@@ -147,6 +147,7 @@ class SchurCoreT final : public SchurCore {
     NL_TRY(dx_.alloc(sizeof(double) * (size_t)ld_));
     NL_TRY(part_.alloc(sizeof(double) * (size_t)std::max(kSymvChunks * ld_, 4 * kRedCTAs)));
     NL_TRY(Linv_.alloc(sizeof(T) * (size_t)ntiles_ * NB * NB));
+    NL_TRY(hop_.alloc(sizeof(T) * 2 * (size_t)ntiles_ * NB * NB));
     // the diagonal-tile factor writes only the blocks on and below the
     // diagonal: the strictly upper blocks of every inverse stay zero
     NL_CUDA(cudaMemsetAsync(Linv_.p, 0, Linv_.bytes, st_));
@@ -243,11 +244,13 @@ class SchurCoreT final : public SchurCore {
   nl_status enqueue_solve(const double* b, double* x, int* status, const int* active) {
     NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
     const int* env = envelope ? env_dev_.as<int>() : nullptr;
-    trsv_fwd_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), b, y_.as<double>(),
+    trsv_fwd_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), hop_.as<T>(), b,
+                                                 y_.as<double>(),
                                                  flags_.as<int>(), flags_.as<int>() + 1, 1, status, wait_limit, env,
                                                  active);
     NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
-    trsv_bwd_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), y_.as<double>(), x,
+    trsv_bwd_kernel<T><<<ntiles_, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), hop_.as<T>(),
+                                                 y_.as<double>(), x,
                                                  flags_.as<int>(), flags_.as<int>() + 1, 1, status, wait_limit, env,
                                                  active);
     launches += 2;
@@ -264,7 +267,8 @@ class SchurCoreT final : public SchurCore {
     if (ntiles_ < 2) return NL_ERR_STATE;
     NL_CUDA(cudaMemsetAsync(flags_.p, 0, flags_.bytes, st_));
     set_int_kernel<<<1, 1, 0, st_>>>(flags_.as<int>(), 1);
-    trsv_fwd_kernel<T><<<ntiles_ - 1, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), bS_.as<double>(),
+    trsv_fwd_kernel<T><<<ntiles_ - 1, SV, trsv_smem<T>(), st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), hop_.as<T>(),
+                                                     bS_.as<double>(),
                                                      y_.as<double>(), flags_.as<int>(), flags_.as<int>() + 1, 1,
                                                      status, wait_limit, nullptr, nullptr);
     launches += 2;
@@ -655,6 +659,12 @@ class SchurCoreT final : public SchurCore {
     {
       NvtxRange r("nl:factorize");
       s = enqueue_factor(status, active);
+      // the hop matrices of the solves (M_I = Linv_I L_I,I-1, Q_I)
+      if (s == NL_OK && ntiles_ > 1) {
+        hop_mat_kernel<T><<<dim3(ntiles_ - 1, 2), 256, 0, st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), hop_.as<T>(),
+                                                                 active);
+        launches++;
+      }
     }
     if (s != NL_OK) return s;
     if (tm) NL_CUDA(cudaEventRecord(ev_[4], st_));
@@ -809,7 +819,7 @@ class SchurCoreT final : public SchurCore {
   long long npairs_ = 0;
   bool need_s0_ = false;
   SchurDev d_{};
-  DevBuf U_, V_, W_, Y_, Vinv_, bU_, bV_, bS_, incU_, incV_, y_, r_, dx_, part_, Linv_, flags_, S_, S0_, tcs_;
+  DevBuf U_, V_, W_, Y_, Vinv_, bU_, bV_, bS_, incU_, incV_, y_, r_, dx_, part_, Linv_, hop_, flags_, S_, S0_, tcs_;
   // envelope of S (host) and its first / last arrays on the device (solves)
   std::vector<int> env_first_, env_last_, env_run_;
   DevBuf env_dev_;

@@ -766,16 +766,19 @@ __device__ inline int confirm_tiles(const int* flags, int J, int end, int step, 
   return r;
 }
 
-// The two matrices of a tile hop, formed once per factorisation (grid
-// ntiles - 1 x 2, CTA (I - 1, 0) and (I - 1, 1) for I = 1 .. ntiles - 1):
-//   M_I = Linv_I L_I,I-1          at hop + I NB^2           (forward)
-//   Q_I-1 = (L_I,I-1 Linv_I-1)'   at hop + (ntiles + I - 1) NB^2   (backward)
-// so that y_I = c_I - M_I y_I-1 with c_I = Linv_I (b_I - sum_{J < I-1} L_IJ y_J)
-// and x_I-1 = c'_I-1 - Q_I-1 x_I with c'_I-1 = Linv_I-1' (y_I-1 - sum_{J > I}
-// L_J,I-1' x_J): after the wait for the neighbouring tile a solve CTA only
-// applies one register-resident 128 x 128 matrix.  Products in T (FP32 for
-// the mixed factor, FP64 for the FP64 one), 8 x 8 outputs per thread.  A
-// tile L_I,I-1 outside the envelope is zero, and so are M_I and Q_I-1.
+// The hop matrices of the solves, formed once per factorisation.  For the
+// d-th neighbour (d = 1 .. kHopDepth):
+//   M_d,I = Linv_I L_I,I-d                 (forward, I >= d)
+//   Q_d,I = (L_I+d,I Linv_I)'              (backward, I + d < ntiles)
+// at hop + ((dir kHopDepth + d - 1) ntiles + I) NB^2, dir 0 forward / 1
+// backward.  With them y_I = c_I - sum_d M_d,I y_I-d, where c_I = Linv_I (b_I
+// - sum_{J < I - kHopDepth} L_IJ y_J) needs only tiles published kHopDepth
+// hops earlier, and likewise x_I = c'_I - sum_d Q_d,I x_I+d: after the wait
+// for its neighbour a solve CTA applies one register-resident 128 x 128
+// matrix.  Grid (ntiles - 1, 2 kHopDepth); products in T (FP32 for the mixed
+// factor, FP64 for the FP64 one), 8 x 8 outputs per thread.  A tile L outside
+// the envelope is zero, and so is its hop matrix.
+constexpr int kHopDepth = 2;
 template <typename T>
 static __global__ void __launch_bounds__(256) hop_mat_kernel(const T* __restrict__ S, int ld, int ntiles,
                                                             const T* __restrict__ Linv, T* __restrict__ hop,
@@ -784,14 +787,17 @@ static __global__ void __launch_bounds__(256) hop_mat_kernel(const T* __restrict
   __shared__ T As[KC][NB + 4];  // As[k][r] = A[r][k0 + k]
   __shared__ T Bs[KC][NB + 4];  // Bs[k][c] = B[k0 + k][c]
   if (active && !*active) return;
-  const int I = blockIdx.x + 1;
-  const bool fwd = blockIdx.y == 0;
-  const T* Lt = S + (size_t)I * NB * ld + (size_t)(I - 1) * NB;
+  const bool fwd = blockIdx.y < kHopDepth;
+  const int d = (int)(blockIdx.y % kHopDepth) + 1;
+  // forward: I = d + x, tile (I, I - d); backward: I = x, tile (I + d, I)
+  const int I = fwd ? d + (int)blockIdx.x : (int)blockIdx.x;
+  if ((fwd && I >= ntiles) || (!fwd && I + d >= ntiles)) return;
+  const T* Lt = fwd ? S + (size_t)I * NB * ld + (size_t)(I - d) * NB : S + (size_t)(I + d) * NB * ld + (size_t)I * NB;
   const T* A = fwd ? Linv + (size_t)I * NB * NB : Lt;
   const size_t lda = fwd ? NB : (size_t)ld;
-  const T* B = fwd ? Lt : Linv + (size_t)(I - 1) * NB * NB;
+  const T* B = fwd ? Lt : Linv + (size_t)I * NB * NB;
   const size_t ldb = fwd ? (size_t)ld : NB;
-  T* out = hop + (size_t)(fwd ? I : ntiles + I - 1) * NB * NB;
+  T* out = hop + ((size_t)blockIdx.y * ntiles + I) * NB * NB;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   T acc[8][8];
 #pragma unroll
@@ -833,10 +839,11 @@ static __global__ void __launch_bounds__(256) hop_mat_kernel(const T* __restrict
 }
 
 // Forward solve L y = b by 128-row tiles.  CTA I (ticket order): streams the
-// tiles J < I - 1 of its row as they are published, forms c_I = Linv_I (b_I -
-// partial) while tile I - 1 is still being solved, then waits for it and
-// finishes y_I = c_I - M_I y_I-1.  Thread (warp w, lane l) holds rows
-// 8 w .. 8 w + 7, columns 4 l .. 4 l + 3 of every 128 x 128 block it applies.
+// tiles J < I - kHopDepth of its row as they are published, forms c_I =
+// Linv_I (b_I - partial) while its neighbours are still being solved, then
+// subtracts M_d,I y_I-d for d = kHopDepth .. 1, each as soon as that tile is
+// published.  Thread (warp w, lane l) holds rows 8 w .. 8 w + 7, columns
+// 4 l .. 4 l + 3 of every 128 x 128 block it applies.
 template <typename T>
 static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict__ L, int ld, int ntiles,
                                                              const T* __restrict__ Linv,
@@ -868,7 +875,7 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
   const double b_own = b[(size_t)I * NB + rsel];
   // with an envelope, the tiles of row I before its first nonzero are zero
   const int J0 = env ? env[I] : 0;
-  const int Jend = I - 1;  // tiles [J0, Jend) are streamed; tile I - 1 goes through M_I
+  const int Jend = I - kHopDepth;  // tiles [J0, Jend) are streamed, the last kHopDepth go through M_d,I
   constexpr bool kPre = sizeof(T) == 4;  // FP32: the next tile loads while this one is used
   Row4<T> cur[8], nxt[8];
   if (J0 < Jend) {
@@ -901,14 +908,6 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
       for (int rr = 0; rr < 8; rr++) cur[rr].load(Lrow + (size_t)rr * ld + (size_t)(J + 1) * NB);
     }
   }
-  // the hop matrix's rows, loaded during c_I
-  const bool hop_in = J0 <= I - 1 && I > 0;  // tile I - 1 inside the envelope
-  Row4<T> mrow[8];
-  if (hop_in) {
-    const T* Mr = hop + (size_t)I * NB * NB + (size_t)(warp * 8) * NB + 4 * lane;
-#pragma unroll
-    for (int rr = 0; rr < 8; rr++) mrow[rr].load(Mr + (size_t)rr * NB);
-  }
   // c_I = Linv_I (b_I - partial)
   {
     const double sr = reduce8(part, lane);
@@ -925,11 +924,18 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
     q8[rr] = lv[0] * av[0] + lv[1] * av[1] + lv[2] * av[2] + lv[3] * av[3];
   }
   double yr = reduce8(q8, lane);
-  // y_I = c_I - M_I y_I-1
-  if (hop_in) {
-    if (I - 1 >= ready && !catch_up(I - 1)) return;
+  // y_I = c_I - sum_d M_d,I y_I-d, nearest tile last
+#pragma unroll
+  for (int d = kHopDepth; d >= 1; d--) {
+    const int J = I - d;
+    if (J < 0 || J < J0) continue;  // outside the matrix or the envelope (uniform)
+    Row4<T> mrow[8];
+    const T* Mr = hop + ((size_t)(d - 1) * ntiles + I) * NB * NB + (size_t)(warp * 8) * NB + 4 * lane;
+#pragma unroll
+    for (int rr = 0; rr < 8; rr++) mrow[rr].load(Mr + (size_t)rr * NB);
+    if (J >= ready && !catch_up(J)) return;
     double yv[4];
-    load4_cg(y + (size_t)(I - 1) * NB + 4 * lane, yv);
+    load4_cg(y + (size_t)J * NB + 4 * lane, yv);
 #pragma unroll
     for (int rr = 0; rr < 8; rr++) q8[rr] = mrow[rr].dot(yv);
     yr -= reduce8(q8, lane);
@@ -939,10 +945,10 @@ static __global__ void __launch_bounds__(SV) trsv_fwd_kernel(const T* __restrict
 }
 
 // Backward solve L' x = y.  CTA I (reverse ticket order): streams the tiles
-// J > I + 1 of column I (rows of L_J,I) as they are published, forms c'_I =
-// Linv_I' (y_I - partial), then waits for tile I + 1 and finishes
-// x_I = c'_I - Q_I x_I+1 (Q_I row-major: row c of Q_I is column c of
-// L_I+1,I Linv_I, so the last step has the forward kernel's row layout).
+// J > I + kHopDepth of column I (rows of L_J,I) as they are published, forms
+// c'_I = Linv_I' (y_I - partial), then subtracts Q_d,I x_I+d for
+// d = kHopDepth .. 1 (Q_d,I row-major: row c is column c of L_I+d,I Linv_I,
+// so these steps have the forward kernel's row layout).
 template <typename T>
 static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict__ L, int ld, int ntiles,
                                                              const T* __restrict__ Linv,
@@ -972,7 +978,7 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
   const double y_own = tid < NB ? yv[(size_t)I * NB + tid] : 0.0;  // loaded off the chain
   // with an envelope, the tiles of column I past its last nonzero are zero
   const int J1 = env ? env[ntiles + I] : ntiles - 1;
-  const int Jend = I + 1;  // tiles (Jend, J1] are streamed; tile I + 1 goes through Q_I
+  const int Jend = I + kHopDepth;  // tiles (Jend, J1] are streamed, the nearest kHopDepth go through Q_d,I
   const T* Lcol = L + (size_t)(warp * 8) * ld + (size_t)I * NB + 4 * lane;  // + J NB ld: tile (J, I)
   constexpr bool kPre = sizeof(T) == 4;
   Row4<T> cur[8], nxt[8];
@@ -1007,13 +1013,6 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
 #pragma unroll
       for (int rr = 0; rr < 8; rr++) cur[rr].load(Lcol + (size_t)((J - 1) * NB + rr) * ld);
     }
-  }
-  const bool hop_in = J1 >= I + 1;  // tile I + 1 inside the envelope
-  Row4<T> qrow[8];
-  if (hop_in) {
-    const T* Qr = hop + (size_t)(ntiles + I) * NB * NB + (size_t)(warp * 8) * NB + 4 * lane;
-#pragma unroll
-    for (int rr = 0; rr < 8; rr++) qrow[rr].load(Qr + (size_t)rr * NB);
   }
 #pragma unroll
   for (int q = 0; q < 4; q++) red[warp][4 * lane + q] = part[q];
@@ -1051,11 +1050,18 @@ static __global__ void __launch_bounds__(SV) trsv_bwd_kernel(const T* __restrict
   __syncthreads();
   const int rsel = warp * 8 + reduce8_row(lane);
   double xr = acc[rsel];
-  // x_I = c'_I - Q_I x_I+1
-  if (hop_in) {
-    if (I + 1 < lo && !catch_up(I + 1)) return;
+  // x_I = c'_I - sum_d Q_d,I x_I+d, nearest tile last
+#pragma unroll
+  for (int d = kHopDepth; d >= 1; d--) {
+    const int J = I + d;
+    if (J >= ntiles || J > J1) continue;  // outside the matrix or the envelope (uniform)
+    Row4<T> qrow[8];
+    const T* Qr = hop + ((size_t)(kHopDepth + d - 1) * ntiles + I) * NB * NB + (size_t)(warp * 8) * NB + 4 * lane;
+#pragma unroll
+    for (int rr = 0; rr < 8; rr++) qrow[rr].load(Qr + (size_t)rr * NB);
+    if (J < lo && !catch_up(J)) return;
     double xv[4];
-    load4_cg(x + (size_t)(I + 1) * NB + 4 * lane, xv);
+    load4_cg(x + (size_t)J * NB + 4 * lane, xv);
     double q8[8];
 #pragma unroll
     for (int rr = 0; rr < 8; rr++) q8[rr] = qrow[rr].dot(xv);

@@ -147,7 +147,7 @@ class SchurCoreT final : public SchurCore {
     NL_TRY(dx_.alloc(sizeof(double) * (size_t)ld_));
     NL_TRY(part_.alloc(sizeof(double) * (size_t)std::max(kSymvChunks * ld_, 4 * kRedCTAs)));
     NL_TRY(Linv_.alloc(sizeof(T) * (size_t)ntiles_ * NB * NB));
-    NL_TRY(hop_.alloc(sizeof(T) * 2 * (size_t)ntiles_ * NB * NB));
+    NL_TRY(hop_.alloc(sizeof(T) * 2 * kHopDepth * (size_t)ntiles_ * NB * NB));
     // the diagonal-tile factor writes only the blocks on and below the
     // diagonal: the strictly upper blocks of every inverse stay zero
     NL_CUDA(cudaMemsetAsync(Linv_.p, 0, Linv_.bytes, st_));
@@ -659,10 +659,10 @@ class SchurCoreT final : public SchurCore {
     {
       NvtxRange r("nl:factorize");
       s = enqueue_factor(status, active);
-      // the hop matrices of the solves (M_I = Linv_I L_I,I-1, Q_I)
+      // the hop matrices of the solves (M_d,I, Q_d,I)
       if (s == NL_OK && ntiles_ > 1) {
-        hop_mat_kernel<T><<<dim3(ntiles_ - 1, 2), 256, 0, st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(), hop_.as<T>(),
-                                                                 active);
+        hop_mat_kernel<T><<<dim3(ntiles_ - 1, 2 * kHopDepth), 256, 0, st_>>>(S_.as<T>(), ld_, ntiles_, Linv_.as<T>(),
+                                                                             hop_.as<T>(), active);
         launches++;
       }
     }

@@ -514,8 +514,10 @@ static __global__ void __launch_bounds__(256) trsm_tile_kernel(float* __restrict
 }
 
 // Slice c owns tile rows 8c .. 8c+7 and 127-8c-7 .. 127-8c: equal shares of
-// the lower triangle.  A_tt's lower triangle only is written.  np <= 2 panels,
-// each staged in its own buffer (np x kDiagUpdSmem bytes of shared memory).
+// the lower triangle.  A_tt's lower triangle only is written.  np <= 4
+// panels through two staging buffers (min(np, 2) x kDiagUpdSmem bytes of
+// shared memory): panel p + 2 is copied in while panel p + 1 is applied.
+constexpr int kDiagUpdMaxPanels = 4;
 __device__ inline int diag_slice_row(int c, int p) { return p < 8 ? 8 * c + p : NB - 1 - 8 * c - (p - 8); }
 
 static __global__ void __launch_bounds__(256) diag_update_kernel(float* __restrict__ S, int ld, int t, int p0, int np,
@@ -526,9 +528,9 @@ static __global__ void __launch_bounds__(256) diag_update_kernel(float* __restri
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, c = blockIdx.x;
   const int ra = diag_slice_row(c, lane >> 2), rb = diag_slice_row(c, 8 + (lane >> 2));
   const float* T0 = S + (size_t)t * NB * ld + (size_t)p0 * NB;
-  // with two panels the first was finished before the stream's preceding
-  // kernel (the row-tile TRSM of the second) started: fetch it while that
-  // kernel runs
+  // all panels but the last were finished before the stream's preceding
+  // kernel (the row-tile TRSM of the last one) started: fetch the first while
+  // that kernel runs
   if (np > 1) stage_rows_f32(T0, ld, NB, sm, tid);
   cp_async_commit();
   chain_wait();
@@ -536,20 +538,28 @@ static __global__ void __launch_bounds__(256) diag_update_kernel(float* __restri
     cp_async_wait<0>();
     return;
   }
-  stage_rows_f32(T0 + (np > 1 ? NB : 0), ld, NB, sm + (np > 1 ? NB * kSlLd : 0), tid);
+  if (np > 1)
+    stage_rows_f32(T0 + NB, ld, NB, sm + NB * kSlLd, tid);
+  else
+    stage_rows_f32(T0, ld, NB, sm, tid);
   cp_async_commit();
   float acc[2][4] = {};
-  if (np > 1)
-    cp_async_wait<1>();
-  else
-    cp_async_wait<0>();
-  __syncthreads();
-  slice_mma(sm + ra * kSlLd, sm + rb * kSlLd, sm, lane, w, acc);
-  if (np > 1) {
-    cp_async_wait<0>();
+  for (int p = 0; p < np; p++) {
+    // committed groups so far: panels 0 .. min(p + 1, np - 1) (one empty
+    // group when np == 1); panel p is complete once at most the newest is
+    // still in flight
+    if (p + 1 < np)
+      cp_async_wait<1>();
+    else
+      cp_async_wait<0>();
     __syncthreads();
-    const float* sb = sm + NB * kSlLd;
+    const float* sb = sm + (p & 1) * NB * kSlLd;
     slice_mma(sb + ra * kSlLd, sb + rb * kSlLd, sb, lane, w, acc);
+    __syncthreads();  // every warp is done with buffer p & 1
+    if (p + 2 < np) {
+      stage_rows_f32(T0 + (size_t)(p + 2) * NB, ld, NB, sm + (p & 1) * NB * kSlLd, tid);
+      cp_async_commit();
+    }
   }
   float* D = S + (size_t)t * NB * ld + (size_t)t * NB;
 #pragma unroll

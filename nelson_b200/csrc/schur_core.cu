@@ -308,8 +308,9 @@ class SchurCoreT final : public SchurCore {
           return NL_ERR_CUDA;
       }
     } else if (sizeof(T) == 4 && use_tc) {
-      NL_CUDA(tc_update_f32(reinterpret_cast<float*>(S_.p), ld_, k, t0, nt, col_only ? 1 : 0, 0, pack_slot(k),
-                            nullptr, active, status, st));
+      TcPacks pk{{pack_slot(k), nullptr, nullptr, nullptr}, 1};
+      NL_CUDA(tc_update_f32(reinterpret_cast<float*>(S_.p), ld_, k, t0, nt, col_only ? 1 : 0, 0, pk, active, status,
+                            st));
       launches++;
     } else {
       if (col_only) {
@@ -361,28 +362,36 @@ class SchurCoreT final : public SchurCore {
 
   uint8_t* pack_slot(int k) const { return static_cast<uint8_t*>(tcs_.p) + (size_t)(k % kPackSlots) * tcs_half_; }
 
-  // Tensor-core schedule: panels in pairs, so the bulk of the trailing update
-  // has K = 256 and every trailing tile is read and written once per pair
-  // instead of once per panel, and the panel work split so that only the
-  // chain  potrf(j) -> TRSM + pack of row tile j+1 -> update of tile
-  // (j+1, j+1) -> potrf(j+1)  runs on the main stream; the rest of each step
-  // runs on the auxiliary stream (top priority) or, for the bulk update, on
-  // the side stream (lowest priority).  For the pair (k, k+1):
-  //   main  A1d  tile (k+1, k+1) with panel k (K = 128); potrf(k+1);
-  //         [wait A1r] TRSM + pack of row tile k+2 of panel k+1;
-  //         [wait B of the previous pair] A2d  tile (k+2, k+2) with panels
-  //         k, k+1 (K = 256); potrf(k+2); [wait A2r] TRSM + pack of row tile k+3
-  //         (A1d / A2d are diag_update_kernel, the row-tile TRSMs
-  //         trsm_tile_kernel: 8 CTAs each, FP32 on CUDA cores)
-  //   aux   A1r  block column k+1 below tile k+2 with panel k; TRSM + pack of
-  //         the rows below tile k+2 of panel k+1; [wait B] A2r  block columns
-  //         k+2 (below its diagonal) and k+3 with panels k, k+1; TRSM + pack of
-  //         the rows below tile k+3 of panel k+2
-  //   side  B    tiles of block columns >= k+4 with panels k, k+1.
-  // Packs live in kPackSlots = 4 slots (panel mod 4); B is the last reader of
-  // a pair's slots and the pair after next waits for it before repacking.
+  // Tensor-core schedule: panels in groups of G = kFactorGroup, so the bulk
+  // of the trailing update has K = 128 G and every trailing tile is read and
+  // written once per group instead of once per panel, and the panel work is
+  // split so that only the chain
+  //   potrf(j) -> TRSM + pack of row tile j+1 -> update of tile (j+1, j+1)
+  //   -> potrf(j+1)
+  // runs on the main stream; the rest of each step runs on the auxiliary
+  // stream (top priority) or, for the bulk update, on the side stream (lowest
+  // priority).  For the group of panels k .. k+G-1, after panel j is factored:
+  //   j < k+G-1 (inside the group):
+  //     main  tile (j+1, j+1) with panel j (K = 128); potrf(j+1); [wait the
+  //           aux update] TRSM + pack of row tile j+2 of panel j+1
+  //     aux   block columns j+1 (below its diagonal tile) .. k+G-1 with panel
+  //           j; TRSM + pack of the rows below tile j+2 of panel j+1
+  //   j = k+G-1 (the group's last panel):
+  //     main  [wait B of the previous group] tile (k+G, k+G) with all G
+  //           panels; potrf(k+G); [wait the aux update] TRSM + pack of row
+  //           tile k+G+1
+  //     aux   [wait B] block columns k+G (below its diagonal) .. k+2G-1 with
+  //           all G panels; TRSM + pack of the rows below tile k+G+1
+  //     side  B: tiles of block columns >= k+2G with all G panels.
+  // (The tile updates of the chain are diag_update_kernel, the row-tile TRSMs
+  // trsm_tile_kernel: 8 CTAs each, FP32 on CUDA cores.)  Packs live in
+  // kPackSlots = 2 G slots (panel mod 2 G): a group's B is the last reader of
+  // its slots, and the group after next repacks them only after waiting for it.
+  // With G = 2 this is the pair schedule (one B per two panels); G = 4 halves
+  // the bulk update's HBM traffic again (rank-512 updates).
   enum { EV_PACKF = 0, EV_POTRF, EV_A1R, EV_PACKR, EV_A2R, EV_B, EV_AUX };
-  nl_status enqueue_factor_pairs(int* status, const int* active) {
+  nl_status enqueue_factor_groups(int* status, const int* active) {
+    constexpr int G = kFactorGroup;
     const bool tm = timing && !active;
     const bool tmc = tm && timing_detail;  // per-panel chain events
     const int nT = ntiles_;
@@ -405,12 +414,14 @@ class SchurCoreT final : public SchurCore {
       for (int j = 0; j < ncols && j < nt; j++) t += std::max(0, nt - std::max(j, rb));
       return t;
     };
-    auto upd = [&](int k, bool pair, int t0, int nt, int ncols, int rb, cudaStream_t st) -> nl_status {
-      nt = std::min(nt, env_end(k + 1) - t0 + 1);  // tile rows past the envelope get zero updates
+    // update with panels k .. k + npan - 1
+    auto upd = [&](int k, int npan, int t0, int nt, int ncols, int rb, cudaStream_t st) -> nl_status {
+      nt = std::min(nt, env_end(k + npan - 1) - t0 + 1);  // tile rows past the envelope get zero updates
       if (nt <= 0 || tiles_of(nt, ncols, rb) <= 0) return NL_OK;
       if (tm) NL_CUDA(cudaEventRecord(upd_ev_[nev], st));
-      NL_CUDA(tc_update_f32(S, ld_, k, t0, nt, ncols, rb, pack_slot(k), pair ? pack_slot(k + 1) : nullptr, active,
-                            status, st));
+      TcPacks pk{{nullptr, nullptr, nullptr, nullptr}, npan};
+      for (int i = 0; i < npan; i++) pk.p[i] = pack_slot(k + i);
+      NL_CUDA(tc_update_f32(S, ld_, k, t0, nt, ncols, rb, pk, active, status, st));
       if (tm) NL_CUDA(cudaEventRecord(upd_ev_[nev + 1], st));
       nev += 2;
       nupd++;
@@ -420,9 +431,10 @@ class SchurCoreT final : public SchurCore {
     };
     // TRSM + pack of panel j's rows [r0, r0 + nrows) (absolute rows, tile aligned)
     auto trsm_pack = [&](int j, int r0, int nrows, cudaStream_t st) -> nl_status {
-      // rows past the envelope are zero in L; the pack covers every row the
-      // pair updates of panels j - 1 .. j + 1 read
-      nrows = std::min(nrows, (env_end(j + 1) + 1) * NB - r0);
+      // rows past the envelope are zero in L; the pack covers every row that
+      // an update of panel j's group reads (env_end of its last panel, at
+      // most j + G - 1)
+      nrows = std::min(nrows, (env_end(j + G - 1) + 1) * NB - r0);
       if (nrows <= 0) return NL_OK;
       // the TRSM writes the BF16 pack of its rows in its epilogue
       trsm_kernel<T><<<cdiv(nrows, TRSM_ROWS), 256, trsm_smem<T>(), st>>>(S_.as<T>(), ld_, j, r0, nrows,
@@ -443,8 +455,8 @@ class SchurCoreT final : public SchurCore {
     // (only where no event wait sits between the two)
     auto diag_upd = [&](int t, int p0, int np, bool pdl) -> nl_status {
       if (tmc) cudaEventRecord(upd_ev_[10 * nT + 4 * (t - 1) + 2], st_);
-      NL_CUDA(launch_chain(diag_update_kernel, kSliceCtas, 256, np * kDiagUpdSmem, pdl && !tmc, S, ld_, t, p0, np,
-                           active));
+      NL_CUDA(launch_chain(diag_update_kernel, kSliceCtas, 256, std::min(np, 2) * kDiagUpdSmem, pdl && !tmc, S, ld_,
+                           t, p0, np, active));
       if (tmc) cudaEventRecord(upd_ev_[10 * nT + 4 * (t - 1) + 3], st_);
       launches++;
       return NL_OK;
@@ -475,45 +487,54 @@ class SchurCoreT final : public SchurCore {
     NL_CUDA(wait(st3_, EV_POTRF));
     if ((r = trsm_pack(0, 2 * NB, ld_ - 2 * NB, st3_)) != NL_OK) return r;
     bool pending_b = false;
-    for (int k = 0; k + 1 < nT; k += 2) {
-      // panel k is factored; row tile k+1 of it is packed (main), the rest
-      // is being packed on the aux stream
-      NL_CUDA(rec(EV_PACKF, st_));
-      if ((r = diag_upd(k + 1, k, 1, true)) != NL_OK) return r;  // A1d
-      NL_CUDA(wait(st3_, EV_PACKF));
-      if ((r = upd(k, false, k + 1, nT - k - 1, 1, 1, st3_)) != NL_OK) return r;  // A1r
-      NL_CUDA(rec(EV_A1R, st3_));
-      if ((r = potrf(k + 1)) != NL_OK) return r;
-      NL_CUDA(rec(EV_POTRF, st_));
-      NL_CUDA(wait(st3_, EV_POTRF));
-      if ((r = trsm_pack(k + 1, (k + 3) * NB, ld_ - (k + 3) * NB, st3_)) != NL_OK) return r;
-      NL_CUDA(rec(EV_PACKR, st3_));
-      NL_CUDA(wait(st_, EV_A1R));
-      if (k + 2 >= nT) break;
-      trsm_first(k + 1);
-      // pair update: A2d on main, A2r on aux, B on the side stream
-      NL_CUDA(rec(EV_PACKF, st_));
-      if (pending_b) NL_CUDA(wait(st_, EV_B));
-      if ((r = diag_upd(k + 2, k, 2, !pending_b)) != NL_OK) return r;  // A2d
-      NL_CUDA(wait(st3_, EV_PACKF));
-      if (pending_b) NL_CUDA(wait(st3_, EV_B));
-      if ((r = upd(k, true, k + 2, nT - k - 2, 2, 1, st3_)) != NL_OK) return r;  // A2r
-      NL_CUDA(rec(EV_A2R, st3_));
-      if (k + 4 < nT) {
-        NL_CUDA(wait(st2_, EV_PACKF));
-        NL_CUDA(wait(st2_, EV_PACKR));
-        if ((r = upd(k, true, k + 4, nT - k - 4, 0, 0, st2_)) != NL_OK) return r;  // B
-        NL_CUDA(rec(EV_B, st2_));
-        pending_b = true;
-      } else {
-        pending_b = false;
+    for (int k = 0; k + 1 < nT; k += G) {
+      const int g = std::min(G, nT - k);  // panels k .. k + g - 1 (the last group may be short)
+      for (int i = 0; i < g; i++) {
+        const int j = k + i;  // panel j is factored, row tile j+1 of it packed (main)
+        if (j + 1 >= nT) break;
+        NL_CUDA(rec(EV_PACKF, st_));
+        if (i + 1 < g) {
+          // inside the group: panel j -> block columns j+1 .. k+g-1
+          if ((r = diag_upd(j + 1, j, 1, true)) != NL_OK) return r;
+          NL_CUDA(wait(st3_, EV_PACKF));
+          if ((r = upd(j, 1, j + 1, nT - j - 1, k + g - 1 - j, 1, st3_)) != NL_OK) return r;
+          NL_CUDA(rec(EV_A1R, st3_));
+          if ((r = potrf(j + 1)) != NL_OK) return r;
+          NL_CUDA(rec(EV_POTRF, st_));
+          NL_CUDA(wait(st3_, EV_POTRF));
+          if ((r = trsm_pack(j + 1, (j + 3) * NB, ld_ - (j + 3) * NB, st3_)) != NL_OK) return r;
+          NL_CUDA(rec(EV_PACKR, st3_));
+          NL_CUDA(wait(st_, EV_A1R));
+          if (j + 2 >= nT) break;
+          trsm_first(j + 1);
+        } else {
+          // the group's last panel: the next group's block columns (main:
+          // its first diagonal tile; aux: the rest), then the bulk (side)
+          const int kn = k + g;  // first panel of the next group
+          if (pending_b) NL_CUDA(wait(st_, EV_B));
+          if ((r = diag_upd(kn, k, g, !pending_b)) != NL_OK) return r;
+          NL_CUDA(wait(st3_, EV_PACKF));
+          if (pending_b) NL_CUDA(wait(st3_, EV_B));
+          if ((r = upd(k, g, kn, nT - kn, G, 1, st3_)) != NL_OK) return r;
+          NL_CUDA(rec(EV_A2R, st3_));
+          if (kn + G < nT) {
+            NL_CUDA(wait(st2_, EV_PACKF));
+            NL_CUDA(wait(st2_, EV_PACKR));
+            if ((r = upd(k, g, kn + G, nT - kn - G, 0, 0, st2_)) != NL_OK) return r;  // B
+            NL_CUDA(rec(EV_B, st2_));
+            pending_b = true;
+          } else {
+            pending_b = false;
+          }
+          if ((r = potrf(kn)) != NL_OK) return r;
+          NL_CUDA(rec(EV_POTRF, st_));
+          NL_CUDA(wait(st3_, EV_POTRF));
+          if ((r = trsm_pack(kn, (kn + 2) * NB, ld_ - (kn + 2) * NB, st3_)) != NL_OK) return r;
+          NL_CUDA(rec(EV_PACKR, st3_));
+          NL_CUDA(wait(st_, EV_A2R));
+          if (kn + 1 < nT) trsm_first(kn);
+        }
       }
-      if ((r = potrf(k + 2)) != NL_OK) return r;
-      NL_CUDA(rec(EV_POTRF, st_));
-      NL_CUDA(wait(st3_, EV_POTRF));
-      if ((r = trsm_pack(k + 2, (k + 4) * NB, ld_ - (k + 4) * NB, st3_)) != NL_OK) return r;
-      NL_CUDA(wait(st_, EV_A2R));
-      if (k + 3 < nT) trsm_first(k + 2);
     }
     // join: the solves that follow read every tile and Linv
     NL_CUDA(rec(EV_AUX, st3_));
@@ -559,7 +580,7 @@ class SchurCoreT final : public SchurCore {
   }
 
   nl_status enqueue_factor(int* status, const int* active) {
-    if (sizeof(T) == 4 && use_tc) return enqueue_factor_pairs(status, active);
+    if (sizeof(T) == 4 && use_tc) return enqueue_factor_groups(status, active);
     const bool tm = timing && !active;
     if (tm && (int)upd_ev_.size() < 4 * ntiles_) {
       for (size_t i = upd_ev_.size(); i < (size_t)4 * ntiles_; i++) {
@@ -835,7 +856,8 @@ class SchurCoreT final : public SchurCore {
   cublasHandle_t cublas2_ = nullptr;
   DevBuf ws2_;
   size_t tcs_half_ = 0;
-  static constexpr int kPackSlots = 4;
+  static constexpr int kFactorGroup = 4;  // panels per bulk trailing update (K = 512)
+  static constexpr int kPackSlots = 2 * kFactorGroup;
   std::vector<cudaEvent_t> upd_ev_;
 
  public:

@@ -12,8 +12,8 @@
 //                  core (m-group g, k-group h') at byte (4 g + h') * 128 of the
 //                  chunk, i.e. LBO (K step) = 128 B, SBO (M step) = 512 B.
 // tc_syrk_kernel   one CTA per lower 128x128 output tile.  One thread runs a
-//                  two-stage pipeline over the K-chunks (K = 128 for one
-//                  panel, 256 for a pair of panels): one cp.async.bulk per
+//                  two-stage pipeline over the K-chunks (K = 128 per panel,
+//                  up to four panels per update): one cp.async.bulk per
 //                  operand chunk (A hi, A lo, B hi, B lo) lands on the
 //                  stage's mbarrier while the previous chunk's six
 //                  tcgen05.mma (M = N = 128, K = 16, kind::f16, BF16 in, FP32
@@ -165,8 +165,7 @@ constexpr int kSmemBytes = TB * kStageLd * 4;  // 67,584 B >= 2 stages x 32 KB o
 static_assert(kStages * kStageBytes <= kSmemBytes, "operand stages alias the epilogue staging");
 
 __global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int ld, int k, int t0, int nt,
-                                                      int ncols, int rb, const uint8_t* __restrict__ pack,
-                                                      const uint8_t* __restrict__ pack2,
+                                                      int ncols, int rb, const TcPacks packs,
                                                       const int* __restrict__ active, int* __restrict__ status) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ __align__(8) uint64_t bar_load[2], bar_mma[2];
@@ -219,12 +218,12 @@ __global__ void __launch_bounds__(256) tc_syrk_kernel(float* __restrict__ S, int
 
   if (tid == 0) {
     int ok = 1;
-    const int nch = kChunksPerPanel * (pack2 ? 2 : 1);
+    const int nch = kChunksPerPanel * packs.n;
     // chunk c: stage c & 1, its (c >> 1)-th use of that stage
     auto issue_load = [&](int c) {
       uint8_t* st = smem + (size_t)(c & 1) * kStageBytes;
       const int panel = c / kChunksPerPanel, cc = c % kChunksPerPanel;
-      const uint8_t* pk = panel == 0 ? pack : pack2;
+      const uint8_t* pk = static_cast<const uint8_t*>(packs.p[panel]);
       const int first = k + 1 + panel;  // first tile row of that pack
       const uint8_t* pa = pk + (size_t)(t0 + I - first) * kPackTile + (size_t)cc * kChunkBytes;
       const uint8_t* pb = pk + (size_t)(t0 + J - first) * kPackTile + (size_t)cc * kChunkBytes;
@@ -340,9 +339,9 @@ cudaError_t tc_prepare() {
   return cudaFuncSetAttribute(tc_syrk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
 }
 
-cudaError_t tc_update_f32(float* S, int ld, int k, int t0, int nt, int ncols, int rb, const void* pack,
-                          const void* pack2,
+cudaError_t tc_update_f32(float* S, int ld, int k, int t0, int nt, int ncols, int rb, const TcPacks& packs,
                           const int* active, int* status, cudaStream_t st) {
+  if (packs.n < 1 || packs.n > kTcMaxPanels) return cudaErrorInvalidValue;
   static int attr_dev = -1;
   int dev = 0;
   cudaGetDevice(&dev);
@@ -359,8 +358,7 @@ cudaError_t tc_update_f32(float* S, int ld, int k, int t0, int nt, int ncols, in
   }
   if (grid <= 0) return cudaSuccess;
   tc_syrk_kernel<<<grid, 256, kSmemBytes, st>>>(S, ld, k, t0, nt, ncols > nt ? nt : ncols, ncols > 0 ? rb : 0,
-                                                static_cast<const uint8_t*>(pack),
-                                                static_cast<const uint8_t*>(pack2), active, status);
+                                                packs, active, status);
   return cudaGetLastError();
 }
 
@@ -368,7 +366,8 @@ cudaError_t tc_syrk_f32(float* S, int ld, int k, int t0, int nt, void* scratch, 
                         cudaStream_t st) {
   cudaError_t e = tc_pack_f32(S, ld, k, 0, nt * TB, scratch, active, st);
   if (e != cudaSuccess) return e;
-  return tc_update_f32(S, ld, k, t0, nt, 0, 0, scratch, nullptr, active, status, st);
+  TcPacks pk{{scratch, nullptr, nullptr, nullptr}, 1};
+  return tc_update_f32(S, ld, k, t0, nt, 0, 0, pk, active, status, st);
 }
 
 }  // namespace nl

@@ -154,6 +154,42 @@ __device__ double cta_max(int cnt, F f, double* sh) {
   return r;
 }
 
+// Sums the 36 per-lane values v over the warp by recursive halving (a
+// reduce-scatter): at offsets 16, 8, 4, 2, 1 each lane keeps half of its
+// values (odd counts padded with a zero) and adds its partner's copy of them.
+// 37 exchanges instead of 36 butterflies of 5.  Lane l ends with two sums,
+// out[i] of entry idx[i] (-1 for a padding slot); every entry lands on
+// exactly one lane, and the order of the additions depends on the lane
+// numbers alone.
+__device__ inline void reduce_scatter36(const double (&v)[36], int lane, double (&out)[2], int (&idx)[2]) {
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2, b0 = lane & 1;
+  double a[18];
+#pragma unroll
+  for (int i = 0; i < 18; i++)
+    a[i] = (b4 ? v[18 + i] : v[i]) + __shfl_xor_sync(0xffffffffu, b4 ? v[i] : v[18 + i], 16);
+  double c[10];
+#pragma unroll
+  for (int i = 0; i < 9; i++)
+    c[i] = (b3 ? a[9 + i] : a[i]) + __shfl_xor_sync(0xffffffffu, b3 ? a[i] : a[9 + i], 8);
+  c[9] = 0.0;
+  double d[6];
+#pragma unroll
+  for (int i = 0; i < 5; i++)
+    d[i] = (b2 ? c[5 + i] : c[i]) + __shfl_xor_sync(0xffffffffu, b2 ? c[i] : c[5 + i], 4);
+  d[5] = 0.0;
+  double f[4];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+    f[i] = (b1 ? d[3 + i] : d[i]) + __shfl_xor_sync(0xffffffffu, b1 ? d[i] : d[3 + i], 2);
+  f[3] = 0.0;
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    out[i] = (b0 ? f[2 + i] : f[i]) + __shfl_xor_sync(0xffffffffu, b0 ? f[i] : f[2 + i], 1);
+    const int l1 = 2 * b0 + i, l2 = 3 * b1 + l1, l3 = 5 * b2 + l2;
+    idx[i] = (l1 < 3 && l2 < 5 && l3 < 9) ? 18 * b4 + 9 * b3 + l3 : -1;
+  }
+}
+
 template <int BC>
 __device__ double cost(const BProb& P, double* sh) {
   return cta_sum(
@@ -334,7 +370,7 @@ __device__ bool compute_increment(const BProb& P, double mu, double* smem, int* 
   for (int b = warp; b < P.nS; b += nw) {
     const int bi = P.s_i[b], bj = P.s_j[b];
     const int t0 = P.s_ptr[b], t1 = P.s_ptr[b + 1];
-    if (BC == 6) {
+    if constexpr (BC == 6) {
       // lane l takes pairs l, l + 32, ... and accumulates the whole 6 x 6
       // product (32 pairs' loads in flight per warp); the lanes' sums are then
       // added by a butterfly, so the order depends on the pair count alone
@@ -359,12 +395,15 @@ __device__ bool compute_increment(const BProb& P, double mu, double* smem, int* 
           for (int c = 0; c < BC; c++)
             acc[r * BC + c] += y[r * 3] * w[c * 3] + y[r * 3 + 1] * w[c * 3 + 1] + y[r * 3 + 2] * w[c * 3 + 2];
       }
+      double sum[2];
+      int ent[2];
+      reduce_scatter36(acc, lane, sum, ent);
 #pragma unroll
-      for (int q = 0; q < NE; q++) {
-        const double v = warp_all_sum(acc[q]);
-        if (lane == (q & 31)) {
+      for (int i = 0; i < 2; i++) {
+        const int q = ent[i];
+        if (q >= 0) {
           const int r = q / BC, c = q % BC;
-          double m = -v;
+          double m = -sum[i];
           if (bi == bj) m += P.U[(size_t)bi * NE + q];
           // block (i, j) of the upper S at lower (j BC + c, i BC + r)
           const int row = bj * BC + c, col = bi * BC + r;

@@ -220,18 +220,21 @@ class BASection {
     if (perm.size() != size_t(desc_.nc_var)) throw Error(NL_ERR_ARG, "setUser2InternalIndexesU");
     check(nl_set_user2internal_u(h_, perm.data()), "nl_set_user2internal_u");
   }
-  // In place of DoubleSection::permuteAMD_SchurU (nelson/DoubleSection.hpp:30-63):
-  // a reverse Cuthill-McKee internal camera order from the same camera graph,
-  // applied when the structure is built (structureReady); it narrows the
-  // envelope that SolverEnvelopeSchurCuda factors.
-  void permuteRCM_SchurU() { rcm_ = true; }
+  // DoubleSection::permuteAMD_SchurU (nelson/DoubleSection.hpp:30-63): the
+  // approximate minimum degree order of the camera graph (the pattern of
+  // U + W W'), applied when the structure is built (structureReady).
+  void permuteAMD_SchurU() { order_ = Order::Amd; }
+  // Alternatively a reverse Cuthill-McKee order of the same graph: it narrows
+  // the envelope that SolverEnvelopeSchurCuda factors.
+  void permuteRCM_SchurU() { order_ = Order::Rcm; }
   // DoubleSection::structureReady (nelson/DoubleSection.hpp:83-246).
   void structureReady() {
     const bool weighted = std::any_of(w_.begin(), w_.end(), [](double x) { return x != 1.0; });
     check(nl_add_ba_edges(h_, int(cam_.size()), cam_.data(), camFixed_.data(), pt_.data(),
                           ptFixed_.data(), obs_.data(), weighted ? w_.data() : nullptr),
           "nl_add_ba_edges");
-    if (rcm_) check(nl_permute_rcm_u(h_), "nl_permute_rcm_u");
+    if (order_ == Order::Rcm) check(nl_permute_rcm_u(h_), "nl_permute_rcm_u");
+    if (order_ == Order::Amd) check(nl_permute_amd_u(h_), "nl_permute_amd_u");
     check(nl_structure_ready(h_), "nl_structure_ready");
     std::vector<int>().swap(cam_);
     std::vector<int>().swap(camFixed_);
@@ -297,7 +300,8 @@ class BASection {
   nl_problem_desc desc_{};
   Hessian hessian_;
   std::vector<int> cam_, camFixed_, pt_, ptFixed_;
-  bool rcm_ = false;
+  enum class Order { User, Amd, Rcm };
+  Order order_ = Order::User;
   std::vector<double> obs_, w_;
 };
 

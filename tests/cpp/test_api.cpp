@@ -79,7 +79,7 @@ Scene make_scene(unsigned seed) {
   return s;
 }
 
-BASection make_section(const Scene& s, int precision, unsigned seed, bool rcm = false) {
+BASection make_section(const Scene& s, int precision, unsigned seed, int order = 0) {  // order: 0 user, 1 RCM, 2 AMD
   BASection ba(9, s.nc, s.np, s.ncFix, s.npFix, precision, 500.0, 320.0, 240.0, 0);
   std::mt19937_64 g(seed);
   std::uniform_real_distribution<double> U(-1, 1);
@@ -97,7 +97,8 @@ BASection make_section(const Scene& s, int precision, unsigned seed, bool rcm = 
     ba.addEdge(NodeId(s.cam[e], s.camFixed[e] ? nelson_b200::NodeType::Fixed : nelson_b200::NodeType::Variable),
                NodeId(s.pt[e], s.ptFixed[e] ? nelson_b200::NodeType::Fixed : nelson_b200::NodeType::Variable),
                s.obs[2 * e], s.obs[2 * e + 1]);
-  if (rcm) ba.permuteRCM_SchurU();
+  if (order == 1) ba.permuteRCM_SchurU();
+  if (order == 2) ba.permuteAMD_SchurU();
   ba.structureReady();
   return ba;
 }
@@ -177,13 +178,23 @@ int main() {
 
       // 5. the reverse Cuthill-McKee camera order (permuteRCM_SchurU): the same
       //    trace up to rounding (another elimination order)
-      BASection r1 = make_section(s, prec, 11, true);
+      BASection r1 = make_section(s, prec, 11, 1);
       nelson_b200::LevenbergMarquardt<nelson_b200::SolverEnvelopeSchurCuda> lmR;
       lmR.settings().maxNumIt = 10;
       const auto rR = lmR.solveOnDevice(r1);
       const double dr = trace_diff(lmD.stats(), lmR.stats(), &n);
       (void)rR;
       expect(dr <= tol, "RCM order per-iteration cost vs user order (rel)", dr, tol);
+
+      // 6. the approximate minimum degree order (permuteAMD_SchurU): the same
+      //    trace up to rounding
+      BASection a1 = make_section(s, prec, 11, 2);
+      nelson_b200::LevenbergMarquardt<nelson_b200::SolverCholeskySchurCuda> lmA;
+      lmA.settings().maxNumIt = 10;
+      const auto rA = lmA.solveOnDevice(a1);
+      const double da = trace_diff(lmD.stats(), lmA.stats(), &n);
+      (void)rA;
+      expect(da <= tol, "AMD order per-iteration cost vs user order (rel)", da, tol);
     }
   } catch (const nelson_b200::Error& e) {
     std::printf("FAIL exception: %s\n", e.what());

@@ -188,12 +188,12 @@ int main() {
 
       // 6. the approximate minimum degree order (permuteAMD_SchurU): the same
       //    trace up to rounding
-      BASection a1 = make_section(s, prec, 11, 2);
-      nelson_b200::LevenbergMarquardt<nelson_b200::SolverCholeskySchurCuda> lmA;
-      lmA.settings().maxNumIt = 10;
-      const auto rA = lmA.solveOnDevice(a1);
-      const double da = trace_diff(lmD.stats(), lmA.stats(), &n);
-      (void)rA;
+      BASection am = make_section(s, prec, 11, 2);
+      nelson_b200::LevenbergMarquardt<nelson_b200::SolverCholeskySchurCuda> lmAmd;
+      lmAmd.settings().maxNumIt = 10;
+      const auto rAmd = lmAmd.solveOnDevice(am);
+      const double da = trace_diff(lmD.stats(), lmAmd.stats(), &n);
+      (void)rAmd;
       expect(da <= tol, "AMD order per-iteration cost vs user order (rel)", da, tol);
     }
   } catch (const nelson_b200::Error& e) {

@@ -157,6 +157,7 @@ class SchurCoreT final : public SchurCore {
                             cudaMemcpyHostToDevice, st_));
     NL_TRY(flags_.alloc(sizeof(int) * (size_t)(ntiles_ + 1)));
     NL_TRY(S_.alloc(sizeof(T) * (size_t)ld_ * ld_));
+    s_cleared_ = false;
     need_s0_ = refine_sweeps > 0 || keep_schur;
     if (need_s0_) NL_TRY(S0_.alloc(sizeof(T) * (size_t)ld_ * ld_));
     if (sizeof(T) == 4 && use_tc) {
@@ -661,8 +662,16 @@ class SchurCoreT final : public SchurCore {
     if (tm) NL_CUDA(cudaEventRecord(ev_[2], st_));
     nvtxRangePop();
     nvtxRangePushA("nl:schur");
-    NL_CUDA(cudaMemsetAsync(S_.p, 0, S_.bytes, st_));
-    if (need_s0_) NL_CUDA(cudaMemsetAsync(S0_.p, 0, S0_.bytes, st_));
+    if (!s_cleared_) {
+      // the first time the whole of S (and S0); afterwards only the envelope
+      NL_CUDA(cudaMemsetAsync(S_.p, 0, S_.bytes, st_));
+      if (need_s0_) NL_CUDA(cudaMemsetAsync(S0_.p, 0, S0_.bytes, st_));
+      s_cleared_ = true;
+    } else {
+      clear_envelope_kernel<T><<<ld_, 128, 0, st_>>>(S_.as<T>(), need_s0_ ? S0_.as<T>() : nullptr, ld_, NB,
+                                                     env_dev_.as<int>(), active);
+      launches++;
+    }
     {
       const int grid = std::max(1, std::min(cdiv(nS_, kSchurWarps), 148 * 8));
       NL_CUDA(cudaMemsetAsync(sched_.p, 0, sizeof(int), st_));
@@ -844,6 +853,7 @@ class SchurCoreT final : public SchurCore {
   // envelope of S (host) and its first / last arrays on the device (solves)
   std::vector<int> env_first_, env_last_, env_run_;
   DevBuf env_dev_;
+  bool s_cleared_ = false;  // S / S0 have had their one full clear (enqueue_increment)
   // last tile row that panel k's TRSM and updates must cover
   int env_end(int k) const { return envelope ? env_run_[std::min(k, ntiles_ - 1)] : ntiles_ - 1; }
   DevBuf v_uid_, w_row_ptr_, w_col_, w_row_, w_col_ptr_, w_col_uid_, u_diag_, s_i_, s_j_, s_uuid_, s_ptr_, pa_, pb_, s_order_,

@@ -307,6 +307,26 @@ static __global__ void __launch_bounds__(WARPS * 32, 2) schur_kernel(SchurDev d,
   }
 }
 
+// Zero the tiles of S (and S0) that can hold nonzeros: row r of tile row I
+// over columns [env_first[I] NB, (I + 1) NB) -- the Cholesky envelope.  The
+// other tiles are zero after the first full clear and stay exactly zero: the
+// Schur blocks lie inside the envelope, and the factorisation writes only
+// zeros there (TRSM and trailing updates of zero tiles).  One CTA per row.
+template <typename T>
+static __global__ void clear_envelope_kernel(T* __restrict__ S, T* __restrict__ S0, int ld, int nb,
+                                             const int* __restrict__ env_first, const int* __restrict__ active) {
+  if (active && !*active) return;
+  const int r = blockIdx.x, I = r / nb;
+  const size_t c0 = (size_t)env_first[I] * nb, c1 = (size_t)(I + 1) * nb;
+  constexpr int EPV = 16 / (int)sizeof(T);  // elements per 16-byte store
+  using V16 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  const V16 z = {};
+  for (size_t c = c0 + (size_t)threadIdx.x * EPV; c < c1; c += (size_t)blockDim.x * EPV) {
+    *reinterpret_cast<V16*>(S + (size_t)r * ld + c) = z;
+    if (S0) *reinterpret_cast<V16*>(S0 + (size_t)r * ld + c) = z;
+  }
+}
+
 // Identity on the padded tail of S (rows n .. ld-1).
 template <typename T>
 static __global__ void pad_identity_kernel(T* __restrict__ S, T* __restrict__ S0, int n, int ld,

@@ -392,6 +392,47 @@ nl_status nl_solver_compute_increment(nl_solver* s, double rel_lambda, double ab
 /* nl_set_solver_kind for the solver-only handle. */
 nl_status nl_solver_set_kind(nl_solver* s, int kind);
 
+/* ---- SingleSection on the device: SE(2) pose graphs of 2D scans --------- */
+/* The reference's single-section problem as its tests build it
+ * (nelson/SingleSection.hpp:63-139, nelson/tests/testGaussNewton2DScansAlign.cpp:
+ * 36-120): nv variable and nf fixed SE(2) poses (x, y, theta); every edge
+ * joins a model pose a and a target pose b with npts point-to-line terms
+ * e_k = (T_a m_k - T_b q_k) . (R_a n_k) (model points m and normals n in a's
+ * frame, target points q in b's frame).  Edge evaluation, the Hessian blocks
+ * (U, b), the damped tiled Cholesky of U (SolverCholeskyDense,
+ * nelson/SolverCholeskyDense.hpp:39-67) and the left SE(2) update
+ * T <- exp(d) T run on the device; LM / GN control on the host. */
+typedef struct nl_pose2d nl_pose2d;
+nl_status nl_pose2d_create(int nv, int nf, int precision, int device, nl_pose2d** out);
+nl_status nl_pose2d_destroy(nl_pose2d* h);
+/* poses as (x, y, theta) triples; either pointer may be null */
+nl_status nl_pose2d_set_poses(nl_pose2d* h, const double* var_xyt, const double* fix_xyt);
+nl_status nl_pose2d_get_poses(nl_pose2d* h, double* var_xyt);
+/* SingleSection::addEdge with a point-to-line edge; a_fixed / b_fixed select
+ * the fixed poses (not both).  Points are (x, y) pairs. */
+nl_status nl_pose2d_add_edge(nl_pose2d* h, int a, int a_fixed, int b, int b_fixed, int npts,
+                             const double* model_pts, const double* model_normals, const double* target_pts);
+/* SingleSection::setUser2InternalIndexes / permuteAMD (nelson/SingleSection.hpp:
+ * 26-52); before nl_pose2d_structure_ready */
+nl_status nl_pose2d_set_user2internal(nl_pose2d* h, const int* perm);
+nl_status nl_pose2d_permute_amd(nl_pose2d* h);
+nl_status nl_pose2d_structure_ready(nl_pose2d* h);
+/* NL_SOLVER_DENSE (default) or NL_SOLVER_ENVELOPE for the Cholesky of U */
+nl_status nl_pose2d_set_solver_kind(nl_pose2d* h, int kind);
+/* SingleSection::update: the cost (sum of e_k^2) and, with hessian, U and b */
+nl_status nl_pose2d_update(nl_pose2d* h, int hessian, double* chi2);
+/* The Hessian of the last update with hessian set, as a dense symmetric
+ * (3 nv) x (3 nv) row-major matrix, and b, both in user pose order (the
+ * section's hessian().H / b); either pointer may be null */
+nl_status nl_pose2d_get_hessian(nl_pose2d* h, double* H, double* b);
+/* LevenbergMarquardt::solve / GaussNewton::solve on the section; trace
+ * records as for nl_lm_solve (8 doubles: iteration, sub-iteration, chi2, mu,
+ * rho, |delta|^2, ok, accepted). */
+nl_status nl_pose2d_lm_solve(nl_pose2d* h, const nl_lm_settings* st, nl_solve_report* rep, double* trace,
+                             int trace_cap);
+nl_status nl_pose2d_gn_solve(nl_pose2d* h, const nl_gn_settings* st, nl_solve_report* rep, double* trace,
+                             int trace_cap);
+
 /* Device self-test of the mixed path's tensor-core trailing update: builds a
  * random FP32 matrix of ntiles x 128 rows on `device`, applies the panel-0
  * update with the tcgen05 kernel and with the CUDA-core kernel, and returns

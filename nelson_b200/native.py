@@ -96,6 +96,10 @@ EXPORTS = [
     "nl_permute_amd_u", "nl_amd_order_camera_graph", "nl_amd_order", "nl_symbolic_fill",
     "nl_set_wait_limit", "nl_check_wait_timeout", "nl_unroll_record", "nl_unroll_adjoint",
     "nl_batch_create", "nl_batch_destroy", "nl_batch_autotune", "nl_batch_lm_solve",
+    "nl_pose2d_create", "nl_pose2d_destroy", "nl_pose2d_set_poses", "nl_pose2d_get_poses", "nl_pose2d_add_edge",
+    "nl_pose2d_set_user2internal", "nl_pose2d_permute_amd", "nl_pose2d_structure_ready",
+    "nl_pose2d_set_solver_kind", "nl_pose2d_update", "nl_pose2d_get_hessian", "nl_pose2d_lm_solve",
+    "nl_pose2d_gn_solve",
     "nl_status_string",
     "nl_version",
 ]
@@ -140,6 +144,19 @@ def load(build_if_missing: bool = True):
     L.nl_batch_lm_solve.argtypes = [vp, C.POINTER(LMSettings), i, i, vp, vp, C.POINTER(d)]
     L.nl_unroll_adjoint.argtypes = [vp, vp, vp, vp, vp, vp, vp, C.POINTER(UnrollReport)]
     L.nl_check_wait_timeout.argtypes = [vp]
+    L.nl_pose2d_create.argtypes = [i, i, i, i, C.POINTER(vp)]
+    L.nl_pose2d_destroy.argtypes = [vp]
+    L.nl_pose2d_set_poses.argtypes = [vp, vp, vp]
+    L.nl_pose2d_get_poses.argtypes = [vp, vp]
+    L.nl_pose2d_add_edge.argtypes = [vp, i, i, i, i, i, vp, vp, vp]
+    L.nl_pose2d_set_user2internal.argtypes = [vp, vp]
+    L.nl_pose2d_permute_amd.argtypes = [vp]
+    L.nl_pose2d_structure_ready.argtypes = [vp]
+    L.nl_pose2d_set_solver_kind.argtypes = [vp, i]
+    L.nl_pose2d_get_hessian.argtypes = [vp, vp, vp]
+    L.nl_pose2d_update.argtypes = [vp, i, C.POINTER(d)]
+    L.nl_pose2d_lm_solve.argtypes = [vp, C.POINTER(LMSettings), C.POINTER(SolveReport), vp, i]
+    L.nl_pose2d_gn_solve.argtypes = [vp, C.POINTER(GNSettings), C.POINTER(SolveReport), vp, i]
     for name in EXPORTS:  # fails loudly if the library lacks an entry point
         if name not in ("nl_status_string", "nl_version"):
             getattr(L, name).restype = C.c_int
@@ -573,3 +590,110 @@ class SchurSolverGPU:
         _chk(self.L, self.L.nl_solver_compute_increment(self.h, rel, abs_, _p(du), _p(dv), C.byref(ok)),
              "nl_solver_compute_increment")
         return bool(ok.value), du, dv
+
+
+class Pose2DGPU:
+    """Device SingleSection of SE(2) poses with point-to-line edges (nl_pose2d_*):
+    addEdge / permuteAMD / setUser2InternalIndexes / structureReady / update
+    of nelson/SingleSection.hpp:26-139 with the edge of
+    nelson/tests/testGaussNewton2DScansAlign.cpp:36-120, solved by
+    LevenbergMarquardt / GaussNewton with the tiled Cholesky of U."""
+
+    def __init__(self, nv, nf=1, precision=PREC_FP64, device=0):
+        self.L = load()
+        self.nv, self.nf = nv, nf
+        h = C.c_void_p()
+        _chk(self.L, self.L.nl_pose2d_create(C.c_int(nv), C.c_int(nf), C.c_int(precision), C.c_int(device),
+                                             C.byref(h)), "nl_pose2d_create")
+        self.h = h
+
+    @classmethod
+    def from_scan_align(cls, prob, precision=PREC_FP64, order="natural", perm=None, device=0):
+        """Build the section of a ScanAlignProblem: scan 0 is the fixed pose,
+        scan i > 0 the variable pose i - 1; edge (i, j) holds scan i's points
+        and normals as the model and scan j's points as the target."""
+        g = cls(len(prob.poses0), 1, precision, device)
+        g.set_poses(prob.poses0, prob.poses_true[:1])
+        for i, j in prob.edges:
+            g.add_edge(i - 1 if i else 0, i == 0, j - 1 if j else 0, j == 0, prob.scans[i], prob.normals[i],
+                       prob.scans[j])
+        if order == "amd":
+            g.permute_amd()
+        elif perm is not None:
+            g.set_user2internal(perm)
+        g.structure_ready()
+        return g
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.nl_pose2d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, rc, what):
+        _chk(self.L, rc, what)
+
+    def set_poses(self, var_xyt, fix_xyt=None):
+        v = np.ascontiguousarray(var_xyt, np.float64).reshape(self.nv, 3)
+        f = None if fix_xyt is None else np.ascontiguousarray(fix_xyt, np.float64).reshape(self.nf, 3)
+        self._c(self.L.nl_pose2d_set_poses(self.h, _p(v), _p(f)), "nl_pose2d_set_poses")
+
+    def get_poses(self):
+        out = np.zeros((self.nv, 3))
+        self._c(self.L.nl_pose2d_get_poses(self.h, _p(out)), "nl_pose2d_get_poses")
+        return out
+
+    def add_edge(self, a, a_fixed, b, b_fixed, model_pts, model_normals, target_pts):
+        m = np.ascontiguousarray(model_pts, np.float64).reshape(-1, 2)
+        n = np.ascontiguousarray(model_normals, np.float64).reshape(-1, 2)
+        t = np.ascontiguousarray(target_pts, np.float64).reshape(-1, 2)
+        if not (len(m) == len(n) == len(t)):
+            raise NelsonError("add_edge: model points, normals and target points differ in length")
+        self._c(self.L.nl_pose2d_add_edge(self.h, C.c_int(a), C.c_int(int(a_fixed)), C.c_int(b),
+                                          C.c_int(int(b_fixed)), C.c_int(len(m)), _p(m), _p(n), _p(t)),
+                "nl_pose2d_add_edge")
+
+    def set_user2internal(self, perm):
+        p = np.ascontiguousarray(perm, np.int32)
+        self._c(self.L.nl_pose2d_set_user2internal(self.h, _p(p)), "nl_pose2d_set_user2internal")
+
+    def permute_amd(self):
+        self._c(self.L.nl_pose2d_permute_amd(self.h), "nl_pose2d_permute_amd")
+
+    def structure_ready(self):
+        self._c(self.L.nl_pose2d_structure_ready(self.h), "nl_pose2d_structure_ready")
+
+    def set_solver_kind(self, kind: int):
+        self._c(self.L.nl_pose2d_set_solver_kind(self.h, C.c_int(kind)), "nl_pose2d_set_solver_kind")
+
+    def update(self, hessian=True):
+        v = C.c_double()
+        self._c(self.L.nl_pose2d_update(self.h, C.c_int(int(hessian)), C.byref(v)), "nl_pose2d_update")
+        return v.value
+
+    def hessian(self):
+        """(H, b) of the last update(True): dense, user pose order."""
+        n = 3 * self.nv
+        H = np.zeros((n, n))
+        b = np.zeros(n)
+        self._c(self.L.nl_pose2d_get_hessian(self.h, _p(H), _p(b)), "nl_pose2d_get_hessian")
+        return H, b
+
+    def lm_solve(self, settings=None, trace_cap=4096):
+        s = settings or LMSettings()
+        rep = SolveReport()
+        tr = np.zeros((max(trace_cap, 1), TRACE_STRIDE))
+        self._c(self.L.nl_pose2d_lm_solve(self.h, C.byref(s), C.byref(rep), _p(tr), trace_cap), "nl_pose2d_lm_solve")
+        return REASONS[rep.reason], tr[:rep.n_trace].copy(), rep.iterations
+
+    def gn_solve(self, settings=None, trace_cap=4096):
+        s = settings or GNSettings()
+        rep = SolveReport()
+        tr = np.zeros((max(trace_cap, 1), TRACE_STRIDE))
+        self._c(self.L.nl_pose2d_gn_solve(self.h, C.byref(s), C.byref(rep), _p(tr), trace_cap), "nl_pose2d_gn_solve")
+        return REASONS[rep.reason], tr[:rep.n_trace].copy(), rep.iterations

@@ -423,3 +423,75 @@ def save_bal(path: str, p: BAProblem) -> None:
             f.write(f"{v:.17g}\n")
         for v in p.pts.reshape(-1):
             f.write(f"{v:.17g}\n")
+
+
+# ---------------------------------------------------------------------------
+# 2D scan alignment: SE(2) pose graphs with point-to-line edges, shaped like
+# the single-section tests of the reference (nelson/tests/
+# testGaussNewton2DScansAlign.cpp:485-737): world points in [-100, 100]^2
+# with random unit normals, num_poses + 1 scan poses exp((10, 10, pi) * U[-1, 1]^3)
+# (scan 0 is the fixed pose), each scan the world points in its own frame;
+# edges (i, j), i < j, with scan i as model (points and normals) and scan j as
+# target, all pairs ("full") or a star from scan 0 plus random pairs
+# ("sparse"); the variable poses start at exp(noise * U[-1, 1]^3) T_true.
+
+
+def se2_exp(v):
+    """exp of se(2) (vx, vy, w): (R(w), V(w) (vx, vy))."""
+    vx, vy, w = v
+    c, s = np.cos(w), np.sin(w)
+    if abs(w) > 1e-9:
+        a, b = s / w, (1.0 - c) / w
+    else:
+        a, b = 1.0 - w * w / 6.0, 0.5 * w
+    return np.array([a * vx - b * vy, b * vx + a * vy, w])
+
+
+def se2_compose(d, p):
+    """exp(d) * T_p for pose p = (x, y, theta): theta + w, R(w) t + V(w) v."""
+    t = se2_exp(d)
+    c, s = np.cos(d[2]), np.sin(d[2])
+    return np.array([c * p[0] - s * p[1] + t[0], s * p[0] + c * p[1] + t[1], p[2] + d[2]])
+
+
+@dataclass
+class ScanAlignProblem:
+    poses_true: np.ndarray   # (num_poses + 1, 3); row 0 is the fixed pose
+    poses0: np.ndarray       # (num_poses, 3) start of the variable poses
+    scans: list              # (npts, 2) points of each scan in its own frame
+    normals: list            # (npts, 2)
+    edges: list              # (i, j): model scan i, target scan j
+    name: str = "scan_align"
+
+
+def scan_align_scene(num_poses: int = 15, points_per_scan: int = 3000, noise=(0.01, 0.01, np.pi / 1000.0),
+                     full_edges: bool = True, seed: int = 5) -> ScanAlignProblem:
+    rng = np.random.default_rng(seed)
+    world = 100.0 * rng.uniform(-1, 1, size=(points_per_scan, 2))
+    nrm = np.empty((points_per_scan, 2))
+    for k in range(points_per_scan):
+        while True:
+            v = rng.uniform(-1, 1, size=2)
+            if v @ v >= 1e-3:
+                break
+        nrm[k] = v / np.linalg.norm(v)
+    poses = np.array([se2_compose(np.array([10.0, 10.0, np.pi]) * rng.uniform(-1, 1, size=3), np.zeros(3))
+                      for _ in range(num_poses + 1)])
+    scans, normals = [], []
+    for x, y, th in poses:
+        c, s = np.cos(th), np.sin(th)
+        R = np.array([[c, -s], [s, c]])
+        scans.append((world - np.array([x, y])) @ R)       # R' (X - t)
+        normals.append(nrm @ R)
+    n_all = num_poses + 1
+    if full_edges:
+        edges = [(i, j) for i in range(n_all) for j in range(i + 1, n_all)]
+    else:
+        edges = [(0, i) for i in range(1, n_all)]
+        for i in range(1, n_all - 1):
+            for _ in range(int(rng.integers(0, n_all - i - 1))):
+                edges.append((i, int(rng.integers(i + 1, n_all))))
+    sig = np.asarray(noise, dtype=float)
+    poses0 = np.array([se2_compose(sig * rng.uniform(-1, 1, size=3), poses[i]) for i in range(1, n_all)])
+    return ScanAlignProblem(poses, poses0, scans, normals, edges,
+                            name=f"scan_align {num_poses} poses {'full' if full_edges else 'sparse'}")

@@ -23,8 +23,9 @@ computeIncrement + oplus + cost + gain ratio, then the Jacobian pass.
 --config 1 (or 0) runs the same measurement on that workload: config 1 is 200
 9-parameter cameras, 50,000 points, 375 k observations (S 1,800 x 1,800).
 --config 3 times the batched configuration (256 uneven problems in one
-persistent launch).  The default config-2 run also carries compact config-1
-and config-3 figures under other_configs (--no-extras skips them).
+persistent launch).  The default config-2 run also carries compact config-1,
+config-3 and 2D scan-alignment (device SingleSection) figures under
+other_configs (--no-extras skips them).
 
 --impl reference times the FP64 CPU oracle (the restatement of the reference's
 CPU path) on the same workload; under torchrun only rank 0 runs it.
@@ -373,6 +374,54 @@ def measure_single(cfg, its, warmup, device):
     return out
 
 
+def measure_pose2d(device, cpu=True):
+    """The device SingleSection (2D scan alignment with point-to-line edges,
+    nl_pose2d_*): the reference test's problem solved to convergence, and a
+    2,000-pose graph, FP64 and mixed.  solve_ms spans the whole LM solve on
+    the library's stream (CUDA events; the host control between launches
+    included).  The CPU baseline is the numpy FP64 oracle of the same solve
+    (the full solve on the small problem, 3 LM iterations on the large one)."""
+    from nelson_b200 import native as N
+    from nelson_b200.problems import pose_graph_scene, scan_align_scene
+    from oracle.pose2d import Pose2DOracle
+    cores = len(os.sched_getaffinity(0))
+    out = {}
+    for key, prob, cpu_its in (("reference_problem", scan_align_scene(15, 3000, seed=5), 100),
+                               ("pose_graph_2000", pose_graph_scene(2000, 500, 3000, 30, seed=7), 3)):
+        npts = sum(len(prob.scans[i]) for i, _ in prob.edges)
+        res = {"workload": f"{prob.name}: {len(prob.poses0)} variable poses + 1 fixed, {len(prob.edges)} edges, "
+                           f"{npts} point-to-line residuals, AMD order, envelope solver",
+               "edge_bytes_per_update": npts * 48}
+        traces = {}
+        for name, prec in (("fp64", N.PREC_FP64), ("mixed", N.PREC_MIXED)):
+            g = N.Pose2DGPU.from_scan_align(prob, precision=prec, order="amd", device=device)
+            g.set_solver_kind(N.SOLVER_ENVELOPE)
+            g.lm_solve(N.LMSettings(maxNumIt=2), trace_cap=0)   # warm-up
+            g.set_poses(prob.poses0)
+            reason, tr, it = g.lm_solve()
+            ms = g.last_report["device_ms"]
+            chi2 = g.update(True)
+            res[name] = {"solve_ms": ms, "iterations": it, "reason": reason, "lm_iters_per_s": max(it, 1) / (ms / 1e3),
+                         "chi2_after": chi2, "chi2_below_1e-12": bool(chi2 < 1e-12)}
+            traces[name] = tr
+            g.close()
+        if cpu:
+            o = Pose2DOracle(prob)
+            t0 = time.perf_counter()
+            r_o, tro, it_o = o.lm_solve(maxNumIt=cpu_its)
+            dt = time.perf_counter() - t0
+            res["cpu_baseline"] = {"value": max(it_o, 1) / dt, "unit": UNIT, "cores": cores, "kind": "port",
+                                   "sample": f"{max(it_o, 1)} LM iteration(s), numpy FP64 oracle ({dt:.2f} s)"}
+            n = min(len(tro), len(traces["fp64"]))
+            rows = [k for k in range(n) if tro[k, 2] > 1e-9]
+            rel = max((abs(traces["fp64"][k, 2] - tro[k, 2]) / tro[k, 2] for k in rows), default=None)
+            res["oracle_parity"] = {"records_compared": len(rows), "fp64_chi2_max_rel_err": rel,
+                                    "ok": bool(rel is not None and rel <= 1e-6)}
+            res["fp64_vs_cpu"] = res["fp64"]["lm_iters_per_s"] / res["cpu_baseline"]["value"]
+        out[key] = res
+    return out
+
+
 def run_batch(args, rank, world):
     """--config 3: the batched configuration as the bench line."""
     import torch
@@ -600,7 +649,8 @@ def main():
     others = None
     if rank == 0 and world == 1 and args.config == 2 and not args.no_extras:
         others = {"config1": measure_single(1, args.steps, 3, local),
-                  "config3": measure_batch(10, 3, local, cpu=not args.no_cpu_baseline)}
+                  "config3": measure_batch(10, 3, local, cpu=not args.no_cpu_baseline),
+                  "pose2d": measure_pose2d(local, cpu=not args.no_cpu_baseline)}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -416,6 +416,9 @@ nl_status nl_pose2d_add_edge(nl_pose2d* h, int a, int a_fixed, int b, int b_fixe
  * 26-52); before nl_pose2d_structure_ready */
 nl_status nl_pose2d_set_user2internal(nl_pose2d* h, const int* perm);
 nl_status nl_pose2d_permute_amd(nl_pose2d* h);
+/* Reverse Cuthill-McKee order of the pose graph (no counterpart in the
+ * reference): the narrow-profile order for NL_SOLVER_ENVELOPE */
+nl_status nl_pose2d_permute_rcm(nl_pose2d* h);
 nl_status nl_pose2d_structure_ready(nl_pose2d* h);
 /* NL_SOLVER_DENSE (default) or NL_SOLVER_ENVELOPE for the Cholesky of U */
 nl_status nl_pose2d_set_solver_kind(nl_pose2d* h, int kind);

@@ -700,6 +700,98 @@ class GaussNewton {
 };
 
 // ---------------------------------------------------------------------------
+// ScanAlignSection: a SingleSection (nelson/SingleSection.hpp:26-139) of SE(2)
+// poses (x, y, theta) joined by point-to-line edges, the problem of
+// nelson/tests/testGaussNewton2DScansAlign.cpp:36-120, resident on one GPU.
+// Call order as in the reference: construct, setPoses, addEdge ...,
+// optionally permuteAMD / setUser2InternalIndexes, structureReady, then
+// solveLM / solveGN (the loops of LevenbergMarquardt.hpp:36-146 and
+// GaussNewton.hpp:32-127 on this section, with the tiled Cholesky of U).
+class ScanAlignSection {
+ public:
+  ScanAlignSection(int numPoses, int numFixedPoses = 1, int precision = NL_PREC_FP64, int device = 0)
+      : nv_(numPoses), nf_(numFixedPoses) {
+    check(nl_pose2d_create(numPoses, numFixedPoses, precision, device, &h_), "nl_pose2d_create");
+  }
+  ~ScanAlignSection() {
+    if (h_) nl_pose2d_destroy(h_);
+  }
+  ScanAlignSection(const ScanAlignSection&) = delete;
+  ScanAlignSection& operator=(const ScanAlignSection&) = delete;
+
+  int numParameters() const { return nv_; }
+  // (x, y, theta) triples; either may be null
+  void setPoses(const double* variable, const double* fixed) {
+    check(nl_pose2d_set_poses(h_, variable, fixed), "nl_pose2d_set_poses");
+  }
+  std::vector<double> poses() const {
+    std::vector<double> p(size_t(nv_) * 3);
+    check(nl_pose2d_get_poses(h_, p.data()), "nl_pose2d_get_poses");
+    return p;
+  }
+  // addEdge(NodeId a, NodeId b, new PointLineEdge(model, normals, target)):
+  // npts (x, y) pairs each; model points and normals in a's frame, target
+  // points in b's frame
+  void addEdge(NodeId a, NodeId b, int npts, const double* model, const double* normals, const double* target) {
+    check(nl_pose2d_add_edge(h_, a.id, a.type == NodeType::Fixed, b.id, b.type == NodeType::Fixed, npts, model,
+                             normals, target),
+          "nl_pose2d_add_edge");
+  }
+  void permuteAMD() { check(nl_pose2d_permute_amd(h_), "nl_pose2d_permute_amd"); }
+  void permuteRCM() { check(nl_pose2d_permute_rcm(h_), "nl_pose2d_permute_rcm"); }
+  void setUser2InternalIndexes(const std::vector<int>& perm) {
+    if ((int)perm.size() != nv_) throw Error(NL_ERR_ARG, "setUser2InternalIndexes");
+    check(nl_pose2d_set_user2internal(h_, perm.data()), "nl_pose2d_set_user2internal");
+  }
+  void structureReady() { check(nl_pose2d_structure_ready(h_), "nl_pose2d_structure_ready"); }
+  void setSolverKind(int kind) { check(nl_pose2d_set_solver_kind(h_, kind), "nl_pose2d_set_solver_kind"); }
+  // update(hessian): returns chi2 (hessian().chi2())
+  double update(bool hessian) {
+    double c = 0.0;
+    check(nl_pose2d_update(h_, hessian ? 1 : 0, &c), "nl_pose2d_update");
+    return c;
+  }
+  // hessian().H() (dense, symmetric, user pose order) and b()
+  void hessian(std::vector<double>& H, std::vector<double>& b) const {
+    const size_t n = size_t(nv_) * 3;
+    H.resize(n * n);
+    b.resize(n);
+    check(nl_pose2d_get_hessian(h_, H.data(), b.data()), "nl_pose2d_get_hessian");
+  }
+  TerminationReason solveLM(const LevenbergMarquardtSettings& st = {}, std::vector<IterationRecord>* trace = nullptr) {
+    const nl_lm_settings c = st.c();
+    return solve([&](nl_solve_report* r, double* t, int cap) { return nl_pose2d_lm_solve(h_, &c, r, t, cap); },
+                 trace, "nl_pose2d_lm_solve");
+  }
+  TerminationReason solveGN(const GaussNewtonSettings& st = {}, std::vector<IterationRecord>* trace = nullptr) {
+    const nl_gn_settings c = st.c();
+    return solve([&](nl_solve_report* r, double* t, int cap) { return nl_pose2d_gn_solve(h_, &c, r, t, cap); },
+                 trace, "nl_pose2d_gn_solve");
+  }
+  const nl_solve_report& lastReport() const { return rep_; }
+
+ private:
+  template <class F>
+  TerminationReason solve(F f, std::vector<IterationRecord>* trace, const char* what) {
+    const int cap = trace ? 4096 : 0;
+    std::vector<double> t(size_t(cap > 0 ? cap : 1) * 8);
+    check(f(&rep_, cap ? t.data() : nullptr, cap), what);
+    if (trace) {
+      trace->clear();
+      for (int i = 0; i < rep_.n_trace; i++) {
+        const double* r = t.data() + size_t(i) * 8;
+        trace->push_back(IterationRecord{int(r[0]), int(r[1]), r[2], r[3], r[4], r[5], r[6] != 0.0, r[7] != 0.0});
+      }
+    }
+    return TerminationReason(rep_.reason);
+  }
+  nl_pose2d* h_ = nullptr;
+  int nv_, nf_;
+  nl_solve_report rep_{};
+};
+
+
+// ---------------------------------------------------------------------------
 // Problem files.
 // Problem / load: the visibility-list format of the reference's samples
 // (nelson/samples/Problems.h:4-12, Problems.cpp:8-30): "nCameras nPoints

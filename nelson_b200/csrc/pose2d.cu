@@ -133,6 +133,7 @@ static __global__ void pose2d_chi2_kernel(const double* __restrict__ ev, int ne,
   __shared__ double red[32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   double s = 0.0;
+#pragma unroll 4
   for (int e = tid; e < ne; e += blockDim.x) s += ev[(size_t)e * kEdgeVals];
   s = p2_warp_sum(s);
   if (lane == 0) red[warp] = s;
@@ -238,7 +239,7 @@ struct Pose2DOps {
         P2_CUDA(cudaGetLastError());
       }
     }
-    pose2d_chi2_kernel<<<1, 256, 0, h->st>>>(h->ebuf.as<double>(), ne, h->scal.as<double>());
+    pose2d_chi2_kernel<<<1, 1024, 0, h->st>>>(h->ebuf.as<double>(), ne, h->scal.as<double>());
     P2_CUDA(cudaGetLastError());
     P2_CUDA(cudaMemcpyAsync(h->pin, h->scal.p, sizeof(double), cudaMemcpyDeviceToHost, h->st));
     if (hess) read_b();
@@ -522,6 +523,26 @@ nl_status nl_pose2d_permute_amd(nl_pose2d* h) {
   return nl_amd_order(h->nv, (int)r.size(), r.data(), c.data(), h->perm.data());
 }
 
+// Reverse Cuthill-McKee order of the same pose graph: the order that keeps
+// U's profile narrow for the envelope solver (on a chain with short loop
+// closures the band stays within a tile or two, where the fill-reducing
+// minimum degree order scatters it).  Each edge between two variable poses
+// enters as a two-pose clique.
+nl_status nl_pose2d_permute_rcm(nl_pose2d* h) {
+  if (!h || h->ready) return NL_ERR_ARG;
+  std::vector<int> cam, pt;
+  int k = 0;
+  for (size_t e = 0; e < h->ea.size(); e++)
+    if (h->ea[e] < h->nv && h->eb[e] < h->nv) {
+      cam.push_back(h->ea[e]);
+      cam.push_back(h->eb[e]);
+      pt.push_back(k);
+      pt.push_back(k);
+      k++;
+    }
+  return nl_rcm_order(h->nv, k, (int)cam.size(), cam.data(), pt.data(), h->perm.data());
+}
+
 // SingleSection::structureReady: the U pattern (upper CSC in internal order),
 // the (edge, sign) lists of every U block and b entry, device buffers, the
 // tiled Cholesky of the reduced system U.
@@ -725,7 +746,17 @@ nl_status nl_pose2d_gn_solve(nl_pose2d* h, const nl_gn_settings* st, nl_solve_re
     NL_CUDA(cudaSetDevice(h->device));
     Pose2DOps P{h};
     int ntr = 0, its = 0;
+    cudaEvent_t e0, e1;
+    NL_CUDA(cudaEventCreate(&e0));
+    NL_CUDA(cudaEventCreate(&e1));
+    NL_CUDA(cudaEventRecord(e0, h->st));
     const int reason = gn_loop(P, *st, trace, std::max(0, trace_cap), &ntr, &its);
+    NL_CUDA(cudaEventRecord(e1, h->st));
+    NL_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     if (rep) {
       rep->reason = reason;
       rep->iterations = its;
@@ -733,7 +764,7 @@ nl_status nl_pose2d_gn_solve(nl_pose2d* h, const nl_gn_settings* st, nl_solve_re
       rep->n_trace = ntr;
       rep->chi2 = h->chi2;
       rep->mu = 0.0;
-      rep->device_ms = 0.0;
+      rep->device_ms = ms;
     }
   } catch (const P2Error& e) {
     return e.s;

@@ -97,7 +97,7 @@ EXPORTS = [
     "nl_set_wait_limit", "nl_check_wait_timeout", "nl_unroll_record", "nl_unroll_adjoint",
     "nl_batch_create", "nl_batch_destroy", "nl_batch_autotune", "nl_batch_lm_solve",
     "nl_pose2d_create", "nl_pose2d_destroy", "nl_pose2d_set_poses", "nl_pose2d_get_poses", "nl_pose2d_add_edge",
-    "nl_pose2d_set_user2internal", "nl_pose2d_permute_amd", "nl_pose2d_structure_ready",
+    "nl_pose2d_set_user2internal", "nl_pose2d_permute_amd", "nl_pose2d_permute_rcm", "nl_pose2d_structure_ready",
     "nl_pose2d_set_solver_kind", "nl_pose2d_update", "nl_pose2d_get_hessian", "nl_pose2d_lm_solve",
     "nl_pose2d_gn_solve",
     "nl_status_string",
@@ -151,6 +151,7 @@ def load(build_if_missing: bool = True):
     L.nl_pose2d_add_edge.argtypes = [vp, i, i, i, i, i, vp, vp, vp]
     L.nl_pose2d_set_user2internal.argtypes = [vp, vp]
     L.nl_pose2d_permute_amd.argtypes = [vp]
+    L.nl_pose2d_permute_rcm.argtypes = [vp]
     L.nl_pose2d_structure_ready.argtypes = [vp]
     L.nl_pose2d_set_solver_kind.argtypes = [vp, i]
     L.nl_pose2d_get_hessian.argtypes = [vp, vp, vp]
@@ -619,6 +620,8 @@ class Pose2DGPU:
                        prob.scans[j])
         if order == "amd":
             g.permute_amd()
+        elif order == "rcm":
+            g.permute_rcm()
         elif perm is not None:
             g.set_user2internal(perm)
         g.structure_ready()
@@ -665,6 +668,9 @@ class Pose2DGPU:
     def permute_amd(self):
         self._c(self.L.nl_pose2d_permute_amd(self.h), "nl_pose2d_permute_amd")
 
+    def permute_rcm(self):
+        self._c(self.L.nl_pose2d_permute_rcm(self.h), "nl_pose2d_permute_rcm")
+
     def structure_ready(self):
         self._c(self.L.nl_pose2d_structure_ready(self.h), "nl_pose2d_structure_ready")
 
@@ -689,6 +695,7 @@ class Pose2DGPU:
         rep = SolveReport()
         tr = np.zeros((max(trace_cap, 1), TRACE_STRIDE))
         self._c(self.L.nl_pose2d_lm_solve(self.h, C.byref(s), C.byref(rep), _p(tr), trace_cap), "nl_pose2d_lm_solve")
+        self.last_report = {n: getattr(rep, n) for n, _ in SolveReport._fields_}
         return REASONS[rep.reason], tr[:rep.n_trace].copy(), rep.iterations
 
     def gn_solve(self, settings=None, trace_cap=4096):
@@ -696,4 +703,5 @@ class Pose2DGPU:
         rep = SolveReport()
         tr = np.zeros((max(trace_cap, 1), TRACE_STRIDE))
         self._c(self.L.nl_pose2d_gn_solve(self.h, C.byref(s), C.byref(rep), _p(tr), trace_cap), "nl_pose2d_gn_solve")
+        self.last_report = {n: getattr(rep, n) for n, _ in SolveReport._fields_}
         return REASONS[rep.reason], tr[:rep.n_trace].copy(), rep.iterations

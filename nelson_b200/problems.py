@@ -495,3 +495,32 @@ def scan_align_scene(num_poses: int = 15, points_per_scan: int = 3000, noise=(0.
     poses0 = np.array([se2_compose(sig * rng.uniform(-1, 1, size=3), poses[i]) for i in range(1, n_all)])
     return ScanAlignProblem(poses, poses0, scans, normals, edges,
                             name=f"scan_align {num_poses} poses {'full' if full_edges else 'sparse'}")
+
+
+def pose_graph_scene(num_poses: int = 2000, points_per_scan: int = 500, closures: int = 3000, max_span: int = 30,
+                     noise=(0.01, 0.01, np.pi / 1000.0), seed: int = 7) -> ScanAlignProblem:
+    """A long 2D scan-alignment pose graph: the scans of scan_align_scene
+    joined in a chain (i, i + 1) plus `closures` loop-closure edges (i, j),
+    0 < j - i <= max_span; pose 0 is fixed."""
+    rng = np.random.default_rng(seed)
+    world = 100.0 * rng.uniform(-1, 1, size=(points_per_scan, 2))
+    ang = rng.uniform(0, 2 * np.pi, size=points_per_scan)
+    nrm = np.stack([np.cos(ang), np.sin(ang)], 1)
+    n_all = num_poses + 1
+    poses = np.stack([np.array([10.0, 10.0, np.pi]) * rng.uniform(-1, 1, size=3) for _ in range(n_all)])
+    scans, normals = [], []
+    for x, y, th in poses:
+        c, s_ = np.cos(th), np.sin(th)
+        R = np.array([[c, -s_], [s_, c]])
+        scans.append((world - np.array([x, y])) @ R)
+        normals.append(nrm @ R)
+    edges = [(i, i + 1) for i in range(num_poses)]
+    for _ in range(closures):
+        i = int(rng.integers(0, max(num_poses - 1, 1)))
+        j = min(num_poses, i + int(rng.integers(2, max_span + 1)))
+        if j > i:
+            edges.append((i, j))
+    sig = np.asarray(noise, dtype=float)
+    poses0 = np.array([se2_compose(sig * rng.uniform(-1, 1, size=3), poses[i]) for i in range(1, n_all)])
+    return ScanAlignProblem(poses, poses0, scans, normals, edges,
+                            name=f"pose graph {num_poses} poses, {len(edges)} edges, {points_per_scan} points/scan")

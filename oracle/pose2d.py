@@ -22,6 +22,7 @@ these problems: chi2 below 1e-12 after the solve
 from __future__ import annotations
 
 import numpy as np
+import scipy.linalg as sla
 
 from nelson_b200.problems import ScanAlignProblem, se2_compose
 
@@ -83,12 +84,11 @@ class Pose2DOracle:
         d = np.diag(Hd) * (1.0 + rel) + abs_
         np.fill_diagonal(Hd, d)
         try:
-            Lc = np.linalg.cholesky(Hd)
+            c = sla.cho_factor(Hd, lower=True, check_finite=False)
         except np.linalg.LinAlgError:
             self.inc[:] = 0.0
             return False
-        y = np.linalg.solve(Lc, -self.b)
-        self.inc = np.linalg.solve(Lc.T, y)
+        self.inc = sla.cho_solve(c, -self.b, check_finite=False)
         return True
 
     def inc_sqnorm(self):

@@ -120,6 +120,47 @@ double trace_diff(const Stats& a, const Stats& b, size_t* n) {
   return worst;
 }
 
+// The 2D scan alignment of nelson/tests/testGaussNewton2DScansAlign.cpp:
+// scans of common world points and normals seen from random SE(2) poses;
+// pose 0 fixed, the others started from a perturbed truth.
+struct Scans {
+  int n = 0, k = 0;
+  std::vector<double> truth;                   // (n + 1) x 3
+  std::vector<std::vector<double>> pts, nrm;   // per scan, k x 2
+};
+
+Scans make_scans(int n, int k, unsigned seed) {
+  std::mt19937 rng(seed);
+  std::uniform_real_distribution<double> u(-1.0, 1.0);
+  Scans sc;
+  sc.n = n;
+  sc.k = k;
+  std::vector<double> wp(2 * k), wn(2 * k);
+  for (int i = 0; i < k; i++) {
+    wp[2 * i] = 100 * u(rng);
+    wp[2 * i + 1] = 100 * u(rng);
+    const double a = 3.14159265358979 * u(rng);
+    wn[2 * i] = std::cos(a);
+    wn[2 * i + 1] = std::sin(a);
+  }
+  for (int p = 0; p <= n; p++) {
+    const double x = 10 * u(rng), y = 10 * u(rng), th = 3.14159265358979 * u(rng);
+    sc.truth.insert(sc.truth.end(), {x, y, th});
+    const double c = std::cos(th), s_ = std::sin(th);
+    std::vector<double> q(2 * k), m(2 * k);
+    for (int i = 0; i < k; i++) {  // R' (X - t), R' n
+      const double dx = wp[2 * i] - x, dy = wp[2 * i + 1] - y;
+      q[2 * i] = c * dx + s_ * dy;
+      q[2 * i + 1] = -s_ * dx + c * dy;
+      m[2 * i] = c * wn[2 * i] + s_ * wn[2 * i + 1];
+      m[2 * i + 1] = -s_ * wn[2 * i] + c * wn[2 * i + 1];
+    }
+    sc.pts.push_back(q);
+    sc.nrm.push_back(m);
+  }
+  return sc;
+}
+
 }  // namespace
 
 int main() {
@@ -196,6 +237,38 @@ int main() {
       (void)rAmd;
       expect(da <= tol, "AMD order per-iteration cost vs user order (rel)", da, tol);
     }
+    // 7. ScanAlignSection (SingleSection with point-to-line edges): LM and GN
+    //    reach the reference test's criterion chi2 < 1e-12, natural and AMD order
+    const Scans sc = make_scans(8, 500, 3);
+    for (int order = 0; order < 2; order++)
+      for (int solver = 0; solver < 2; solver++) {
+        nelson_b200::ScanAlignSection sa(sc.n, 1, NL_PREC_FP64);
+        std::vector<double> start(sc.truth.begin() + 3, sc.truth.end());
+        for (int p = 0; p < sc.n; p++) {
+          start[3 * p] += 0.01 * ((p % 3) - 1);
+          start[3 * p + 1] -= 0.01 * ((p % 2) ? 1 : -1);
+          start[3 * p + 2] += 0.003 * ((p % 5) - 2);
+        }
+        sa.setPoses(start.data(), sc.truth.data());
+        for (int i = 0; i <= sc.n; i++)
+          for (int j = i + 1; j <= sc.n; j++) {
+            const NodeId a = i == 0 ? NodeId::fixed(0) : NodeId(i - 1);
+            sa.addEdge(a, NodeId(j - 1), sc.k, sc.pts[i].data(), sc.nrm[i].data(), sc.pts[j].data());
+          }
+        if (order == 1) sa.permuteAMD();
+        sa.structureReady();
+        const double c0 = sa.update(true);
+        std::vector<nelson_b200::IterationRecord> tr;
+        const auto reason = solver == 0 ? sa.solveLM({}, &tr) : sa.solveGN({}, &tr);
+        const double c1 = sa.update(true);
+        const std::vector<double> p = sa.poses();
+        double err = 0;
+        for (int q = 0; q < 3 * sc.n; q++) err = std::max(err, std::fabs(p[q] - sc.truth[3 + q]));
+        std::printf("scan align %s %s: reason %d, %zu records\n", order ? "amd" : "natural",
+                    solver ? "GN" : "LM", int(reason), tr.size());
+        expect(c1 < 1e-12 && c0 > 1.0, "scan alignment chi2 below 1e-12 after the solve", c0, c1);
+        expect(err < 1e-6, "scan alignment poses equal the truth", err, 1e-6);
+      }
   } catch (const nelson_b200::Error& e) {
     std::printf("FAIL exception: %s\n", e.what());
     return 2;

@@ -2,7 +2,8 @@
 
 CPU: the header and the C++ test programs compile and link against the
 library.  GPU: test_api runs (host-loop LM / GN vs the device loop, fixed
-nodes, cost reduction) and exits 0; test_solver_concept drives the
+nodes, cost reduction, the envelope solver and camera orders, the
+ScanAlignSection single section reaching chi2 < 1e-12) and exits 0; test_solver_concept drives the
 reference-shaped LevenbergMarquardt / GaussNewton loops (the calls of
 nelson/LevenbergMarquardt.hpp:36-146 on the Solver and problem concepts) with
 a host-assembled problem (the reference's 5 x 2D / 3 x 3D fixture, final

@@ -141,7 +141,7 @@ def test_larger_pose_graph_matches_oracle():
         i = int(rng.integers(0, 380))
         edges.append((i, i + int(rng.integers(2, 20))))
     p.edges = edges
-    for order in ("natural", "amd"):
+    for order in ("natural", "amd", "rcm"):
         g = N.Pose2DGPU.from_scan_align(p, order=order)
         g.set_solver_kind(N.SOLVER_ENVELOPE)
         reason, tr, it = g.lm_solve()

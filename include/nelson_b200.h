@@ -37,7 +37,8 @@ typedef enum {
   NL_ERR_NOT_SPD = 5,      /* a damped block or the reduced system not SPD     */
   NL_ERR_NONFINITE = 6,    /* non-finite cost / increment                      */
   NL_ERR_TIMEOUT = 7,      /* a bounded device-side wait gave up               */
-  NL_ERR_NOMEM = 8         /* device allocation failed                         */
+  NL_ERR_NOMEM = 8,        /* device allocation failed                         */
+  NL_ERR_CALLBACK = 9      /* a user callback returned non-zero                */
 } nl_status;
 
 /* ---- precision modes ---------------------------------------------------- */
@@ -435,6 +436,70 @@ nl_status nl_pose2d_lm_solve(nl_pose2d* h, const nl_lm_settings* st, nl_solve_re
                              int trace_cap);
 nl_status nl_pose2d_gn_solve(nl_pose2d* h, const nl_gn_settings* st, nl_solve_report* rep, double* trace,
                              int trace_cap);
+
+/* ---- user-defined edges: a DoubleSection whose edges the caller evaluates -
+ * The reference's DoubleSection with user EdgeBinary / EdgeUnary subclasses
+ * (nelson/DoubleSection.hpp:338-365, nelson/EdgeBinary.h:133-157,
+ * nelson/EdgeUnary.h:84-92, accumulated by BaseSection::updateHessianBlocks,
+ * nelson/BaseSection.cpp:5-86).  The caller owns the parameters and the edge
+ * code on the device; the section owns the Hessian, the Schur solve and the
+ * LM / GN control.  U blocks have bu = 2, 3, 6 or 9 parameters, V blocks 3. */
+typedef struct nl_section nl_section;
+#define NL_EDGE_UV 0 /* binary, U block a and V block b */
+#define NL_EDGE_UU 1 /* binary, U blocks a != b         */
+#define NL_EDGE_U 2  /* unary on U block a              */
+#define NL_EDGE_V 3  /* unary on V block a              */
+/* Callbacks, run on the calling thread after the section's stream has drained.
+ * Device work they start must be on `stream` (a cudaStream_t) or finished when
+ * they return.  Return 0 on success; anything else ends the call with
+ * NL_ERR_CALLBACK.
+ *   evaluate: every edge's whitened residual into r and, if jacobians != 0,
+ *     its Jacobian blocks into J (device arrays, offsets of nl_section_layout:
+ *     edge e's residual at r + r_off[e] (m_e values), its J_a (m_e x dim_a,
+ *     row-major) at J + j_off[e], then J_b (m_e x dim_b) for a binary edge;
+ *     dim is bu for a U block, 3 for a V block).  The cost is sum r'r.
+ *   oplus: apply the increment (device, user order: incU nu x bu, incV nv x 3).
+ *   backup / rollback: keep / restore the parameters (LM only). */
+typedef struct {
+  void* user;
+  int (*evaluate)(void* user, void* stream, int jacobians, double* r, double* J);
+  int (*oplus)(void* user, void* stream, const double* incU, const double* incV);
+  int (*backup)(void* user, void* stream);
+  int (*rollback)(void* user, void* stream);
+} nl_section_callbacks;
+nl_status nl_section_create(int bu, int nu, int nv, int precision, int device, nl_section** out);
+nl_status nl_section_destroy(nl_section* s);
+/* addEdge for n edges: kind NL_EDGE_*, blocks a (and b for binary kinds),
+ * residual dimension m (1..64) */
+nl_status nl_section_add_edges(nl_section* s, int n, const int* kind, const int* a, const int* b, const int* m);
+/* setUser2InternalIndexesU / permuteAMD_SchurU (nelson/DoubleSection.hpp:
+ * 23-63); before nl_section_structure_ready */
+nl_status nl_section_set_user2internal_u(nl_section* s, const int* perm);
+nl_status nl_section_permute_amd_u(nl_section* s);
+/* perm[user U block] = internal position */
+nl_status nl_section_get_user2internal_u(nl_section* s, int* perm);
+nl_status nl_section_structure_ready(nl_section* s);
+/* counts after structure_ready: U / W blocks, residual and Jacobian lengths */
+nl_status nl_section_get_counts(nl_section* s, int* nU, int* nW, long long* r_len, long long* j_len);
+/* per-edge offsets into r and J (ne + 1 entries each) */
+nl_status nl_section_layout(nl_section* s, long long* r_off, long long* j_off);
+/* the U pattern (nU (row, col) pairs, internal order, upper CSC) and the W
+ * pattern (nW (U block, V block) pairs, internal order, CSR) */
+nl_status nl_section_get_patterns(nl_section* s, int* u_rc, int* w_rc);
+nl_status nl_section_set_callbacks(nl_section* s, const nl_section_callbacks* cb);
+nl_status nl_section_set_solver_kind(nl_section* s, int kind);
+/* update(hessian): evaluate and accumulate; chi2 may be null */
+nl_status nl_section_update(nl_section* s, int hessian, double* chi2);
+/* the blocks of the last update with hessian set, in pattern order (U: nU x
+ * bu x bu, V: nv x 3 x 3, W: nW x bu x 3, row-major), bU in internal order;
+ * any pointer may be null */
+nl_status nl_section_get_hessian(nl_section* s, double* U, double* V, double* W, double* bU, double* bV);
+/* computeIncrement(rel, abs) on the current Hessian; increments in user order */
+nl_status nl_section_compute_increment(nl_section* s, double rel, double abs_, double* incU, double* incV, int* ok);
+nl_status nl_section_lm_solve(nl_section* s, const nl_lm_settings* st, nl_solve_report* rep, double* trace,
+                              int trace_cap);
+nl_status nl_section_gn_solve(nl_section* s, const nl_gn_settings* st, nl_solve_report* rep, double* trace,
+                              int trace_cap);
 
 /* Device self-test of the mixed path's tensor-core trailing update: builds a
  * random FP32 matrix of ntiles x 128 rows on `device`, applies the panel-0

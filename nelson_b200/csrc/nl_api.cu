@@ -527,6 +527,7 @@ const char* nl_status_string(int s) {
     case NL_ERR_NONFINITE: return "non-finite value";
     case NL_ERR_TIMEOUT: return "device wait timed out";
     case NL_ERR_NOMEM: return "device allocation failed";
+    case NL_ERR_CALLBACK: return "a user callback failed";
     default: return "unknown status";
   }
 }

@@ -24,7 +24,8 @@
 // rel) + abs, then factor and solve), dense or envelope.  oplus applies the
 // SE(2) exponential on the left: theta += w, t <- R(w) t + V(w) v with
 // V(w) = [[sin w / w, -(1 - cos w) / w], [(1 - cos w) / w, sin w / w]].
-// The LM / GN control runs on the host, one device round trip per step.
+// The LM / GN control runs on the host (host_lm.cuh), one device round trip
+// per step.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -33,6 +34,7 @@
 #include <memory>
 #include <vector>
 
+#include "host_lm.cuh"
 #include "schur_core.cuh"
 
 namespace nl {
@@ -199,15 +201,9 @@ struct nl_pose2d {
 
 namespace {
 
-struct P2Error {
-  nl_status s;
-};
-inline void p2_check(nl_status s) {
-  if (s != NL_OK) throw P2Error{s};
-}
-#define P2_CUDA(x)                                 \
-  do {                                             \
-    if ((x) != cudaSuccess) throw P2Error{NL_ERR_CUDA}; \
+#define P2_CUDA(x)                                       \
+  do {                                                   \
+    if ((x) != cudaSuccess) throw HostError{NL_ERR_CUDA}; \
   } while (0)
 
 // The problem operations the LM / GN loops need (the problem concept of
@@ -267,7 +263,7 @@ struct Pose2DOps {
   }
   double max_abs_hdiag() {
     double* dv = h->scal.as<double>() + 1;
-    p2_check(h->core->enqueue_hdiag(dv));
+    host_check(h->core->enqueue_hdiag(dv));
     P2_CUDA(cudaMemcpyAsync(h->pin + 1, dv, sizeof(double), cudaMemcpyDeviceToHost, h->st));
     P2_CUDA(cudaStreamSynchronize(h->st));
     return h->pin[1];
@@ -279,7 +275,7 @@ struct Pose2DOps {
     P2_CUDA(cudaMemcpyAsync(h->lam.p, h->pin + 2, 2 * sizeof(double), cudaMemcpyHostToDevice, h->st));
     int* status = reinterpret_cast<int*>(h->lam.as<double>() + 2);
     P2_CUDA(cudaMemsetAsync(status, 0, sizeof(int), h->st));
-    p2_check(h->core->enqueue_increment(h->lam.as<double>(), status, nullptr));
+    host_check(h->core->enqueue_increment(h->lam.as<double>(), status, nullptr));
     const int n = 3 * h->nv;
     inc.assign(n, 0.0);
     if (n) P2_CUDA(cudaMemcpyAsync(inc.data(), h->core->incU, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st));
@@ -287,7 +283,7 @@ struct Pose2DOps {
     P2_CUDA(cudaStreamSynchronize(h->st));
     int stt = 0;
     memcpy(&stt, h->pin + 4, sizeof(int));
-    if (stt & ST_SPIN_TIMEOUT) throw P2Error{NL_ERR_TIMEOUT};
+    if (stt & ST_SPIN_TIMEOUT) throw HostError{NL_ERR_TIMEOUT};
     return stt == 0;
   }
   double inc_sqnorm() const {
@@ -316,118 +312,6 @@ struct Pose2DOps {
     P2_CUDA(cudaMemcpyAsync(h->pose.p, h->pose_bck.p, h->pose.bytes, cudaMemcpyDeviceToDevice, h->st));
   }
 };
-
-void trace_rec(double* trace, int cap, int* n, double it, double sub, double chi2, double mu, double rh, double inc,
-               double ok, double acc) {
-  if (trace && *n < cap) {
-    double* t = trace + (size_t)(*n) * 8;
-    t[0] = it;
-    t[1] = sub;
-    t[2] = chi2;
-    t[3] = mu;
-    t[4] = rh;
-    t[5] = inc;
-    t[6] = ok;
-    t[7] = acc;
-  }
-  (*n)++;
-}
-
-// LevenbergMarquardt::solve (nelson/LevenbergMarquardt.hpp:36-146)
-int lm_loop(Pose2DOps& P, const nl_lm_settings& s, double* trace, int cap, int* ntr, int* iters, int* subs) {
-  int n = 0, iter = -1, nsub = 0;
-  auto finish = [&](int reason) {
-    if (ntr) *ntr = std::min(n, cap);
-    *iters = iter;
-    *subs = nsub;
-    return reason;
-  };
-  P.update(true);
-  trace_rec(trace, cap, &n, iter, 0, P.chi2(), 0, 0, 0, 1, 1);
-  if (P.max_abs_b() <= s.epsBVector) return finish(NL_SUCCESS_AT_START);
-  P.backup();
-  double oldChi2 = P.chi2();
-  double mu = s.tau * P.max_abs_hdiag();
-  double curV = s.initV;
-  iter = 0;
-  while (iter < s.maxNumIt) {
-    int subiter = 0;
-    bool toRepeat = false;
-    do {
-      const double mu_used = mu;
-      const bool ok = P.compute_increment(0.0, mu);
-      nsub++;
-      const double inc = P.inc_sqnorm();
-      if (ok && iter >= s.minNumIt && inc <= s.epsIncSquare) {
-        trace_rec(trace, cap, &n, iter, subiter, P.chi2(), mu_used, 0, inc, 1, 0);
-        return finish(NL_SUCCESS_SMALL_INCREMENT);
-      }
-      double rh = -1.0, chi2_rec = -1.0;
-      if (ok) {
-        P.oplus();
-        P.update(false);
-        chi2_rec = P.chi2();
-        rh = P.rho(mu, oldChi2);
-      }
-      const bool acc = ok && rh > 0;
-      trace_rec(trace, cap, &n, iter, subiter, chi2_rec, mu_used, rh, inc, ok ? 1 : 0, acc ? 1 : 0);
-      if (acc) {
-        if (iter > s.minNumIt && P.max_abs_b() <= s.epsBVector) return finish(NL_SUCCESS_EPS_B);
-        if (iter > s.minNumIt && P.chi2() < s.epsChi2) return finish(NL_SUCCESS_SMALL_RESIDUALS);
-        const double fc = 2 * rh - 1;
-        double alpha = std::min(s.maxScaleFactor, 1 - fc * fc * fc);
-        alpha = std::max(s.minScaleFactor, alpha);
-        mu = mu * alpha;
-        curV = s.initV;
-      } else {
-        P.rollback();
-        mu = mu * curV;
-        curV = curV * s.penaltyV;
-      }
-      subiter++;
-      if (subiter >= s.maxNumSubIt) return finish(NL_MAX_SUBITERATION_REACHED);
-      toRepeat = (rh <= 0 || !ok);
-    } while (toRepeat);
-    P.update(true);
-    P.backup();
-    oldChi2 = P.chi2();
-    iter++;
-  }
-  return finish(NL_MAX_ITERATION_REACHED);
-}
-
-// GaussNewton::solve (nelson/GaussNewton.hpp:32-127)
-int gn_loop(Pose2DOps& P, const nl_gn_settings& s, double* trace, int cap, int* ntr, int* iters) {
-  int n = 0, iter = -1;
-  auto finish = [&](int reason) {
-    if (ntr) *ntr = std::min(n, cap);
-    *iters = iter;
-    return reason;
-  };
-  P.update(true);
-  trace_rec(trace, cap, &n, iter, 0, P.chi2(), 0, 0, 0, 1, 1);
-  if (P.max_abs_b() <= s.epsBVector) return finish(NL_SUCCESS_AT_START);
-  iter = 0;
-  while (iter < s.maxNumIt) {
-    const bool ok = P.compute_increment(s.relLambda, s.absLambda);
-    const double inc = P.inc_sqnorm();
-    if (!ok) {
-      trace_rec(trace, cap, &n, iter, 0, -1, 0, 0, inc, 0, 0);
-      return finish(NL_SOLVER_FAILURE);
-    }
-    if (iter >= s.minNumIt && inc <= s.epsIncSquare) {
-      trace_rec(trace, cap, &n, iter, 0, P.chi2(), 0, 0, inc, 1, 0);
-      return finish(NL_SUCCESS_SMALL_INCREMENT);
-    }
-    P.oplus();
-    P.update(true);
-    trace_rec(trace, cap, &n, iter, 0, P.chi2(), 0, 0, inc, 1, 1);
-    if (iter > s.minNumIt && P.max_abs_b() <= s.epsBVector) return finish(NL_SUCCESS_EPS_B);
-    if (iter > s.minNumIt && P.chi2() < s.epsChi2) return finish(NL_SUCCESS_SMALL_RESIDUALS);
-    iter++;
-  }
-  return finish(NL_MAX_ITERATION_REACHED);
-}
 
 }  // namespace
 
@@ -698,7 +582,7 @@ nl_status nl_pose2d_update(nl_pose2d* h, int hessian, double* chi2) {
     Pose2DOps P{h};
     P.update(hessian != 0);
     if (chi2) *chi2 = h->chi2;
-  } catch (const P2Error& e) {
+  } catch (const HostError& e) {
     return e.s;
   }
   return NL_OK;
@@ -716,7 +600,7 @@ nl_status nl_pose2d_lm_solve(nl_pose2d* h, const nl_lm_settings* st, nl_solve_re
     NL_CUDA(cudaEventCreate(&e0));
     NL_CUDA(cudaEventCreate(&e1));
     NL_CUDA(cudaEventRecord(e0, h->st));
-    const int reason = lm_loop(P, *st, trace, std::max(0, trace_cap), &ntr, &its, &subs);
+    const int reason = host_lm_loop(P, *st, trace, std::max(0, trace_cap), &ntr, &its, &subs, nullptr);
     NL_CUDA(cudaEventRecord(e1, h->st));
     NL_CUDA(cudaEventSynchronize(e1));
     float ms = 0;
@@ -732,7 +616,7 @@ nl_status nl_pose2d_lm_solve(nl_pose2d* h, const nl_lm_settings* st, nl_solve_re
       rep->mu = 0.0;
       rep->device_ms = ms;
     }
-  } catch (const P2Error& e) {
+  } catch (const HostError& e) {
     return e.s;
   }
   return NL_OK;
@@ -750,7 +634,7 @@ nl_status nl_pose2d_gn_solve(nl_pose2d* h, const nl_gn_settings* st, nl_solve_re
     NL_CUDA(cudaEventCreate(&e0));
     NL_CUDA(cudaEventCreate(&e1));
     NL_CUDA(cudaEventRecord(e0, h->st));
-    const int reason = gn_loop(P, *st, trace, std::max(0, trace_cap), &ntr, &its);
+    const int reason = host_gn_loop(P, *st, trace, std::max(0, trace_cap), &ntr, &its);
     NL_CUDA(cudaEventRecord(e1, h->st));
     NL_CUDA(cudaEventSynchronize(e1));
     float ms = 0;
@@ -766,7 +650,7 @@ nl_status nl_pose2d_gn_solve(nl_pose2d* h, const nl_gn_settings* st, nl_solve_re
       rep->mu = 0.0;
       rep->device_ms = ms;
     }
-  } catch (const P2Error& e) {
+  } catch (const HostError& e) {
     return e.s;
   }
   return NL_OK;

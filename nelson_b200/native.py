@@ -100,6 +100,11 @@ EXPORTS = [
     "nl_pose2d_set_user2internal", "nl_pose2d_permute_amd", "nl_pose2d_permute_rcm", "nl_pose2d_structure_ready",
     "nl_pose2d_set_solver_kind", "nl_pose2d_update", "nl_pose2d_get_hessian", "nl_pose2d_lm_solve",
     "nl_pose2d_gn_solve",
+    "nl_section_create", "nl_section_destroy", "nl_section_add_edges", "nl_section_set_user2internal_u",
+    "nl_section_permute_amd_u", "nl_section_get_user2internal_u", "nl_section_structure_ready",
+    "nl_section_get_counts", "nl_section_layout",
+    "nl_section_get_patterns", "nl_section_set_callbacks", "nl_section_set_solver_kind", "nl_section_update",
+    "nl_section_get_hessian", "nl_section_compute_increment", "nl_section_lm_solve", "nl_section_gn_solve",
     "nl_status_string",
     "nl_version",
 ]
@@ -155,6 +160,23 @@ def load(build_if_missing: bool = True):
     L.nl_pose2d_structure_ready.argtypes = [vp]
     L.nl_pose2d_set_solver_kind.argtypes = [vp, i]
     L.nl_pose2d_get_hessian.argtypes = [vp, vp, vp]
+    L.nl_section_create.argtypes = [i, i, i, i, i, C.POINTER(vp)]
+    L.nl_section_destroy.argtypes = [vp]
+    L.nl_section_add_edges.argtypes = [vp, i, vp, vp, vp, vp]
+    L.nl_section_set_user2internal_u.argtypes = [vp, vp]
+    L.nl_section_permute_amd_u.argtypes = [vp]
+    L.nl_section_get_user2internal_u.argtypes = [vp, vp]
+    L.nl_section_structure_ready.argtypes = [vp]
+    L.nl_section_get_counts.argtypes = [vp, vp, vp, vp, vp]
+    L.nl_section_layout.argtypes = [vp, vp, vp]
+    L.nl_section_get_patterns.argtypes = [vp, vp, vp]
+    L.nl_section_set_callbacks.argtypes = [vp, C.POINTER(SectionCallbacks)]
+    L.nl_section_set_solver_kind.argtypes = [vp, i]
+    L.nl_section_update.argtypes = [vp, i, C.POINTER(d)]
+    L.nl_section_get_hessian.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.nl_section_compute_increment.argtypes = [vp, d, d, vp, vp, C.POINTER(i)]
+    L.nl_section_lm_solve.argtypes = [vp, C.POINTER(LMSettings), C.POINTER(SolveReport), vp, i]
+    L.nl_section_gn_solve.argtypes = [vp, C.POINTER(GNSettings), C.POINTER(SolveReport), vp, i]
     L.nl_pose2d_update.argtypes = [vp, i, C.POINTER(d)]
     L.nl_pose2d_lm_solve.argtypes = [vp, C.POINTER(LMSettings), C.POINTER(SolveReport), vp, i]
     L.nl_pose2d_gn_solve.argtypes = [vp, C.POINTER(GNSettings), C.POINTER(SolveReport), vp, i]
@@ -703,5 +725,170 @@ class Pose2DGPU:
         rep = SolveReport()
         tr = np.zeros((max(trace_cap, 1), TRACE_STRIDE))
         self._c(self.L.nl_pose2d_gn_solve(self.h, C.byref(s), C.byref(rep), _p(tr), trace_cap), "nl_pose2d_gn_solve")
+        self.last_report = {n: getattr(rep, n) for n, _ in SolveReport._fields_}
+        return REASONS[rep.reason], tr[:rep.n_trace].copy(), rep.iterations
+
+
+EDGE_UV, EDGE_UU, EDGE_U, EDGE_V = 0, 1, 2, 3
+_EVAL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p)
+_OPLUS_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
+_STATE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p)
+
+
+class SectionCallbacks(C.Structure):
+    _fields_ = [("user", C.c_void_p), ("evaluate", _EVAL_FN), ("oplus", _OPLUS_FN), ("backup", _STATE_FN),
+                ("rollback", _STATE_FN)]
+
+
+class SectionGPU:
+    """A DoubleSection with user-defined edges (nl_section_*): the caller's
+    code evaluates every edge's whitened residual and Jacobian blocks into the
+    section's device arrays; the section assembles U / V / W / b on the device,
+    solves with the Schur complement and runs LevenbergMarquardt / GaussNewton
+    (nelson/DoubleSection.hpp:338-365 with user EdgeBinary / EdgeUnary edges,
+    nelson/BaseSection.cpp:5-86).
+
+    Callbacks are Python callables; device arrays are passed as integer
+    addresses:
+      evaluate(jacobians: bool, r_ptr, J_ptr, stream_ptr)
+      oplus(incU_ptr, incV_ptr, stream_ptr)   (increments in user order)
+      backup(stream_ptr), rollback(stream_ptr)
+    An exception raised in a callback ends the library call, which then
+    raises it."""
+
+    def __init__(self, bu, nu, nv, precision=PREC_FP64, device=0):
+        self.L = load()
+        self.bu, self.nu, self.nv = bu, nu, nv
+        h = C.c_void_p()
+        _chk(self.L, self.L.nl_section_create(C.c_int(bu), C.c_int(nu), C.c_int(nv), C.c_int(precision),
+                                              C.c_int(device), C.byref(h)), "nl_section_create")
+        self.h = h
+        self.ne = 0
+        self._exc = None
+        self._cb = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.nl_section_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, rc, what):
+        if self._exc is not None:
+            e, self._exc = self._exc, None
+            raise e
+        _chk(self.L, rc, what)
+
+    def add_edges(self, kind, a, b, m):
+        k = np.ascontiguousarray(kind, np.int32)
+        aa = np.ascontiguousarray(a, np.int32)
+        bb = np.ascontiguousarray(b, np.int32)
+        mm = np.ascontiguousarray(m, np.int32)
+        if not (k.size == aa.size == bb.size == mm.size):
+            raise NelsonError("add_edges: kind, a, b and m differ in length")
+        self._c(self.L.nl_section_add_edges(self.h, C.c_int(k.size), _p(k), _p(aa), _p(bb), _p(mm)),
+                "nl_section_add_edges")
+        self.ne += k.size
+
+    def set_user2internal(self, perm):
+        p = np.ascontiguousarray(perm, np.int32)
+        self._c(self.L.nl_section_set_user2internal_u(self.h, _p(p)), "nl_section_set_user2internal_u")
+
+    def permute_amd(self):
+        self._c(self.L.nl_section_permute_amd_u(self.h), "nl_section_permute_amd_u")
+
+    def user2internal(self):
+        p = np.zeros(self.nu, np.int32)
+        self._c(self.L.nl_section_get_user2internal_u(self.h, _p(p)), "nl_section_get_user2internal_u")
+        return p
+
+    def structure_ready(self):
+        self._c(self.L.nl_section_structure_ready(self.h), "nl_section_structure_ready")
+
+    def counts(self):
+        nU, nW, rl, jl = C.c_int(), C.c_int(), C.c_longlong(), C.c_longlong()
+        self._c(self.L.nl_section_get_counts(self.h, C.byref(nU), C.byref(nW), C.byref(rl), C.byref(jl)),
+                "nl_section_get_counts")
+        return nU.value, nW.value, rl.value, jl.value
+
+    def layout(self):
+        r = np.zeros(self.ne + 1, np.int64)
+        j = np.zeros(self.ne + 1, np.int64)
+        self._c(self.L.nl_section_layout(self.h, _p(r), _p(j)), "nl_section_layout")
+        return r, j
+
+    def patterns(self):
+        nU, nW, _, _ = self.counts()
+        u = np.zeros((max(nU, 1), 2), np.int32)
+        w = np.zeros((max(nW, 1), 2), np.int32)
+        self._c(self.L.nl_section_get_patterns(self.h, _p(u), _p(w)), "nl_section_get_patterns")
+        return u[:nU], w[:nW]
+
+    def set_callbacks(self, evaluate, oplus, backup=None, rollback=None):
+        def guard(fn):
+            def run(*args):
+                try:
+                    fn(*args)
+                    return 0
+                except BaseException as e:   # reported by the library call that ran it
+                    self._exc = e
+                    return 1
+            return run
+
+        ev = _EVAL_FN(guard(lambda u, st, jac, r, J: evaluate(bool(jac), r, J, st)))
+        op = _OPLUS_FN(guard(lambda u, st, du, dv: oplus(du, dv, st)))
+        bk = _STATE_FN(guard(lambda u, st: backup(st))) if backup else _STATE_FN()
+        rb = _STATE_FN(guard(lambda u, st: rollback(st))) if rollback else _STATE_FN()
+        cb = SectionCallbacks(None, ev, op, bk, rb)
+        self._cb = (cb, ev, op, bk, rb)   # keep the trampolines alive
+        self._c(self.L.nl_section_set_callbacks(self.h, C.byref(cb)), "nl_section_set_callbacks")
+
+    def set_solver_kind(self, kind: int):
+        self._c(self.L.nl_section_set_solver_kind(self.h, C.c_int(kind)), "nl_section_set_solver_kind")
+
+    def update(self, hessian=True):
+        v = C.c_double()
+        self._c(self.L.nl_section_update(self.h, C.c_int(int(hessian)), C.byref(v)), "nl_section_update")
+        return v.value
+
+    def hessian(self):
+        """(U, V, W, bU, bV) of the last update(True): blocks in pattern order,
+        bU in internal order."""
+        nU, nW, _, _ = self.counts()
+        bu = self.bu
+        U = np.zeros((nU, bu, bu))
+        V = np.zeros((self.nv, 3, 3))
+        W = np.zeros((nW, bu, 3))
+        bU = np.zeros(self.nu * bu)
+        bV = np.zeros(self.nv * 3)
+        self._c(self.L.nl_section_get_hessian(self.h, _p(U), _p(V), _p(W), _p(bU), _p(bV)), "nl_section_get_hessian")
+        return U, V, W, bU, bV
+
+    def compute_increment(self, rel, abs_):
+        du = np.zeros(self.nu * self.bu)
+        dv = np.zeros(self.nv * 3)
+        ok = C.c_int()
+        self._c(self.L.nl_section_compute_increment(self.h, rel, abs_, _p(du), _p(dv), C.byref(ok)),
+                "nl_section_compute_increment")
+        return bool(ok.value), du, dv
+
+    def lm_solve(self, settings=None, trace_cap=4096):
+        s = settings or LMSettings()
+        rep = SolveReport()
+        tr = np.zeros((max(trace_cap, 1), TRACE_STRIDE))
+        self._c(self.L.nl_section_lm_solve(self.h, C.byref(s), C.byref(rep), _p(tr), trace_cap), "nl_section_lm_solve")
+        self.last_report = {n: getattr(rep, n) for n, _ in SolveReport._fields_}
+        return REASONS[rep.reason], tr[:rep.n_trace].copy(), rep.iterations
+
+    def gn_solve(self, settings=None, trace_cap=4096):
+        s = settings or GNSettings()
+        rep = SolveReport()
+        tr = np.zeros((max(trace_cap, 1), TRACE_STRIDE))
+        self._c(self.L.nl_section_gn_solve(self.h, C.byref(s), C.byref(rep), _p(tr), trace_cap), "nl_section_gn_solve")
         self.last_report = {n: getattr(rep, n) for n, _ in SolveReport._fields_}
         return REASONS[rep.reason], tr[:rep.n_trace].copy(), rep.iterations

@@ -524,3 +524,85 @@ def pose_graph_scene(num_poses: int = 2000, points_per_scan: int = 500, closures
     poses0 = np.array([se2_compose(sig * rng.uniform(-1, 1, size=3), poses[i]) for i in range(1, n_all)])
     return ScanAlignProblem(poses, poses0, scans, normals, edges,
                             name=f"pose graph {num_poses} poses, {len(edges)} edges, {points_per_scan} points/scan")
+
+
+@dataclass
+class RangeScene:
+    """A DoubleSection with all four user edge kinds, for the user-edge
+    section: U blocks x_u (bu = 3, 6 or 9: a 3D position, then bu - 3 extra
+    parameters), V blocks p_v (3D points).
+      U-V edge (m = 2): r = (|pos_u - p_v| - d,  a . (pos_u - p_v) + c . extra_u - e)
+      U-U edge (m = bu): r = x_a - x_b - delta_ab
+      U unary (m = bu):  r = w (x_u - prior_u)
+      V unary (m = 3):   r = w (p_v - prior_v)
+    Measurements are those of the true parameters plus noise; x0 / p0 start
+    from the truth plus a perturbation."""
+    bu: int
+    x_true: np.ndarray
+    p_true: np.ndarray
+    x0: np.ndarray
+    p0: np.ndarray
+    kind: np.ndarray          # per edge
+    a: np.ndarray
+    b: np.ndarray
+    m: np.ndarray
+    d: np.ndarray             # U-V: range, linear measurement e, unit a (3), c (bu - 3)
+    e: np.ndarray
+    avec: np.ndarray
+    cvec: np.ndarray
+    delta: np.ndarray         # U-U: (n, bu)
+    prior: np.ndarray         # U / V unary: (n, bu) (V priors use the first 3 entries)
+    w: np.ndarray
+
+
+def range_scene(bu: int = 3, nu: int = 40, nv: int = 400, obs_per_point: int = 4, uu_edges: int = 60,
+                noise: float = 0.01, start: float = 0.05, seed: int = 3) -> RangeScene:
+    rng = np.random.default_rng(seed)
+    x_true = np.concatenate([rng.uniform(-10, 10, size=(nu, 3)), rng.normal(size=(nu, bu - 3))], 1)
+    p_true = rng.uniform(-10, 10, size=(nv, 3)) + np.array([0.0, 0.0, 25.0])
+    kind, a, b = [], [], []
+    for v in range(nv):
+        for u in rng.choice(nu, size=obs_per_point, replace=False):
+            kind.append(0)
+            a.append(int(u))
+            b.append(v)
+    for _ in range(uu_edges):
+        i, j = rng.choice(nu, size=2, replace=False)
+        kind.append(1)
+        a.append(int(i))
+        b.append(int(j))
+    for u in range(nu):   # priors on every U block hold the gauge and the extra parameters
+        kind.append(2)
+        a.append(u)
+        b.append(-1)
+    for v in range(0, nv, 7):
+        kind.append(3)
+        a.append(v)
+        b.append(-1)
+    kind, a, b = np.array(kind, np.int32), np.array(a, np.int32), np.array(b, np.int32)
+    ne = kind.size
+    m = np.where(kind == 0, 2, np.where(kind == 3, 3, bu)).astype(np.int32)
+    avec = rng.normal(size=(ne, 3))
+    avec /= np.linalg.norm(avec, axis=1, keepdims=True)
+    cvec = rng.normal(size=(ne, bu - 3))
+    d = np.zeros(ne)
+    e = np.zeros(ne)
+    delta = np.zeros((ne, bu))
+    prior = np.zeros((ne, bu))
+    w = np.ones(ne)
+    for k in range(ne):
+        if kind[k] == 0:
+            diff = x_true[a[k], :3] - p_true[b[k]]
+            d[k] = np.linalg.norm(diff) + noise * rng.normal()
+            e[k] = avec[k] @ diff + cvec[k] @ x_true[a[k], 3:] + noise * rng.normal()
+        elif kind[k] == 1:
+            delta[k] = x_true[a[k]] - x_true[b[k]] + noise * rng.normal(size=bu)
+        elif kind[k] == 2:
+            prior[k] = x_true[a[k]] + rng.normal(size=bu)
+            w[k] = 0.1
+        else:
+            prior[k, :3] = p_true[a[k]] + noise * rng.normal(size=3)
+            w[k] = 0.5
+    x0 = x_true + start * rng.normal(size=x_true.shape)
+    p0 = p_true + start * rng.normal(size=p_true.shape)
+    return RangeScene(bu, x_true, p_true, x0, p0, kind, a, b, m, d, e, avec, cvec, delta, prior, w)

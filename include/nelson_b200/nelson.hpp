@@ -792,6 +792,125 @@ class ScanAlignSection {
 
 
 // ---------------------------------------------------------------------------
+// DeviceEdgeSection: a DoubleSection with user-defined edges (the reference's
+// DoubleSection subclass with EdgeBinary / EdgeUnary edges, nelson/
+// DoubleSection.hpp:338-365), resident on one GPU.  Derive from it, keep the
+// parameters on the device and implement:
+//   evaluate(stream, jacobians, r, J): every edge's whitened residual into r
+//     and, with jacobians, its Jacobian blocks into J (device arrays; edge e
+//     at rOffsets()[e] / jOffsets()[e]: J_a (m x dim_a, row-major) then J_b);
+//   oplus(stream, incU, incV): apply the increment (device, user order);
+//   backupSolution / rollbackSolution(stream): keep / restore the parameters.
+// Device work goes on `stream` (a cudaStream_t) or is finished on return; a
+// non-zero return ends the solve with NL_ERR_CALLBACK.  Call order: addEdge
+// ..., optionally permuteAMD_SchurU, structureReady, then solveLM / solveGN.
+class DeviceEdgeSection {
+ public:
+  DeviceEdgeSection(int bu, int numU, int numV, int precision = NL_PREC_FP64, int device = 0)
+      : bu_(bu), nu_(numU), nv_(numV) {
+    check(nl_section_create(bu, numU, numV, precision, device, &h_), "nl_section_create");
+  }
+  virtual ~DeviceEdgeSection() {
+    if (h_) nl_section_destroy(h_);
+  }
+  DeviceEdgeSection(const DeviceEdgeSection&) = delete;
+  DeviceEdgeSection& operator=(const DeviceEdgeSection&) = delete;
+
+  // kind NL_EDGE_UV (a: U block, b: V block), NL_EDGE_UU (two U blocks),
+  // NL_EDGE_U / NL_EDGE_V (unary on block a); m residuals
+  void addEdge(int kind, int a, int b, int m) {
+    check(nl_section_add_edges(h_, 1, &kind, &a, &b, &m), "nl_section_add_edges");
+    ++ne_;
+  }
+  void permuteAMD_SchurU() { check(nl_section_permute_amd_u(h_), "nl_section_permute_amd_u"); }
+  void structureReady() {
+    check(nl_section_structure_ready(h_), "nl_section_structure_ready");
+    rOff_.resize(ne_ + 1);
+    jOff_.resize(ne_ + 1);
+    check(nl_section_layout(h_, rOff_.data(), jOff_.data()), "nl_section_layout");
+    nl_section_callbacks cb{this, &DeviceEdgeSection::evalT, &DeviceEdgeSection::oplusT,
+                            &DeviceEdgeSection::backupT, &DeviceEdgeSection::rollbackT};
+    check(nl_section_set_callbacks(h_, &cb), "nl_section_set_callbacks");
+  }
+  const std::vector<long long>& rOffsets() const { return rOff_; }
+  const std::vector<long long>& jOffsets() const { return jOff_; }
+  int numEdges() const { return ne_; }
+  void setSolverKind(int kind) { check(nl_section_set_solver_kind(h_, kind), "nl_section_set_solver_kind"); }
+  double update(bool hessian) {
+    double c = 0.0;
+    check(nl_section_update(h_, hessian ? 1 : 0, &c), "nl_section_update");
+    return c;
+  }
+  TerminationReason solveLM(const LevenbergMarquardtSettings& st = {}, std::vector<IterationRecord>* trace = nullptr) {
+    const nl_lm_settings c = st.c();
+    return run([&](nl_solve_report* r, double* t, int cap) { return nl_section_lm_solve(h_, &c, r, t, cap); }, trace,
+               "nl_section_lm_solve");
+  }
+  TerminationReason solveGN(const GaussNewtonSettings& st = {}, std::vector<IterationRecord>* trace = nullptr) {
+    const nl_gn_settings c = st.c();
+    return run([&](nl_solve_report* r, double* t, int cap) { return nl_section_gn_solve(h_, &c, r, t, cap); }, trace,
+               "nl_section_gn_solve");
+  }
+  const nl_solve_report& lastReport() const { return rep_; }
+
+ protected:
+  virtual int evaluate(void* stream, bool jacobians, double* r, double* J) = 0;
+  virtual int oplus(void* stream, const double* incU, const double* incV) = 0;
+  virtual int backupSolution(void*) { return 1; }
+  virtual int rollbackSolution(void*) { return 1; }
+  int bu_, nu_, nv_;
+
+ private:
+  static int evalT(void* u, void* st, int jac, double* r, double* J) {
+    try {
+      return static_cast<DeviceEdgeSection*>(u)->evaluate(st, jac != 0, r, J);
+    } catch (...) {
+      return 1;
+    }
+  }
+  static int oplusT(void* u, void* st, const double* du, const double* dv) {
+    try {
+      return static_cast<DeviceEdgeSection*>(u)->oplus(st, du, dv);
+    } catch (...) {
+      return 1;
+    }
+  }
+  static int backupT(void* u, void* st) {
+    try {
+      return static_cast<DeviceEdgeSection*>(u)->backupSolution(st);
+    } catch (...) {
+      return 1;
+    }
+  }
+  static int rollbackT(void* u, void* st) {
+    try {
+      return static_cast<DeviceEdgeSection*>(u)->rollbackSolution(st);
+    } catch (...) {
+      return 1;
+    }
+  }
+  template <class F>
+  TerminationReason run(F f, std::vector<IterationRecord>* trace, const char* what) {
+    const int cap = trace ? 4096 : 0;
+    std::vector<double> t(size_t(cap > 0 ? cap : 1) * 8);
+    check(f(&rep_, cap ? t.data() : nullptr, cap), what);
+    if (trace) {
+      trace->clear();
+      for (int i = 0; i < rep_.n_trace; i++) {
+        const double* r = t.data() + size_t(i) * 8;
+        trace->push_back(IterationRecord{int(r[0]), int(r[1]), r[2], r[3], r[4], r[5], r[6] != 0.0, r[7] != 0.0});
+      }
+    }
+    return TerminationReason(rep_.reason);
+  }
+  nl_section* h_ = nullptr;
+  int ne_ = 0;
+  std::vector<long long> rOff_, jOff_;
+  nl_solve_report rep_{};
+};
+
+
+// ---------------------------------------------------------------------------
 // Problem files.
 // Problem / load: the visibility-list format of the reference's samples
 // (nelson/samples/Problems.h:4-12, Problems.cpp:8-30): "nCameras nPoints

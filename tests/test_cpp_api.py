@@ -3,7 +3,9 @@
 CPU: the header and the C++ test programs compile and link against the
 library.  GPU: test_api runs (host-loop LM / GN vs the device loop, fixed
 nodes, cost reduction, the envelope solver and camera orders, the
-ScanAlignSection single section reaching chi2 < 1e-12) and exits 0; test_solver_concept drives the
+ScanAlignSection single section reaching chi2 < 1e-12) and exits 0;
+test_section_edges (nvcc) subclasses DeviceEdgeSection with CUDA edge
+kernels and reaches chi2 < 1e-12 and the true parameters; test_solver_concept drives the
 reference-shaped LevenbergMarquardt / GaussNewton loops (the calls of
 nelson/LevenbergMarquardt.hpp:36-146 on the Solver and problem concepts) with
 a host-assembled problem (the reference's 5 x 2D / 3 x 3D fixture, final
@@ -37,6 +39,39 @@ def _compile(out_dir, name="test_api"):
     assert r.returncode == 0, r.stderr
     assert "warning" not in r.stderr, r.stderr
     return exe
+
+
+def _compile_cu(out_dir, name):
+    """An nvcc-compiled C++ test (user edges as CUDA kernels), sm_100a."""
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("no nvcc")
+    if not os.path.exists(nb_build.LIB):
+        nb_build.build()
+    exe = os.path.join(out_dir, name)
+    lib_dir = os.path.dirname(nb_build.LIB)
+    src = os.path.join(ROOT, "tests", "cpp", name + ".cu")
+    cmd = [nvcc, "-O2", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-I" + os.path.join(ROOT, "include"),
+           src, "-o", exe, "-L" + lib_dir, "-lnelson_b200", "-Xlinker", "-rpath," + lib_dir,
+           "-Xlinker", "--allow-shlib-undefined"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def test_section_edges_compiles(tmp_path):
+    assert os.path.exists(_compile_cu(str(tmp_path), "test_section_edges"))
+
+
+@pytest.mark.gpu
+def test_section_edges_runs(tmp_path):
+    """DeviceEdgeSection subclassed with CUDA edge kernels: LM and GN, natural
+    and AMD order, reach chi2 < 1e-12 and the true parameters."""
+    exe = _compile_cu(str(tmp_path), "test_section_edges")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "ALL OK" in r.stdout
 
 
 def test_cpp_api_compiles(tmp_path):

@@ -98,9 +98,12 @@ class Oracle:
         self.L = lib()
         self.kind, self.bu, self.bv = kind, bu, bv
         self.nu_var, self.nu_fix, self.nv_var, self.nv_fix = nu_var, nu_fix, nv_var, nv_fix
-        self.h = self.L.orc_create(kind, bu, bv, nu_var, nu_fix, nv_var, nv_fix, threads)
-        if not self.h:
+        h = self.L.orc_create(kind, bu, bv, nu_var, nu_fix, nv_var, nv_fix, threads)
+        if not h:
             raise ValueError("orc_create rejected the problem description")
+        # kept as a pointer object: the entry points declared without argtypes
+        # would pass a plain Python int as a 32-bit C int and cut the address
+        self.h = C.c_void_p(h)
         self.ne = 0
 
     def __del__(self):

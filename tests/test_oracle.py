@@ -276,3 +276,14 @@ def test_oracle_adjoint_matches_finite_differences():
     assert big.sum() >= 10
     assert (np.abs(adjs[big] - fds[big]) <= 1e-4 * np.abs(fds[big])).all(), (adjs, fds)
     assert np.abs(adjs - fds).max() <= 1e-4 * np.abs(fds).max()
+
+
+def test_handle_passes_as_a_full_pointer(oracle_lib):
+    """The oracle handle stays a pointer object: its entry points without
+    declared argument types would otherwise receive a 32-bit C int and lose
+    the upper half of a heap address above 4 GB."""
+    import ctypes
+    o = oracle_lib.Oracle.from_ba(make_config(0))
+    assert isinstance(o.h, ctypes.c_void_p) and o.h.value
+    o.update(True)
+    assert o.chi2() > 0

@@ -662,8 +662,15 @@ class SchurCoreT final : public SchurCore {
     if (tm) NL_CUDA(cudaEventRecord(ev_[2], st_));
     nvtxRangePop();
     nvtxRangePushA("nl:schur");
-    if (!s_cleared_) {
-      // the first time the whole of S (and S0); afterwards only the envelope
+    // The first time the whole of S (and S0); afterwards only the envelope,
+    // whose outside stays exactly zero -- but only where every kernel that
+    // writes S honours `active`.  The FP64 path's cuBLAS trailing updates
+    // cannot: the sub-iterations that a device-side LM loop leaves in flight
+    // after it has finished still subtract L L' from the stale factor, and the
+    // overflow that builds up there reaches tiles outside the envelope
+    // (0 * inf).  That path clears all of S every time.
+    const bool unpredicated_writes = sizeof(T) == 8 && cublas_ != nullptr;
+    if (!s_cleared_ || unpredicated_writes) {
       NL_CUDA(cudaMemsetAsync(S_.p, 0, S_.bytes, st_));
       if (need_s0_) NL_CUDA(cudaMemsetAsync(S0_.p, 0, S0_.bytes, st_));
       s_cleared_ = true;

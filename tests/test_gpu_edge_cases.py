@@ -148,3 +148,23 @@ def test_solver_only_ba_hessian(oracle_lib, prec):
     du_o, dv_o = o.increment()
     assert rel(du, du_o) < INC_TOL[prec] and rel(dv, dv_o) < INC_TOL[prec]
     s.close()
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("kind", [N.SOLVER_DENSE, N.SOLVER_ENVELOPE])
+def test_second_solve_on_a_reused_handle(prec, kind):
+    """A handle solved once, reset with set_params and solved again gives the
+    trace of a fresh handle.  The first solve's device loop leaves
+    sub-iterations in flight after it finishes; whatever they leave in S must
+    not reach the next solve (the FP64 path's library trailing updates run in
+    them, unpredicated)."""
+    p = make_config(2, 0.3)
+    g = N.BAProblemGPU.from_ba(p, precision=prec)
+    g.set_solver_kind(kind)
+    _, tr1, it1, _ = g.lm_solve(N.LMSettings(maxNumIt=3), trace_cap=64)
+    g.set_params(p.cams, p.pts)
+    _, tr2, it2, _ = g.lm_solve(N.LMSettings(maxNumIt=3), trace_cap=64)
+    assert it1 == it2 == 3
+    assert np.array_equal(tr1[:, [0, 1, 6, 7]], tr2[:, [0, 1, 6, 7]])
+    assert np.array_equal(tr1[:, 2], tr2[:, 2])     # the same kernels on the same inputs: bit-identical
+    g.close()

@@ -194,10 +194,10 @@ def workload_config(cfg, scale, prob, world):
 
 def trace_parity(tr_gpu, tr_orc):
     """Largest relative differences of the per-sub-iteration records (chi2,
-    mu, rho) between a GPU trace and the oracle's, over the records both have
-    while the oracle's cost is still falling."""
+    mu, rho, |delta|^2) between a GPU trace and the oracle's, over the records
+    both have while the oracle's cost is still falling."""
     n = min(len(tr_gpu), len(tr_orc))
-    out = {"records": 0, "chi2": 0.0, "mu": 0.0, "rho": 0.0}
+    out = {"records": 0, "chi2": 0.0, "mu": 0.0, "rho": 0.0, "inc_sqnorm": 0.0}
     for k in range(n):
         a, b = tr_gpu[k], tr_orc[k]
         if b[2] < 0 or a[2] < 0:
@@ -210,6 +210,8 @@ def trace_parity(tr_gpu, tr_orc):
             out["mu"] = max(out["mu"], abs(a[3] - b[3]) / abs(b[3]))
         if k > 0:
             out["rho"] = max(out["rho"], abs(a[4] - b[4]) / max(abs(b[4]), 1e-300))
+        if b[5] > 0:
+            out["inc_sqnorm"] = max(out["inc_sqnorm"], abs(a[5] - b[5]) / b[5])
     return out
 
 
@@ -367,8 +369,9 @@ def measure_single(cfg, its, warmup, device):
     out["cpu_baseline"] = {"value": max(its_o, 1) / dt, "unit": UNIT, "cores": cores, "kind": "port",
                            "sample": f"the full {its_o}-iteration LM solve (FP64 C++/OpenMP oracle, {dt:.1f} s)"}
     pm, pd = trace_parity(traces["mixed"], tro), trace_parity(traces["fp64_gpu"], tro)
-    out["oracle_parity"] = {"records_compared": pd["records"], "fp64_gpu": {k: pd[k] for k in ("chi2", "mu", "rho")},
-                            "mixed": {k: pm[k] for k in ("chi2", "mu", "rho")},
+    out["oracle_parity"] = {"records_compared": pd["records"],
+                            "fp64_gpu": {k: pd[k] for k in ("chi2", "mu", "rho", "inc_sqnorm")},
+                            "mixed": {k: pm[k] for k in ("chi2", "mu", "rho", "inc_sqnorm")},
                             "ok": bool(pd["chi2"] <= 1e-9 and pm["chi2"] <= 1e-6 and pd["records"] > 0)}
     out["fp64_gpu_vs_cpu"] = out["fp64_gpu"]["value"] / out["cpu_baseline"]["value"]
     return out
@@ -640,10 +643,20 @@ def main():
                          f"FP64 C++/OpenMP oracle ({dt:.1f} s)"}
         pm, pd = trace_parity(tr_m, tro), trace_parity(tr_d, tro)
         parity = {"oracle_iterations": int(its_o), "records_compared": pd["records"],
-                  "fp64_gpu": {k: pd[k] for k in ("chi2", "mu", "rho")},
-                  "mixed": {k: pm[k] for k in ("chi2", "mu", "rho")},
+                  "fp64_gpu": {k: pd[k] for k in ("chi2", "mu", "rho", "inc_sqnorm")},
+                  "mixed": {k: pm[k] for k in ("chi2", "mu", "rho", "inc_sqnorm")},
                   "bounds": {"fp64_chi2": 1e-9, "mixed_chi2": 1e-6},
                   "ok": bool(pd["chi2"] <= 1e-9 and pm["chi2"] <= 1e-6 and pd["records"] > 0)}
+        # the parameters after the oracle's iterations (outside every timed region)
+        u_o, v_o = o.get_params()
+        par = {}
+        for name, g in (("fp64_gpu", gd), ("mixed", gm)):
+            g.set_params(prob.cams, prob.pts)
+            g.lm_solve(N.LMSettings(maxNumIt=int(its_o)), trace_cap=0)
+            u_g, v_g = g.get_params()
+            par[name] = {"cams_max_rel": float(np.abs(u_g - u_o).max() / np.abs(u_o).max()),
+                         "pts_max_rel": float(np.abs(v_g - v_o).max() / np.abs(v_o).max())}
+        parity["params_after_oracle_iterations"] = par
 
     # ---- the other configurations' headline figures, on rank 0 of a 1-GPU run ----
     others = None

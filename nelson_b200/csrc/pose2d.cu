@@ -40,7 +40,6 @@
 namespace nl {
 namespace {
 
-constexpr int kPoseNT = 256;
 inline int p2_cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 constexpr int kEdgeVals = 10;  // chi2, Hs (00 01 02 11 12 22), bs (0 1 2)
 
@@ -50,27 +49,36 @@ __device__ __forceinline__ double p2_warp_sum(double v) {
   return v;
 }
 
-static __global__ void __launch_bounds__(kPoseNT) pose2d_edge_kernel(
+// One warp per chunk of at most kChunkPts points of one edge (8 warps per
+// CTA): the lane-strided points, 16-byte (x, y) loads, the 10 values
+// butterfly-reduced over the warp, lane i writing value i of the chunk's
+// record.  A fixed order everywhere, so the records are bit-reproducible.
+constexpr int kChunkPts = 128;
+constexpr int kChunkWarps = 8;
+static __global__ void __launch_bounds__(32 * kChunkWarps, 4) pose2d_edge_kernel(
     const double* __restrict__ pose, const int* __restrict__ ea, const int* __restrict__ eb,
-    const int* __restrict__ pt_ptr, const double* __restrict__ mp, const double* __restrict__ mn,
-    const double* __restrict__ tp, double* __restrict__ out, int with_h) {
-  __shared__ double red[kPoseNT / 32][kEdgeVals];
-  const int e = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int* __restrict__ chunk_edge, const int* __restrict__ chunk_p0, int nchunks,
+    const int* __restrict__ pt_ptr, const double2* __restrict__ mp, const double2* __restrict__ mn,
+    const double2* __restrict__ tp, double* __restrict__ out, int with_h) {
+  const int c = blockIdx.x * kChunkWarps + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (c >= nchunks) return;  // the whole warp
+  const int e = chunk_edge[c];
+  const int k0 = chunk_p0[c], k1 = min(k0 + kChunkPts, pt_ptr[e + 1]);
   const double* A = pose + 3 * (size_t)ea[e];
   const double* B = pose + 3 * (size_t)eb[e];
   double ca, sa, cb, sb;
   sincos(A[2], &sa, &ca);
   sincos(B[2], &sb, &cb);
+  const double ax = A[0], ay = A[1], bx = B[0], by = B[1];
   double v[kEdgeVals];
 #pragma unroll
   for (int i = 0; i < kEdgeVals; i++) v[i] = 0.0;
-  for (int k = pt_ptr[e] + tid; k < pt_ptr[e + 1]; k += kPoseNT) {
-    const double m0 = mp[2 * (size_t)k], m1 = mp[2 * (size_t)k + 1];
-    const double n0 = mn[2 * (size_t)k], n1 = mn[2 * (size_t)k + 1];
-    const double q0 = tp[2 * (size_t)k], q1 = tp[2 * (size_t)k + 1];
-    const double xm0 = ca * m0 - sa * m1 + A[0], xm1 = sa * m0 + ca * m1 + A[1];
-    const double N0 = ca * n0 - sa * n1, N1 = sa * n0 + ca * n1;
-    const double xt0 = cb * q0 - sb * q1 + B[0], xt1 = sb * q0 + cb * q1 + B[1];
+#pragma unroll 4
+  for (int k = k0 + lane; k < k1; k += 32) {
+    const double2 m = mp[k], n = mn[k], q = tp[k];
+    const double xm0 = ca * m.x - sa * m.y + ax, xm1 = sa * m.x + ca * m.y + ay;
+    const double N0 = ca * n.x - sa * n.y, N1 = sa * n.x + ca * n.y;
+    const double xt0 = cb * q.x - sb * q.y + bx, xt1 = sb * q.x + cb * q.y + by;
     const double err = (xm0 - xt0) * N0 + (xm1 - xt1) * N1;
     v[0] += err * err;
     if (with_h) {
@@ -86,18 +94,26 @@ static __global__ void __launch_bounds__(kPoseNT) pose2d_edge_kernel(
       v[9] += g2 * err;
     }
   }
+  double mine = 0.0;
 #pragma unroll
   for (int i = 0; i < kEdgeVals; i++) {
-    const double s = p2_warp_sum(v[i]);
-    if (lane == 0) red[warp][i] = s;
+    const double t = p2_warp_sum(v[i]);
+    if (lane == i) mine = t;
   }
-  __syncthreads();
-  if (tid < kEdgeVals) {
-    double s = 0.0;
-#pragma unroll
-    for (int w = 0; w < kPoseNT / 32; w++) s += red[w][tid];
-    out[(size_t)e * kEdgeVals + tid] = s;
-  }
+  if (lane < kEdgeVals) out[(size_t)c * kEdgeVals + lane] = mine;
+}
+
+// an edge's record: its chunks' records summed in chunk order; the edge's
+// cost also goes to the contiguous echi (read by the chi2 reduction)
+static __global__ void pose2d_chunk_sum_kernel(const double* __restrict__ cv, const int* __restrict__ cptr, int ne,
+                                               double* __restrict__ ev, double* __restrict__ echi) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ne * kEdgeVals) return;
+  const int e = t / kEdgeVals, i = t - e * kEdgeVals;
+  double s = 0.0;
+  for (int c = cptr[e]; c < cptr[e + 1]; c++) s += cv[(size_t)c * kEdgeVals + i];
+  ev[t] = s;
+  if (i == 0) echi[e] = s;
 }
 
 // U block entries and b entries from the edges: item q of the (uid, entry)
@@ -130,13 +146,13 @@ static __global__ void pose2d_assemble_kernel(const double* __restrict__ ev, int
   }
 }
 
-// chi2 = sum of the edges' costs, in edge order
-static __global__ void pose2d_chi2_kernel(const double* __restrict__ ev, int ne, double* __restrict__ out) {
+// chi2 = sum of the edges' costs (contiguous), in a fixed order
+static __global__ void pose2d_chi2_kernel(const double* __restrict__ echi, int ne, double* __restrict__ out) {
   __shared__ double red[32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   double s = 0.0;
 #pragma unroll 4
-  for (int e = tid; e < ne; e += blockDim.x) s += ev[(size_t)e * kEdgeVals];
+  for (int e = tid; e < ne; e += blockDim.x) s += echi[e];
   s = p2_warp_sum(s);
   if (lane == 0) red[warp] = s;
   __syncthreads();
@@ -183,6 +199,9 @@ struct nl_pose2d {
   cublasHandle_t cublas = nullptr;
   DevBuf ws, pose, pose_bck, ebuf, scal, lam;
   DevBuf d_ea, d_eb, d_ptr, d_mp, d_mn, d_tp, d_perm, d_uptr, d_uedge, d_usign, d_bptr, d_bedge, d_bsign;
+  DevBuf d_cedge, d_cp0, d_cptr, cbuf;  // point chunks of the edges (kChunkPts each)
+  DevBuf echi;                          // per-edge cost, contiguous
+  int nchunks = 0;
   std::unique_ptr<SchurCore> core;
   std::vector<int> ea, eb, pt_ptr{0}, perm;
   std::vector<std::pair<int, int>> blocks;  // U pattern, (col, row) internal, CSC order
@@ -213,9 +232,14 @@ struct Pose2DOps {
   void update(bool hess) {
     const int ne = (int)h->ea.size();
     if (ne > 0) {
-      pose2d_edge_kernel<<<ne, kPoseNT, 0, h->st>>>(h->pose.as<double>(), h->d_ea.as<int>(), h->d_eb.as<int>(),
-                                                    h->d_ptr.as<int>(), h->d_mp.as<double>(), h->d_mn.as<double>(),
-                                                    h->d_tp.as<double>(), h->ebuf.as<double>(), hess ? 1 : 0);
+      pose2d_edge_kernel<<<p2_cdiv(h->nchunks, kChunkWarps), 32 * kChunkWarps, 0, h->st>>>(
+          h->pose.as<double>(), h->d_ea.as<int>(), h->d_eb.as<int>(), h->d_cedge.as<int>(), h->d_cp0.as<int>(),
+          h->nchunks, h->d_ptr.as<int>(), h->d_mp.as<double2>(), h->d_mn.as<double2>(), h->d_tp.as<double2>(),
+          h->cbuf.as<double>(), hess ? 1 : 0);
+      pose2d_chunk_sum_kernel<<<p2_cdiv(ne * kEdgeVals, 256), 256, 0, h->st>>>(h->cbuf.as<double>(),
+                                                                               h->d_cptr.as<int>(), ne,
+                                                                               h->ebuf.as<double>(),
+                                                                               h->echi.as<double>());
       P2_CUDA(cudaGetLastError());
     }
     if (hess) {
@@ -235,7 +259,7 @@ struct Pose2DOps {
         P2_CUDA(cudaGetLastError());
       }
     }
-    pose2d_chi2_kernel<<<1, 1024, 0, h->st>>>(h->ebuf.as<double>(), ne, h->scal.as<double>());
+    pose2d_chi2_kernel<<<1, 1024, 0, h->st>>>(h->echi.as<double>(), ne, h->scal.as<double>());
     P2_CUDA(cudaGetLastError());
     P2_CUDA(cudaMemcpyAsync(h->pin, h->scal.p, sizeof(double), cudaMemcpyDeviceToHost, h->st));
     if (hess) read_b();
@@ -497,6 +521,26 @@ nl_status nl_pose2d_structure_ready(nl_pose2d* h) {
   if ((s = upload(h->pose, h->pose_h, h->st)) != NL_OK) return s;
   if ((s = h->pose_bck.alloc(h->pose.bytes)) != NL_OK) return s;
   if ((s = h->ebuf.alloc(sizeof(double) * kEdgeVals * (size_t)std::max(ne, 1))) != NL_OK) return s;
+  {
+    // point chunks: every edge gets ceil(npts / kChunkPts) of them, at least one
+    std::vector<int> cedge, cp0, cptr{0};
+    for (int e = 0; e < ne; e++) {
+      const int p0 = h->pt_ptr[e], p1 = h->pt_ptr[e + 1];
+      int p = p0;
+      do {
+        cedge.push_back(e);
+        cp0.push_back(p);
+        p += kChunkPts;
+      } while (p < p1);
+      cptr.push_back((int)cedge.size());
+    }
+    h->nchunks = (int)cedge.size();
+    if ((s = upload(h->d_cedge, cedge, h->st)) != NL_OK) return s;
+    if ((s = upload(h->d_cp0, cp0, h->st)) != NL_OK) return s;
+    if ((s = upload(h->d_cptr, cptr, h->st)) != NL_OK) return s;
+    if ((s = h->cbuf.alloc(sizeof(double) * kEdgeVals * (size_t)std::max(h->nchunks, 1))) != NL_OK) return s;
+    if ((s = h->echi.alloc(sizeof(double) * (size_t)std::max(ne, 1))) != NL_OK) return s;
+  }
   if ((s = h->scal.alloc(64)) != NL_OK) return s;
   if ((s = h->lam.alloc(64)) != NL_OK) return s;
   // the reduced system: U only (bu = 3, nv = 0)

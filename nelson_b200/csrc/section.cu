@@ -10,9 +10,9 @@
 // the device: an evaluate callback writes every edge's whitened residual r_e
 // and Jacobian blocks J_a, J_b into two device arrays owned by the section
 // (fixed per-edge offsets, nl_section_layout), and the section does the rest:
-//   * section_assemble_kernel: one thread per entry of a U / V / W block or
-//     of bU / bV, summing its edges' contributions in edge order (lists built
-//     at structureReady), so H and b are bit-reproducible and need no
+//   * section_assemble_kernel: one thread per row of a U / V / W block or
+//     entry of bU / bV, summing its edges' contributions in edge order (lists
+//     built at structureReady), so H and b are bit-reproducible and need no
 //     atomics; U = sum J_a' J_a (+ J_a' J_b for a U-U edge), V = sum J_v' J_v,
 //     W = sum J_u' J_v, b = sum J' r;
 //   * chi2 = sum r_e' r_e, a fixed-grid two-level reduction;
@@ -38,13 +38,14 @@
 namespace nl {
 namespace {
 
-// One output entry: kind 0 U, 1 V, 2 W (block idx, entry (r, c)), 3 bU, 4 bV
-// (parameter block idx, component r); contributions [q0, q1).
+// One output row: kind 0 U, 1 V, 2 W (block idx, row r, all its columns), 3 bU,
+// 4 bV (parameter block idx, component r); contributions [q0, q1).
 struct SecTask {
-  int kind, idx, r, c, q0, q1;
+  int kind, idx, r, q0, q1, pad;
 };
-// One edge's share of an output: sum over k < m of A[a + k sa + r] * B[b + k sb + c],
-// A the Jacobian array, B the Jacobian array (matrices) or the residuals (vectors).
+// One edge's share of an output: for each column c, sum over k < m of
+// A[a + k sa + r] * B[b + k sb + c], A the Jacobian array, B the Jacobian
+// array (matrices) or the residuals (vectors, one column).
 struct SecContrib {
   long long a, b;
   int sa, sb, m, pad;
@@ -52,8 +53,12 @@ struct SecContrib {
 
 constexpr int kSecNT = 256;
 constexpr int kSecRedCTAs = 296;  // 2 per SM
+constexpr int kSecMaxCols = 9;
 inline int sec_cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 
+// One thread per output row: A[.. + r] is read once per residual row and the
+// B row (contiguous, up to 9 values) feeds every column.  Each entry's sum
+// runs over the contributions in edge order and their rows in order.
 template <typename T>
 static __global__ void __launch_bounds__(128) section_assemble_kernel(
     const SecTask* __restrict__ tasks, int ntasks, const SecContrib* __restrict__ q, const double* __restrict__ J,
@@ -63,20 +68,80 @@ static __global__ void __launch_bounds__(128) section_assemble_kernel(
   if (t >= ntasks) return;
   const SecTask k = tasks[t];
   const double* X = k.kind >= 3 ? R : J;
-  double s = 0.0;
+  const int ncols = k.kind == 0 ? bu : (k.kind <= 2 ? 3 : 1);
+  double s[kSecMaxCols];
+#pragma unroll
+  for (int c = 0; c < kSecMaxCols; c++) s[c] = 0.0;
   for (int i = k.q0; i < k.q1; i++) {
     const SecContrib c = q[i];
     const double* pa = J + c.a + k.r;
-    const double* pb = X + c.b + k.c;
-    for (int row = 0; row < c.m; row++) s += pa[(long long)row * c.sa] * pb[(long long)row * c.sb];
+    const double* pb = X + c.b;
+    for (int row = 0; row < c.m; row++) {
+      const double a = pa[(long long)row * c.sa];
+      const double* brow = pb + (long long)row * c.sb;
+#pragma unroll
+      for (int col = 0; col < kSecMaxCols; col++)
+        if (col < ncols) s[col] += a * brow[col];
+    }
   }
+  T* out;
   switch (k.kind) {
-    case 0: U[(size_t)k.idx * LU + k.r * bu + k.c] = (T)s; break;
-    case 1: V[(size_t)k.idx * LV + k.r * 3 + k.c] = (T)s; break;
-    case 2: W[(size_t)k.idx * LW + k.r * 3 + k.c] = (T)s; break;
-    case 3: bU[(size_t)k.idx * bu + k.r] = (T)s; break;
-    default: bV[(size_t)k.idx * 3 + k.r] = (T)s; break;
+    case 0: out = U + (size_t)k.idx * LU + k.r * bu; break;
+    case 1: out = V + (size_t)k.idx * LV + k.r * 3; break;
+    case 2: out = W + (size_t)k.idx * LW + k.r * 3; break;
+    case 3: out = bU + (size_t)k.idx * bu + k.r; break;
+    default: out = bV + (size_t)k.idx * 3 + k.r; break;
   }
+#pragma unroll
+  for (int col = 0; col < kSecMaxCols; col++)
+    if (col < ncols) out[col] = (T)s[col];
+}
+
+// The rows with long contribution lists (a U block's diagonal rows gather
+// every edge of that block): one warp per row, the lanes striding over the
+// contributions, the partial rows butterfly-reduced in a fixed order.
+constexpr int kSecLongList = 16;
+template <typename T>
+static __global__ void __launch_bounds__(256) section_assemble_warp_kernel(
+    const SecTask* __restrict__ tasks, int ntasks, const SecContrib* __restrict__ q, const double* __restrict__ J,
+    const double* __restrict__ R, int bu, T* __restrict__ U, int LU, T* __restrict__ V, int LV, T* __restrict__ W,
+    int LW, T* __restrict__ bU, T* __restrict__ bV) {
+  const int t = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (t >= ntasks) return;  // the whole warp
+  const SecTask k = tasks[t];
+  const double* X = k.kind >= 3 ? R : J;
+  const int ncols = k.kind == 0 ? bu : (k.kind <= 2 ? 3 : 1);
+  double s[kSecMaxCols];
+#pragma unroll
+  for (int c = 0; c < kSecMaxCols; c++) s[c] = 0.0;
+  for (int i = k.q0 + lane; i < k.q1; i += 32) {
+    const SecContrib c = q[i];
+    const double* pa = J + c.a + k.r;
+    const double* pb = X + c.b;
+    for (int row = 0; row < c.m; row++) {
+      const double a = pa[(long long)row * c.sa];
+      const double* brow = pb + (long long)row * c.sb;
+#pragma unroll
+      for (int col = 0; col < kSecMaxCols; col++)
+        if (col < ncols) s[col] += a * brow[col];
+    }
+  }
+#pragma unroll
+  for (int col = 0; col < kSecMaxCols; col++)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s[col] += __shfl_xor_sync(0xffffffffu, s[col], o);
+  if (lane != 0) return;
+  T* out;
+  switch (k.kind) {
+    case 0: out = U + (size_t)k.idx * LU + k.r * bu; break;
+    case 1: out = V + (size_t)k.idx * LV + k.r * 3; break;
+    case 2: out = W + (size_t)k.idx * LW + k.r * 3; break;
+    case 3: out = bU + (size_t)k.idx * bu + k.r; break;
+    default: out = bV + (size_t)k.idx * 3 + k.r; break;
+  }
+#pragma unroll
+  for (int col = 0; col < kSecMaxCols; col++)
+    if (col < ncols) out[col] = (T)s[col];
 }
 
 __device__ __forceinline__ double sec_block_sum(double v, double* sh) {
@@ -103,10 +168,13 @@ static __global__ void __launch_bounds__(kSecNT) section_sumsq_kernel(const doub
   if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
 
+// one warp: lane-strided partials, then a butterfly (a fixed order)
 static __global__ void section_sum_kernel(const double* __restrict__ part, int n, double* __restrict__ out) {
   double s = 0.0;
-  for (int i = 0; i < n; i++) s += part[i];
-  *out = s;
+  for (int i = threadIdx.x; i < n; i += 32) s += part[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (threadIdx.x == 0) *out = s;
 }
 
 // per-CTA partials of |delta|^2 and delta . b over (U, V)
@@ -151,13 +219,13 @@ struct nl_section {
   bool ready = false;
   cudaStream_t st = nullptr;
   cublasHandle_t cublas = nullptr;
-  DevBuf ws, r, jac, tasks, contribs, d_perm, inc_user, scal, lam, part;
+  DevBuf ws, r, jac, tasks, tasks_long, contribs, d_perm, inc_user, scal, lam, part;
   std::unique_ptr<SchurCore> core;
   std::vector<int> kind, ea, eb, em, perm;
   std::vector<long long> r_off{0}, j_off{0};
   std::vector<std::pair<int, int>> ublk;  // U pattern, (col, row) internal, CSC order
   std::vector<std::pair<int, int>> wblk;  // W pattern, (U block internal, V block), CSR order
-  int ntasks = 0;
+  int ntasks = 0, ntasks_long = 0;  // rows with short / long contribution lists
   nl_section_callbacks cb{};
   bool have_cb = false;
   double chi2 = 0.0, max_b = 0.0, inc_sq = 0.0, inc_b = 0.0;
@@ -194,18 +262,25 @@ struct SectionOps {
     const long long R = h->r_off.back();
     const int g = (int)h->red_grid(R);
     section_sumsq_kernel<<<g, kSecNT, 0, h->st>>>(h->r.as<double>(), R, h->part.as<double>());
-    section_sum_kernel<<<1, 1, 0, h->st>>>(h->part.as<double>(), g, h->scal.as<double>());
+    section_sum_kernel<<<1, 32, 0, h->st>>>(h->part.as<double>(), g, h->scal.as<double>());
     SEC_CUDA(cudaGetLastError());
     SEC_CUDA(cudaMemcpyAsync(h->pin, h->scal.p, sizeof(double), cudaMemcpyDeviceToHost, h->st));
     if (hess) {
       const bool f64 = h->precision == NL_PREC_FP64;
-      if (h->ntasks > 0) {
-        const int blocks = sec_cdiv(h->ntasks, 128);
-#define SEC_ASM(T, BC)                                                                                             \
-  section_assemble_kernel<T><<<blocks, 128, 0, h->st>>>(                                                            \
-      h->tasks.as<SecTask>(), h->ntasks, h->contribs.as<SecContrib>(), h->jac.as<double>(), h->r.as<double>(), h->bu, \
-      (T*)h->core->dU(), Layout<T, BC>::U, (T*)h->core->dV(), Layout<T, BC>::V, (T*)h->core->dW(), Layout<T, BC>::W, \
-      (T*)h->core->dbU(), (T*)h->core->dbV())
+      if (h->ntasks + h->ntasks_long > 0) {
+#define SEC_ASM(T, BC)                                                                                               \
+  do {                                                                                                                \
+    if (h->ntasks > 0)                                                                                                \
+      section_assemble_kernel<T><<<sec_cdiv(h->ntasks, 128), 128, 0, h->st>>>(                                        \
+          h->tasks.as<SecTask>(), h->ntasks, h->contribs.as<SecContrib>(), h->jac.as<double>(), h->r.as<double>(),    \
+          h->bu, (T*)h->core->dU(), Layout<T, BC>::U, (T*)h->core->dV(), Layout<T, BC>::V, (T*)h->core->dW(),         \
+          Layout<T, BC>::W, (T*)h->core->dbU(), (T*)h->core->dbV());                                                  \
+    if (h->ntasks_long > 0)                                                                                           \
+      section_assemble_warp_kernel<T><<<sec_cdiv(h->ntasks_long, 8), 256, 0, h->st>>>(                                \
+          h->tasks_long.as<SecTask>(), h->ntasks_long, h->contribs.as<SecContrib>(), h->jac.as<double>(),             \
+          h->r.as<double>(), h->bu, (T*)h->core->dU(), Layout<T, BC>::U, (T*)h->core->dV(), Layout<T, BC>::V,         \
+          (T*)h->core->dW(), Layout<T, BC>::W, (T*)h->core->dbU(), (T*)h->core->dbV());                               \
+  } while (0)
         switch (h->bu) {
           case 2: if (f64) SEC_ASM(double, 2); else SEC_ASM(float, 2); break;
           case 3: if (f64) SEC_ASM(double, 3); else SEC_ASM(float, 3); break;
@@ -469,13 +544,13 @@ nl_status nl_section_structure_ready(nl_section* s) {
     }
   }
   std::vector<SecContrib> contribs;
-  std::vector<SecTask> tasks;
-  auto add = [&](int kind, int idx, int rows, int cols, const std::vector<SecContrib>& l) {
+  std::vector<SecTask> tasks, tasks_long;
+  auto add = [&](int kind, int idx, int rows, int /*cols: all of the row's, in the kernel*/,
+                 const std::vector<SecContrib>& l) {
     const int q0 = (int)contribs.size();
     contribs.insert(contribs.end(), l.begin(), l.end());
     const int q1 = (int)contribs.size();
-    for (int r = 0; r < rows; r++)
-      for (int c = 0; c < cols; c++) tasks.push_back({kind, idx, r, c, q0, q1});
+    for (int r = 0; r < rows; r++) (q1 - q0 > kSecLongList ? tasks_long : tasks).push_back({kind, idx, r, q0, q1, 0});
   };
   for (int q = 0; q < nU; q++) add(0, q, bu, bu, uq[q]);
   for (int p = 0; p < nv; p++) add(1, p, 3, 3, vq[p]);
@@ -484,8 +559,10 @@ nl_status nl_section_structure_ready(nl_section* s) {
   for (int p = 0; p < nv; p++) add(4, p, 3, 1, cq[p]);
   if (contribs.size() > (size_t)0x7fffffff || tasks.size() > (size_t)0x7fffffff) return NL_ERR_UNSUPPORTED;
   s->ntasks = (int)tasks.size();
+  s->ntasks_long = (int)tasks_long.size();
   nl_status st;
   if ((st = upload(s->tasks, tasks, s->st)) != NL_OK) return st;
+  if ((st = upload(s->tasks_long, tasks_long, s->st)) != NL_OK) return st;
   if ((st = upload(s->contribs, contribs, s->st)) != NL_OK) return st;
   if ((st = upload(s->d_perm, s->perm, s->st)) != NL_OK) return st;
   if ((st = s->r.alloc(sizeof(double) * (size_t)std::max(s->r_off.back(), 1LL))) != NL_OK) return st;

@@ -54,3 +54,31 @@ def test_bad_descriptors_rejected_without_device(lib):
     L = native.load()
     assert L.nl_create(ctypes.byref(desc), ctypes.byref(h)) == 1  # NL_ERR_ARG
     assert L.nl_create(None, ctypes.byref(h)) == 1
+
+
+def test_header_is_c99_and_links(tmp_path):
+    """include/nelson_b200.h is plain C (a cgo / JNI / ctypes binder includes
+    it from C): a C99 program that takes the address of every declared entry
+    point compiles with -pedantic -Werror and links against the library."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    nb_build.build()
+    syms = declared_symbols()
+    src = tmp_path / "abi.c"
+    body = "\n".join(f"  (entry_point)&{s}," for s in syms)
+    src.write_text('#include "nelson_b200.h"\n#include <stdio.h>\n'
+                   "typedef void (*entry_point)(void);\n"
+                   f"static const entry_point entry_points[] = {{\n{body}\n}};\n"
+                   "int main(void) {\n  printf(\"%d\\n\", (int)(sizeof entry_points / sizeof entry_points[0]));\n"
+                   "  return 0;\n}\n")
+    exe = tmp_path / "abi"
+    lib_dir = os.path.dirname(nb_build.LIB)
+    r = subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                        "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(exe), "-L" + lib_dir,
+                        "-lnelson_b200", "-Wl,-rpath," + lib_dir, "-Wl,--allow-shlib-undefined"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert len(syms) > 80

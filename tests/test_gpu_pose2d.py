@@ -173,3 +173,22 @@ def test_errors():
     with pytest.raises(N.NelsonError):
         g.structure_ready()
     g.close()
+
+
+def test_edge_without_points():
+    """An edge holding no points adds nothing (its chunk record is zero)."""
+    p = scan_align_scene(6, 300, noise=NOISE, full_edges=False, seed=4)
+    g = N.Pose2DGPU(6, 1)
+    g.set_poses(p.poses0, p.poses_true[:1])
+    for i, j in p.edges:
+        g.add_edge(i - 1 if i else 0, i == 0, j - 1 if j else 0, j == 0, p.scans[i], p.normals[i], p.scans[j])
+    g.add_edge(0, False, 1, False, np.zeros((0, 2)), np.zeros((0, 2)), np.zeros((0, 2)))
+    g.structure_ready()
+    o = Pose2DOracle(p)
+    o.update(True)
+    assert g.update(True) == pytest.approx(o.chi2, rel=1e-12)
+    H, b = g.hessian()
+    assert np.abs(H - o.H).max() <= 1e-12 * np.abs(o.H).max()
+    g.lm_solve()
+    assert g.update(True) < CHI2_OK
+    g.close()

@@ -266,3 +266,18 @@ def test_errors():
     with pytest.raises(ValueError):
         sec.update(True)
     sec.close()
+
+
+@pytest.mark.parametrize("prec", [N.PREC_FP64, N.PREC_MIXED])
+def test_section_without_v_blocks(prec):
+    """Only U-U edges and U priors (no V blocks): the Schur solve degenerates
+    to the tiled Cholesky of U, as in a pose graph."""
+    s = range_scene(3, nu=12, nv=0, obs_per_point=4, uu_edges=30, seed=3)
+    sec, ev = make(s, prec)
+    assert sec.counts()[1] == 0
+    reason, tr, it = sec.lm_solve(N.LMSettings(maxNumIt=10, epsIncSquare=1e-12))
+    o = SectionOracle(s)
+    r_o, tro, it_o = o.lm_solve(maxNumIt=10, epsIncSquare=1e-12)
+    assert reason == r_o and it == it_o
+    _trace_check(tr, tro, 1e-9 if prec == N.PREC_FP64 else 1e-6)
+    sec.close()

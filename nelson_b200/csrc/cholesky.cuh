@@ -418,27 +418,39 @@ static __global__ void __launch_bounds__(256) trsm_kernel(T* __restrict__ S, int
 // along K: the 8 row addresses of an A load and the 4 of a B load fall in
 // distinct banks, so every warp load is one wavefront, and the 32 FMAs per
 // 6 loads keep the FP32 pipe, not shared memory, the limit.
-constexpr int kSliceRows = 16;
-constexpr int kSliceCtas = NB / kSliceRows;  // 8
+constexpr int kSliceRows = 16;  // rows per CTA of the chain kernels at most (shared-memory sizes)
+// Rows per CTA of the row-tile TRSM and the diagonal-tile update on the
+// factorisation's critical path: 4 (32 CTAs).  Config 2, LM it/s on the
+// B200 with identical results: 16 rows (8 CTAs) 93.1, 8 rows 94.6, 4 rows
+// 95.6 -- every CTA stages the whole panel, so more CTAs cut each one's
+// FMAs, not its copies.
+constexpr int kChainRows = 4;
+static_assert(kChainRows == 16 || kChainRows == 8 || kChainRows == 4, "chain kernels: 4, 8 or 16 rows per CTA");
 constexpr int kSlLd = NB + 4;                // 132
 constexpr size_t kTrsmTileSmem = sizeof(float) * (size_t)(NB + kSliceRows) * kSlLd;  // 76,032 B
 constexpr size_t kDiagUpdSmem = sizeof(float) * (size_t)NB * kSlLd;                 // 67,584 B per panel
 
 // acc[h][m] += sum_l a_h[l] b[16 w + (lane & 3) + 4 m][l], l < NB
+// A CTA of the chain kernels owns RPC rows of a 128 x 128 result as RPC / 2
+// row pairs (a0, a1); warp w owns columns 16 w .. 16 w + 15.  Lane l: pair
+// l / CG, columns 16 w + l % CG + CG m (m < 16 / CG), CG = 32 / (RPC / 2).
+// Each output sums over l = 0 .. 127 in order (x, y, z, w of every float4).
+template <int RPC>
 __device__ inline void slice_mma(const float* __restrict__ a0, const float* __restrict__ a1,
-                                 const float* __restrict__ sb, int lane, int w, float acc[2][4]) {
-  const float* pb = sb + (16 * w + (lane & 3)) * kSlLd;
+                                 const float* __restrict__ sb, int lane, int w, float acc[2][16 / (64 / RPC)]) {
+  constexpr int CG = 64 / RPC, M = 16 / CG;
+  const float* pb = sb + (16 * w + (lane % CG)) * kSlLd;
 #pragma unroll 4
   for (int l = 0; l < NB; l += 4) {
-    float4 a[2], b[4];
+    float4 a[2], b[M];
     a[0] = *reinterpret_cast<const float4*>(a0 + l);
     a[1] = *reinterpret_cast<const float4*>(a1 + l);
 #pragma unroll
-    for (int m = 0; m < 4; m++) b[m] = *reinterpret_cast<const float4*>(pb + 4 * m * kSlLd + l);
+    for (int m = 0; m < M; m++) b[m] = *reinterpret_cast<const float4*>(pb + CG * m * kSlLd + l);
 #pragma unroll
     for (int h = 0; h < 2; h++)
 #pragma unroll
-      for (int m = 0; m < 4; m++) {
+      for (int m = 0; m < M; m++) {
         acc[h][m] = fmaf(a[h].x, b[m].x, acc[h][m]);
         acc[h][m] = fmaf(a[h].y, b[m].y, acc[h][m]);
         acc[h][m] = fmaf(a[h].z, b[m].z, acc[h][m]);
@@ -469,41 +481,43 @@ __device__ inline void stage_rows_f32(const float* __restrict__ src, size_t ld, 
   }
 }
 
+template <int RPC>
 static __global__ void __launch_bounds__(256) trsm_tile_kernel(float* __restrict__ S, int ld, int j,
                                                                const float* __restrict__ Linv,
                                                                uint8_t* __restrict__ pack,
                                                                const int* __restrict__ active) {
+  constexpr int P = RPC / 2, CG = 32 / P, M = 16 / CG;
   extern __shared__ float4 smf4[];
   float* sb = reinterpret_cast<float*>(smf4);  // inv(L_jj), row i = output column i
-  float* sa = sb + NB * kSlLd;                 // the slice's 16 rows of A_(j+1),j
+  float* sa = sb + NB * kSlLd;                 // the slice's RPC rows of A_(j+1),j
   chain_release();
   chain_wait();
   if (active && !*active) return;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const int rel0 = blockIdx.x * kSliceRows;  // first slice row within the tile
+  const int rel0 = blockIdx.x * RPC;  // first slice row within the tile
   float* A = S + (size_t)((j + 1) * NB + rel0) * ld + (size_t)j * NB;
   stage_rows_f32(Linv + (size_t)j * NB * NB, NB, NB, sb, tid);  // zeros above the diagonal included
-  stage_rows_f32(A, ld, kSliceRows, sa, tid);
+  stage_rows_f32(A, ld, RPC, sa, tid);
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
-  float acc[2][4] = {};
-  const float* a0 = sa + (lane >> 2) * kSlLd;
-  slice_mma(a0, a0 + 8 * kSlLd, sb, lane, w, acc);
+  float acc[2][M] = {};
+  const float* a0 = sa + (lane / CG) * kSlLd;
+  slice_mma<RPC>(a0, a0 + P * kSlLd, sb, lane, w, acc);
   // stage the slice of L row-major over the A rows, then store rows to S
   // (float4) and the pack (8 consecutive columns per item)
   __syncthreads();
 #pragma unroll
   for (int h = 0; h < 2; h++)
 #pragma unroll
-    for (int m = 0; m < 4; m++) sa[((lane >> 2) + 8 * h) * kSlLd + 16 * w + (lane & 3) + 4 * m] = acc[h][m];
+    for (int m = 0; m < M; m++) sa[((lane / CG) + P * h) * kSlLd + 16 * w + (lane % CG) + CG * m] = acc[h][m];
   __syncthreads();
-  for (int e = tid; e < kSliceRows * NB / 4; e += 256) {
+  for (int e = tid; e < RPC * NB / 4; e += 256) {
     const int r = e >> 5, c4 = e & 31;
     *reinterpret_cast<float4*>(A + (size_t)r * ld + 4 * c4) = *reinterpret_cast<const float4*>(sa + r * kSlLd + 4 * c4);
   }
   if (pack) {
-    for (int e = tid; e < kSliceRows * 16; e += 256) {
+    for (int e = tid; e < RPC * 16; e += 256) {
       const int r = e >> 4, h = e & 15;
       float x[8];
 #pragma unroll
@@ -513,20 +527,27 @@ static __global__ void __launch_bounds__(256) trsm_tile_kernel(float* __restrict
   }
 }
 
-// Slice c owns tile rows 8c .. 8c+7 and 127-8c-7 .. 127-8c: equal shares of
-// the lower triangle.  A_tt's lower triangle only is written.  np <= 4
-// panels through two staging buffers (min(np, 2) x kDiagUpdSmem bytes of
-// shared memory): panel p + 2 is copied in while panel p + 1 is applied.
+// Slice c of RPC rows owns tile rows P c .. P c + P - 1 and 127 - P c - P + 1
+// .. 127 - P c (P = RPC / 2): equal shares of the lower triangle.  A_tt's
+// lower triangle only is written.  np <= 4 panels through two staging
+// buffers (min(np, 2) x kDiagUpdSmem bytes of shared memory): panel p + 2 is
+// copied in while panel p + 1 is applied.
 constexpr int kDiagUpdMaxPanels = 4;
-__device__ inline int diag_slice_row(int c, int p) { return p < 8 ? 8 * c + p : NB - 1 - 8 * c - (p - 8); }
+template <int RPC>
+__device__ inline int diag_slice_row(int c, int p) {
+  constexpr int P = RPC / 2;
+  return p < P ? P * c + p : NB - 1 - P * c - (p - P);
+}
 
+template <int RPC>
 static __global__ void __launch_bounds__(256) diag_update_kernel(float* __restrict__ S, int ld, int t, int p0, int np,
                                                                  const int* __restrict__ active) {
+  constexpr int P = RPC / 2, CG = 32 / P, M = 16 / CG;
   extern __shared__ float4 smf4[];
   float* sm = reinterpret_cast<float*>(smf4);  // L_t,p (all 128 rows) per panel
   chain_release();
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, c = blockIdx.x;
-  const int ra = diag_slice_row(c, lane >> 2), rb = diag_slice_row(c, 8 + (lane >> 2));
+  const int ra = diag_slice_row<RPC>(c, lane / CG), rb = diag_slice_row<RPC>(c, P + lane / CG);
   const float* T0 = S + (size_t)t * NB * ld + (size_t)p0 * NB;
   // all panels but the last were finished before the stream's preceding
   // kernel (the row-tile TRSM of the last one) started: fetch the first while
@@ -543,7 +564,7 @@ static __global__ void __launch_bounds__(256) diag_update_kernel(float* __restri
   else
     stage_rows_f32(T0, ld, NB, sm, tid);
   cp_async_commit();
-  float acc[2][4] = {};
+  float acc[2][M] = {};
   for (int p = 0; p < np; p++) {
     // committed groups so far: panels 0 .. min(p + 1, np - 1) (one empty
     // group when np == 1); panel p is complete once at most the newest is
@@ -554,7 +575,7 @@ static __global__ void __launch_bounds__(256) diag_update_kernel(float* __restri
       cp_async_wait<0>();
     __syncthreads();
     const float* sb = sm + (p & 1) * NB * kSlLd;
-    slice_mma(sb + ra * kSlLd, sb + rb * kSlLd, sb, lane, w, acc);
+    slice_mma<RPC>(sb + ra * kSlLd, sb + rb * kSlLd, sb, lane, w, acc);
     __syncthreads();  // every warp is done with buffer p & 1
     if (p + 2 < np) {
       stage_rows_f32(T0 + (size_t)(p + 2) * NB, ld, NB, sm + (p & 1) * NB * kSlLd, tid);
@@ -566,8 +587,8 @@ static __global__ void __launch_bounds__(256) diag_update_kernel(float* __restri
   for (int h = 0; h < 2; h++) {
     const int r = h ? rb : ra;
 #pragma unroll
-    for (int m = 0; m < 4; m++) {
-      const int i = 16 * w + (lane & 3) + 4 * m;
+    for (int m = 0; m < M; m++) {
+      const int i = 16 * w + (lane % CG) + CG * m;
       if (i <= r) D[(size_t)r * ld + i] -= acc[h][m];
     }
   }

@@ -215,8 +215,10 @@ class SchurCoreT final : public SchurCore {
     NL_CUDA(cudaFuncSetAttribute(trsm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem<T>()));
     NL_CUDA(cudaFuncSetAttribute(trsv_fwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsv_smem<T>()));
     NL_CUDA(cudaFuncSetAttribute(trsv_bwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsv_smem<T>()));
-    NL_CUDA(cudaFuncSetAttribute(trsm_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmTileSmem));
-    NL_CUDA(cudaFuncSetAttribute(diag_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * (int)kDiagUpdSmem));
+    NL_CUDA(cudaFuncSetAttribute(trsm_tile_kernel<kChainRows>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kTrsmTileSmem));
+    NL_CUDA(cudaFuncSetAttribute(diag_update_kernel<kChainRows>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 2 * (int)kDiagUpdSmem));
     if (!ev_[0]) {
       for (auto& e : ev_) NL_CUDA(cudaEventCreate(&e));
       NL_CUDA(cudaEventCreateWithFlags(&ev_panel_, cudaEventDisableTiming));
@@ -385,7 +387,7 @@ class SchurCoreT final : public SchurCore {
   //           all G panels; TRSM + pack of the rows below tile k+G+1
   //     side  B: tiles of block columns >= k+2G with all G panels.
   // (The tile updates of the chain are diag_update_kernel, the row-tile TRSMs
-  // trsm_tile_kernel: 8 CTAs each, FP32 on CUDA cores.)  Packs live in
+  // trsm_tile_kernel: NB / kChainRows CTAs each, FP32 on CUDA cores.)  Packs live in
   // kPackSlots = 2 G slots (panel mod 2 G): a group's B is the last reader of
   // its slots, and the group after next repacks them only after waiting for it.
   // With G = 2 this is the pair schedule (one B per two panels); G = 4 halves
@@ -444,11 +446,11 @@ class SchurCoreT final : public SchurCore {
       return NL_OK;
     };
     // row tile j+1 of panel j (the critical one) and the diagonal-tile
-    // updates: 8-CTA FP32 kernels on the main stream
+    // updates: 32-CTA FP32 kernels on the main stream (kChainRows rows each)
     auto trsm_first = [&](int j) {
       if (tmc) cudaEventRecord(upd_ev_[10 * nT + 4 * j], st_);
-      trsm_tile_kernel<<<kSliceCtas, 256, kTrsmTileSmem, st_>>>(S, ld_, j, reinterpret_cast<const float*>(Linv_.p),
-                                                                pack_slot(j), active);
+      trsm_tile_kernel<kChainRows><<<NB / kChainRows, 256, kTrsmTileSmem, st_>>>(
+          S, ld_, j, reinterpret_cast<const float*>(Linv_.p), pack_slot(j), active);
       if (tmc) cudaEventRecord(upd_ev_[10 * nT + 4 * j + 1], st_);
       launches++;
     };
@@ -456,7 +458,8 @@ class SchurCoreT final : public SchurCore {
     // (only where no event wait sits between the two)
     auto diag_upd = [&](int t, int p0, int np, bool pdl) -> nl_status {
       if (tmc) cudaEventRecord(upd_ev_[10 * nT + 4 * (t - 1) + 2], st_);
-      NL_CUDA(launch_chain(diag_update_kernel, kSliceCtas, 256, std::min(np, 2) * kDiagUpdSmem, pdl && !tmc, S, ld_,
+      NL_CUDA(launch_chain(diag_update_kernel<kChainRows>, NB / kChainRows, 256, std::min(np, 2) * kDiagUpdSmem,
+                           pdl && !tmc, S, ld_,
                            t, p0, np, active));
       if (tmc) cudaEventRecord(upd_ev_[10 * nT + 4 * (t - 1) + 3], st_);
       launches++;
@@ -562,7 +565,7 @@ class SchurCoreT final : public SchurCore {
       times.panel_ms = pt;
       times.panels = tmc ? npev : 0;
       // per row tile j+1: the waits for the other streams (potrf(j) end ->
-      // TRSM start, TRSM end -> update start) and the two 8-CTA kernels
+      // TRSM start, TRSM end -> update start) and the two chain kernels
       float wt = 0, ft = 0;
       for (int j = 0; j + 1 < npev && tmc; j++) {
         const cudaEvent_t* e = &upd_ev_[10 * nT + 4 * j];

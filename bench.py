@@ -179,6 +179,31 @@ def measured_peaks():
     return {"hbm": 6650.0, "bf16": 1590.0, "bf16_sustained": 1400.0, "src": "fallback"}
 
 
+def fp64_gemm_peak(device):
+    """Dense FP64 throughput of this GPU (TF/s): cuBLAS DGEMM through
+    torch.matmul on 8192^3 (2 N^3 flop), best of 5, CUDA events.  The FP64
+    pipe peak has no driver-measured figure, so the bench measures it here."""
+    import torch
+    n = 8192
+    dev = torch.device("cuda", device)
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize(dev)
+    best = None
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
 def workload_config(cfg, scale, prob, world):
     """The `config` object both arms print for the same workload."""
     s_bytes = (-(-prob.nc_var * prob.bc // 128) * 128) ** 2 * 4
@@ -561,6 +586,21 @@ def main():
     envelope["speedup_vs_fp64_gpu"] = envelope["mixed"]["value"] / envelope["fp64"]["value"]
     envelope["final_chi2_equal_to_dense"] = envelope["mixed"]["final_chi2"] == chi2_m
 
+    # ---- the FP64 comparison path: its trailing update against a measured DGEMM ----
+    fp64_pipe = None
+    if rank == 0:
+        gd.set_params(prob.cams, prob.pts)
+        gd.update(True)
+        gd.compute_increment(0.0, 1e-3 * gd.max_abs_hdiag())
+        p64 = gd.phase_times()
+        dpk = fp64_gemm_peak(local)
+        u64 = p64["update_ms"] * 1e-3
+        a64 = p64["update_flop"] / u64 / 1e12 if u64 > 0 else None
+        fp64_pipe = {"kernel": "cuBLAS DSYRK / DGEMM: the trailing update of the FP64 path's Cholesky",
+                     "achieved_tflops": a64, "peak_tflops": dpk, "frac": (a64 / dpk) if a64 else None,
+                     "peak_source": "measured here: torch.matmul float64 8192^3, best of 5, CUDA events",
+                     "update_ms": p64["update_ms"], "factor_ms": p64["factor_ms"]}
+
     # ---- roofline of the dominant kernel: the trailing update of the factorisation ----
     peaks = measured_peaks()
     hbm, bf16 = peaks["hbm"], peaks["bf16_sustained"]
@@ -671,7 +711,7 @@ def main():
                 "vs_baseline": None, "dtype": "f32 (FP64 refinement residual, solve accumulators, cost)",
                 "data": f"synthetic (seeded, config-{args.config} shapes; no public dataset)",
                 "config": workload_config(args.config, args.scale, prob, world),
-                "fp64_gpu": {"value": fp64_value, "unit": UNIT, "ms_per_step": ms_d / its_d},
+                "fp64_gpu": {"value": fp64_value, "unit": UNIT, "ms_per_step": ms_d / its_d, "pipe": fp64_pipe},
                 "speedup_vs_fp64_gpu": value / fp64_value,
                 "final_cost_rel_err_vs_fp64": final_rel, "per_iter_cost_rel_err_vs_fp64": iter_rel,
                 "oracle_parity": parity,

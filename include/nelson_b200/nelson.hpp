@@ -10,6 +10,10 @@
 //                                                   LevenbergMarquardt<Solver>
 //   GaussNewton<Solver> (GaussNewton.h/.hpp)        GaussNewton<Solver>
 //   LevenbergMarquardtSettings / GaussNewtonSettings  same names and defaults
+//   DoubleSection subclass with user EdgeBinary /  DeviceEdgeSection subclass
+//     EdgeUnary edges (DoubleSection.hpp:338-365)    with device edge code
+//   SingleSection of SE(2) poses, point-to-line     ScanAlignSection
+//     edges (tests/testGaussNewton2DScansAlign.cpp)
 //
 // The solvers meet the reference's Solver concept (nelson/SolverCholeskySchur.h:
 // 71-115: Type, hasSettings, Settings, init(H, b), maxAbsHDiag(),

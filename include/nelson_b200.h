@@ -404,6 +404,7 @@ nl_status nl_solver_set_kind(nl_solver* s, int kind);
  * nelson/SolverCholeskyDense.hpp:39-67) and the left SE(2) update
  * T <- exp(d) T run on the device; LM / GN control on the host. */
 typedef struct nl_pose2d nl_pose2d;
+/* nv >= 1 variable poses, nf >= 0 fixed poses */
 nl_status nl_pose2d_create(int nv, int nf, int precision, int device, nl_pose2d** out);
 nl_status nl_pose2d_destroy(nl_pose2d* h);
 /* poses as (x, y, theta) triples; either pointer may be null */
@@ -467,6 +468,7 @@ typedef struct {
   int (*backup)(void* user, void* stream);
   int (*rollback)(void* user, void* stream);
 } nl_section_callbacks;
+/* nu >= 1 U blocks of bu parameters, nv >= 0 V blocks of 3 */
 nl_status nl_section_create(int bu, int nu, int nv, int precision, int device, nl_section** out);
 nl_status nl_section_destroy(nl_section* s);
 /* addEdge for n edges: kind NL_EDGE_*, blocks a (and b for binary kinds),

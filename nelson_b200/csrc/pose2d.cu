@@ -342,7 +342,7 @@ struct Pose2DOps {
 extern "C" {
 
 nl_status nl_pose2d_create(int nv, int nf, int precision, int device, nl_pose2d** out) {
-  if (nv < 0 || nf < 0 || !out || (precision != NL_PREC_FP64 && precision != NL_PREC_MIXED)) return NL_ERR_ARG;
+  if (nv < 1 || nf < 0 || !out || (precision != NL_PREC_FP64 && precision != NL_PREC_MIXED)) return NL_ERR_ARG;
   *out = nullptr;
   std::unique_ptr<nl_pose2d> h(new nl_pose2d());
   h->nv = nv;

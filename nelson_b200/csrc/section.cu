@@ -370,7 +370,7 @@ struct SectionOps {
 extern "C" {
 
 nl_status nl_section_create(int bu, int nu, int nv, int precision, int device, nl_section** out) {
-  if (!out || nu < 0 || nv < 0 || (bu != 2 && bu != 3 && bu != 6 && bu != 9) ||
+  if (!out || nu < 1 || nv < 0 || (bu != 2 && bu != 3 && bu != 6 && bu != 9) ||
       (precision != NL_PREC_FP64 && precision != NL_PREC_MIXED))
     return NL_ERR_ARG;
   *out = nullptr;

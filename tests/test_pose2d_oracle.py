@@ -91,6 +91,7 @@ def test_handle_argument_checks_without_device():
     L = N.load()
     h = ctypes.c_void_p()
     assert L.nl_pose2d_create(-1, 1, N.PREC_FP64, 0, ctypes.byref(h)) == 1      # NL_ERR_ARG
+    assert L.nl_pose2d_create(0, 1, N.PREC_FP64, 0, ctypes.byref(h)) == 1       # no variable pose
     assert L.nl_pose2d_create(3, 1, 7, 0, ctypes.byref(h)) == 1                 # unknown precision
     assert L.nl_pose2d_create(3, 1, N.PREC_FP64, 0, None) == 1
     assert L.nl_pose2d_destroy(None) == 1

@@ -82,6 +82,7 @@ def test_entry_points_reject_bad_arguments_without_device():
     h = ctypes.c_void_p()
     assert L.nl_section_create(4, 10, 10, N.PREC_FP64, 0, ctypes.byref(h)) == 1    # bu not in 2, 3, 6, 9
     assert L.nl_section_create(3, -1, 10, N.PREC_FP64, 0, ctypes.byref(h)) == 1
+    assert L.nl_section_create(3, 0, 10, N.PREC_FP64, 0, ctypes.byref(h)) == 1      # no U block
     assert L.nl_section_create(3, 10, 10, 5, 0, ctypes.byref(h)) == 1              # precision
     assert L.nl_section_destroy(None) == 1
     assert L.nl_section_update(None, 1, None) == 1

@@ -509,6 +509,12 @@ nl_status nl_section_gn_solve(nl_section* s, const nl_gn_settings* st, nl_solve_
  * max |difference| / max |CUDA-core result| over the updated lower tiles.
  * (No counterpart in the reference: it checks the B200 kernel itself.) */
 nl_status nl_selftest_tc_update(int ntiles, unsigned long long seed, int device, double* max_rel_err);
+/* The same for the rank-K update of the factorisation's panel groups: panels
+ * 0 .. np-1 (np <= 4, K = 128 np) applied in one launch to the trailing tiles
+ * np .. ntiles-1, checked against the CUDA-core update panel by panel; then
+ * `reps` more launches timed alone (best_ms, CUDA events; may be null). */
+nl_status nl_selftest_tc_update_k(int ntiles, int np, unsigned long long seed, int device, int reps,
+                                  double* max_rel_err, double* best_ms);
 
 /* ---- cost without any device allocation ---------------------------------- */
 /* No counterpart in the reference.  The FP64 cost chi2 = sum_e w_e |r_e|^2 of

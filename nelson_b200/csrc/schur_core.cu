@@ -972,3 +972,71 @@ extern "C" nl_status nl_selftest_tc_update(int ntiles, unsigned long long seed, 
   *max_rel_err = md / std::max(mb, 1e-300);
   return NL_OK;
 }
+
+// Self-test and in-isolation timing of the rank-K update the factorisation's
+// groups use: panels 0 .. np-1 of a random FP32 matrix are packed and applied
+// to the trailing tiles np .. ntiles-1 in one launch (K = 128 np), checked
+// against the CUDA-core update applied panel by panel, then timed over
+// `reps` further launches (best, CUDA events).
+extern "C" nl_status nl_selftest_tc_update_k(int ntiles, int np, unsigned long long seed, int device, int reps,
+                                             double* max_rel_err, double* best_ms) {
+  using namespace nl;
+  if (ntiles < 2 || ntiles > 96 || np < 1 || np > kTcMaxPanels || np >= ntiles || reps < 0 || !max_rel_err)
+    return NL_ERR_ARG;
+  NL_CUDA(cudaSetDevice(device));
+  NL_CUDA(tc_prepare());
+  const int ld = ntiles * NB;
+  const size_t n = (size_t)ld * ld;
+  const size_t slot = tc_syrk_scratch_bytes(ld);
+  DevBuf a, b, packs, st;
+  nl_status r;
+  if ((r = a.alloc(n * 4)) != NL_OK || (r = b.alloc(n * 4)) != NL_OK ||
+      (r = packs.alloc(slot * (size_t)np)) != NL_OK || (r = st.alloc(16)) != NL_OK)
+    return r;
+  NL_CUDA(cudaMemset(st.p, 0, 16));
+  selftest_fill_kernel<<<(unsigned)((n + 255) / 256), 256>>>(a.as<float>(), n, seed);
+  NL_CUDA(cudaMemcpy(b.p, a.p, n * 4, cudaMemcpyDeviceToDevice));
+  TcPacks pk{{nullptr, nullptr, nullptr, nullptr}, np};
+  for (int i = 0; i < np; i++) {
+    pk.p[i] = static_cast<uint8_t*>(packs.p) + slot * (size_t)i;
+    NL_CUDA(tc_pack_f32(a.as<float>(), ld, i, 0, ld - (i + 1) * NB, const_cast<void*>(pk.p[i]), nullptr, 0));
+  }
+  const int t0 = np, nt = ntiles - np;
+  NL_CUDA(tc_update_f32(a.as<float>(), ld, 0, t0, nt, 0, 0, pk, nullptr, st.as<int>(), 0));
+  for (int i = 0; i < np; i++) syrk_cc_kernel<float><<<nt * (nt + 1) / 2, 256>>>(b.as<float>(), ld, i, t0, nt, nullptr);
+  NL_CUDA(cudaGetLastError());
+  NL_CUDA(cudaDeviceSynchronize());
+  int stat = 0;
+  NL_CUDA(cudaMemcpy(&stat, st.p, 4, cudaMemcpyDeviceToHost));
+  if (stat & ST_SPIN_TIMEOUT) return NL_ERR_TIMEOUT;
+  std::vector<float> ha(n), hb(n);
+  NL_CUDA(cudaMemcpy(ha.data(), a.p, n * 4, cudaMemcpyDeviceToHost));
+  NL_CUDA(cudaMemcpy(hb.data(), b.p, n * 4, cudaMemcpyDeviceToHost));
+  double md = 0, mb = 0;
+  for (int i = t0 * NB; i < ld; i++)
+    for (int j = t0 * NB; j <= i; j++) {
+      const double x = ha[(size_t)i * ld + j], y = hb[(size_t)i * ld + j];
+      md = std::max(md, std::fabs(x - y));
+      mb = std::max(mb, std::fabs(y));
+    }
+  *max_rel_err = md / std::max(mb, 1e-300);
+  if (best_ms) {
+    double best = 0.0;
+    cudaEvent_t e0, e1;
+    NL_CUDA(cudaEventCreate(&e0));
+    NL_CUDA(cudaEventCreate(&e1));
+    for (int k = 0; k < reps; k++) {
+      NL_CUDA(cudaEventRecord(e0, 0));
+      NL_CUDA(tc_update_f32(a.as<float>(), ld, 0, t0, nt, 0, 0, pk, nullptr, st.as<int>(), 0));
+      NL_CUDA(cudaEventRecord(e1, 0));
+      NL_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      best = (k == 0) ? ms : std::min(best, (double)ms);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *best_ms = best;
+  }
+  return NL_OK;
+}

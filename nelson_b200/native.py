@@ -105,6 +105,7 @@ EXPORTS = [
     "nl_section_get_counts", "nl_section_layout",
     "nl_section_get_patterns", "nl_section_set_callbacks", "nl_section_set_solver_kind", "nl_section_update",
     "nl_section_get_hessian", "nl_section_compute_increment", "nl_section_lm_solve", "nl_section_gn_solve",
+    "nl_selftest_tc_update_k",
     "nl_status_string",
     "nl_version",
 ]
@@ -138,6 +139,7 @@ def load(build_if_missing: bool = True):
     L.nl_solver_create.argtypes = [C.POINTER(SolverDesc), vp, vp, vp, C.POINTER(vp)]
     L.nl_solver_compute_increment.argtypes = [vp, d, d, vp, vp, C.POINTER(i)]
     L.nl_selftest_tc_update.argtypes = [i, C.c_ulonglong, i, C.POINTER(d)]
+    L.nl_selftest_tc_update_k.argtypes = [i, i, C.c_ulonglong, i, i, C.POINTER(d), C.POINTER(d)]
     L.nl_lm_solve_batch.argtypes = [C.POINTER(vp), i, C.POINTER(LMSettings), vp, vp]
     L.nl_adjoint.argtypes = [vp, vp, vp, i, vp, vp, vp, vp, C.POINTER(AdjointReport)]
     L.nl_ba_cost_noalloc.argtypes = [i, i, vp, vp, vp, vp, vp, vp, d, d, d, vp, vp]
@@ -562,6 +564,16 @@ def selftest_tc_update(ntiles=8, seed=1, device=0) -> float:
     err = C.c_double()
     _chk(L, L.nl_selftest_tc_update(ntiles, seed, device, C.byref(err)), "nl_selftest_tc_update")
     return err.value
+
+
+def selftest_tc_update_k(ntiles=48, npanels=4, seed=1, reps=5, device=0):
+    """(max relative difference against the CUDA-core update, best launch ms)
+    of one rank-(128 npanels) tensor-core update of the trailing tiles."""
+    L = load()
+    err, ms = C.c_double(), C.c_double()
+    _chk(L, L.nl_selftest_tc_update_k(ntiles, npanels, seed, device, reps, C.byref(err), C.byref(ms)),
+         "nl_selftest_tc_update_k")
+    return err.value, ms.value
 
 
 class SchurSolverGPU:

@@ -580,12 +580,14 @@ nl_status nl_pose2d_get_hessian(nl_pose2d* h, double* H, double* b) {
   const int LU = f64 ? Layout<double, 3>::U : Layout<float, 3>::U;
   std::vector<double> U((size_t)h->nU * LU), bu(n);
   if (f64) {
-    if (h->nU) NL_CUDA(cudaMemcpyAsync(U.data(), h->core->dU(), sizeof(double) * U.size(), cudaMemcpyDeviceToHost, h->st));
+    if (h->nU)
+      NL_CUDA(cudaMemcpyAsync(U.data(), h->core->dU(), sizeof(double) * U.size(), cudaMemcpyDeviceToHost, h->st));
     if (n) NL_CUDA(cudaMemcpyAsync(bu.data(), h->core->dbU(), sizeof(double) * n, cudaMemcpyDeviceToHost, h->st));
     NL_CUDA(cudaStreamSynchronize(h->st));
   } else {
     std::vector<float> Uf(U.size()), bf(n);
-    if (h->nU) NL_CUDA(cudaMemcpyAsync(Uf.data(), h->core->dU(), sizeof(float) * Uf.size(), cudaMemcpyDeviceToHost, h->st));
+    if (h->nU)
+      NL_CUDA(cudaMemcpyAsync(Uf.data(), h->core->dU(), sizeof(float) * Uf.size(), cudaMemcpyDeviceToHost, h->st));
     if (n) NL_CUDA(cudaMemcpyAsync(bf.data(), h->core->dbU(), sizeof(float) * n, cudaMemcpyDeviceToHost, h->st));
     NL_CUDA(cudaStreamSynchronize(h->st));
     std::copy(Uf.begin(), Uf.end(), U.begin());

@@ -92,7 +92,8 @@ EXPORTS = [
     "nl_rollback", "nl_max_abs_b", "nl_chi2", "nl_rho", "nl_lm_solve", "nl_gn_solve", "nl_phase_timings",
     "nl_kernel_launches", "nl_solver_create", "nl_solver_destroy", "nl_solver_set_hessian",
     "nl_solver_max_abs_hdiag", "nl_solver_compute_increment", "nl_selftest_tc_update", "nl_ba_cost_noalloc",
-    "nl_adjoint", "nl_lm_solve_batch", "nl_set_timing_detail", "nl_set_solver_kind", "nl_solver_set_kind", "nl_permute_rcm_u", "nl_get_user2internal_u", "nl_rcm_order",
+    "nl_adjoint", "nl_lm_solve_batch", "nl_set_timing_detail", "nl_set_solver_kind", "nl_solver_set_kind",
+    "nl_permute_rcm_u", "nl_get_user2internal_u", "nl_rcm_order",
     "nl_permute_amd_u", "nl_amd_order_camera_graph", "nl_amd_order", "nl_symbolic_fill",
     "nl_set_wait_limit", "nl_check_wait_timeout", "nl_unroll_record", "nl_unroll_adjoint",
     "nl_batch_create", "nl_batch_destroy", "nl_batch_autotune", "nl_batch_lm_solve",

@@ -406,18 +406,17 @@ static __global__ void __launch_bounds__(256) trsm_kernel(T* __restrict__ S, int
 }
 
 // ---------------------------------------------------------------------------
-// Critical-path kernels of the tensor-core schedule (FP32).  Each runs as 8
-// CTAs of 256 threads, CTA c owning a 16-row slice of one 128 x 128 tile:
+// Critical-path kernels of the tensor-core schedule (FP32).  Each runs as
+// 128 / RPC CTAs of 256 threads, CTA c owning an RPC-row slice of one
+// 128 x 128 tile (RPC = kChainRows below):
 //   trsm_tile_kernel    L_(j+1),j = A_(j+1),j inv(L_jj)' for row tile j+1 of
 //                       panel j, and its BF16 pack
 //   diag_update_kernel  A_tt -= sum_p L_t,p L_t,p' on diagonal tile t over
 //                       panels p in [p0, p0 + np)
-// Thread (w, lane) of a 16 x 128 slice computes slice rows (lane >> 2) + 8 h
-// (h < 2) and columns 16 w + (lane & 3) + 4 m (m < 4).  Both operands stay
-// row-major in shared memory (row stride 132 floats) and are read as float4
-// along K: the 8 row addresses of an A load and the 4 of a B load fall in
-// distinct banks, so every warp load is one wavefront, and the 32 FMAs per
-// 6 loads keep the FP32 pipe, not shared memory, the limit.
+// Thread (w, lane) of an RPC x 128 slice computes RPC / 2 row pairs (the
+// lane's pair lane / CG, CG = 64 / RPC) and columns 16 w + lane % CG + CG m
+// (m < 16 / CG).  Both operands stay row-major in shared memory (row stride
+// 132 floats) and are read as float4 along K.
 constexpr int kSliceRows = 16;  // rows per CTA of the chain kernels at most (shared-memory sizes)
 // Rows per CTA of the row-tile TRSM and the diagonal-tile update on the
 // factorisation's critical path: 4 (32 CTAs).  Config 2, LM it/s on the
